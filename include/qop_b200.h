@@ -1,0 +1,36 @@
+/*
+ * qop_b200.h -- B200-only extensions to the QOP interface (qop.h).
+ * None of these has a counterpart in the reference; a QOPQDP caller needs
+ * only qop.h.  They expose what a GPU caller needs around the reference
+ * API: the stream the library orders its work on, and per-kernel device
+ * timings for roofline accounting.
+ */
+#ifndef _QOP_B200_H
+#define _QOP_B200_H
+#include "qop.h"
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* The cudaStream_t (as void*) on which every kernel and copy of the library
+   is ordered.  Valid after QOP_init.  A caller may record CUDA events on it
+   to time library calls on the device. */
+void *QOPB_stream(void);
+
+/* Per-kernel-class device timing.  Between QOPB_prof_begin() and
+   QOPB_prof_end() every Dslash-class launch is bracketed by CUDA events on
+   the library stream.  QOPB_prof_end synchronises, fills up to `max`
+   records and returns the number of kernel classes seen. */
+typedef struct {
+  char name[32];            /* kernel class, e.g. "hop_f16_r13"           */
+  int launches;             /* launches recorded                          */
+  double total_ms;          /* summed device time of those launches       */
+  double bytes_per_launch;  /* algorithmic (compulsory) bytes per launch  */
+} QOPB_kstat_t;
+int QOPB_prof_begin(void);
+int QOPB_prof_end(QOPB_kstat_t *out, int max);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

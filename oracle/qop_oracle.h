@@ -1,0 +1,92 @@
+/*
+ * qop_oracle.h -- TEST INFRASTRUCTURE ONLY.
+ *
+ * CPU restatement (plain C99 + OpenMP, FP64 throughout) of the QOPQDP
+ * asqtad/HISQ hot path.  It is the parity checker for the CUDA library and
+ * the timed CPU baseline; nothing in the product links or calls it.
+ *
+ * Parity status: numerically UNPINNED.  The reference cannot be built here
+ * (it needs the external QDP/C, QLA and QMP libraries, none present) and it
+ * ships no golden vectors.  The oracle is pinned to the reference's own
+ * self-consistency tests instead: examples/asqtad_test.c check_op (the
+ * Dslash definition, sign and normalisation, rebuilt from unscaled links
+ * and plain shifts) and check_resids (the eo-solve residual definition).
+ *
+ * Fields are host arrays of doubles in the reference raw layout:
+ *   vector  : V x 3 x (re,im)       matrix : V x 3 x 3 x (re,im)
+ *   site order: even sites first, then odd (lib/layout_user.c:237-258).
+ */
+#ifndef QOP_ORACLE_H
+#define QOP_ORACLE_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct or_lat or_lat;
+typedef struct or_fla or_fla;
+
+typedef struct {
+  double mixed_rsq; int max_iter; int restart; int max_restarts; int evenodd;
+} or_invert_arg;
+typedef struct {
+  double rsqmin, final_rsq, relmin, final_rel; int final_iter, final_restart;
+} or_resid_arg;
+
+/* lattice geometry and raw site order */
+or_lat *or_lat_create(const int L[4]);
+void or_lat_destroy(or_lat *g);
+long or_lat_volume(const or_lat *g);
+long or_raw_index(const or_lat *g, const int x[4]);
+void or_raw_coords(const or_lat *g, long idx, int x[4]);
+long or_neighbor(const or_lat *g, long idx, int mu, int disp);
+
+/* gauge-field setup */
+void or_rephase_G(const or_lat *g, double *links[4], const int r0[4],
+                  const double *bc_reim /* 8 doubles or NULL */,
+                  const int *signmask /* 4 ints or NULL */);
+void or_make_imp_links(const or_lat *g, const double coef[6],
+                       double *gf[4], double *gfLong[4],
+                       double *fl[4], double *ll[4] /* NULL => no Naik */);
+int or_u3_un_analytic(const double V[18], double W[18], int allow_svd,
+                      double svd_rel_err, double svd_abs_err);
+int or_u3reunit(const or_lat *g, double *Vf, double *Wf);
+/* HISQ: returns number of SVD-fallback sites. out fat/long = asqtad stage
+   (eps index 0); hcoef layout = 17 doubles:
+   fat7[1,3,5,7,lepage], asqtad[1,3,5,7,lepage,naik], diff[1,naik],
+   use_fat7_lepage, allow_svd, svd_rel, svd_abs */
+int or_hisq_links(const or_lat *g, const double hcoef[17], double *gauge[4],
+                  double *fat[4], double *lng[4], double *W[4] /* may be NULL */);
+
+/* asqtad operator object (links scaled by 1/2, double stored) */
+or_fla *or_fla_create(or_lat *g, double *fat[4], double *lng[4] /* may be NULL */);
+void or_fla_destroy(or_fla *f);
+void or_dslash(or_fla *f, double mass, double *out, const double *in,
+               int eo_out, int eo_in);
+void or_dslash_dir(or_fla *f, int dir, int fb, double wtfat, double wtlong,
+                   double *out, const double *in, int eo_out);
+void or_ddagd(or_fla *f, double mass, double *out, const double *in, int eo);
+double or_ddagd_norm2(or_fla *f, double mass, double *out, const double *in, int eo);
+/* examples/asqtad_test.c:37-81: |chk-out|^2/|in|^2 with chk rebuilt from
+   unscaled links and plain shifts */
+double or_check_op(or_fla *f, double mass, const double *in,
+                   double *fat[4], double *lng[4]);
+double or_relnorm2(const or_lat *g, const double *r, const double *x, int eo);
+
+/* inverters (lib/asqtad_invert_p.c) */
+void or_invert(or_fla *f, or_invert_arg *ia, or_resid_arg *ra, double mass,
+               double *out, const double *in, double *final_flop);
+void or_invert_multi(or_fla *f, or_invert_arg *ia, or_resid_arg **ra[],
+                     double *masses[], int nmass[], double **out[],
+                     double *in[], int nsrc, double *final_flop);
+void or_solve_multi(or_fla *f, or_invert_arg *ia, or_resid_arg *ra[],
+                    double masses[], double *out[], double *in[], int nsolve,
+                    double *final_flop);
+
+/* threads used by OpenMP regions (0 = leave default) */
+void or_set_threads(int n);
+int or_get_threads(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

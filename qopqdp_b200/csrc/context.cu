@@ -1,0 +1,237 @@
+// context.cu -- library state, QOP_init/finalize, options, allocation.
+// Reference: lib/common.c:39-191 (init, version, verbosity, raw index),
+// lib/asqtad_invert.c:9-113 (inverter options), lib/hisq_links.c:32-78.
+#include "qopb.h"
+#include <cstdarg>
+#include <sys/time.h>
+
+namespace qopb {
+
+static Context g_ctx;
+Context &ctx() { return g_ctx; }
+
+void check_cuda(cudaError_t e, const char *what, const char *file, int line) {
+  if (e == cudaSuccess) return;
+  cudaGetLastError();   // clear sticky-free errors
+  char buf[512];
+  snprintf(buf, sizeof buf, "CUDA error '%s' in %s (%s:%d)", cudaGetErrorString(e), what, file, line);
+  throw Fail(e == cudaErrorMemoryAllocation ? QOP_MEM_ERROR : QOP_FAIL, buf);
+}
+
+void fail(QOP_status_t s, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  throw Fail(s, buf);
+}
+
+void log0(int level, const char *fmt, ...) {
+  if (g_ctx.verbosity < level) return;
+  va_list ap;
+  va_start(ap, fmt);
+  vprintf(fmt, ap);
+  va_end(ap);
+  fflush(stdout);
+}
+
+double wtime() {
+  struct timeval tv;
+  gettimeofday(&tv, nullptr);
+  return tv.tv_sec + 1e-6 * tv.tv_usec;
+}
+
+void require_init(const char *fn) {
+  if (!g_ctx.inited) fail(QOP_FAIL, "%s: QOP_init has not been called", fn);
+}
+
+void ensure_ready() {
+  Context &c = g_ctx;
+  if (c.s) return;
+  QCHECK(cudaGetDevice(&c.device));
+  QCHECK(cudaStreamCreateWithFlags(&c.s, cudaStreamNonBlocking));
+  int sms = 0;
+  QCHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device));
+  c.red_blocks = sms * 8;
+  QCHECK(cudaMalloc(&c.d_part, sizeof(double) * 8 * c.red_blocks));
+  QCHECK(cudaMalloc(&c.d_count, sizeof(unsigned) * 4));
+  QCHECK(cudaMemset(c.d_count, 0, sizeof(unsigned) * 4));
+  QCHECK(cudaMalloc(&c.d_res, sizeof(double) * 64));
+  QCHECK(cudaMallocHost(&c.h_res, sizeof(double) * 64));
+  // keep freed blocks cached in the stream-ordered pool
+  cudaMemPool_t pool;
+  QCHECK(cudaDeviceGetDefaultMemPool(&pool, c.device));
+  uint64_t thr = UINT64_MAX;
+  QCHECK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+}
+
+void *dmalloc(size_t bytes) {
+  ensure_ready();
+  void *p = nullptr;
+  if (bytes == 0) bytes = 16;
+  cudaError_t e = cudaMallocAsync(&p, bytes, g_ctx.s);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    fail(QOP_MEM_ERROR, "device allocation of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
+  }
+  return p;
+}
+void dfree(void *p) {
+  if (p && g_ctx.s) cudaFreeAsync(p, g_ctx.s);
+}
+void dzero(void *p, size_t bytes) { QCHECK(cudaMemsetAsync(p, 0, bytes, g_ctx.s)); }
+void sync() { QCHECK(cudaStreamSynchronize(g_ctx.s)); }
+
+int grid_for(i64 n, int block) {
+  i64 b = (n + block - 1) / block;
+  if (b < 1) b = 1;
+  if (b > 0x7fffffff) b = 0x7fffffff;
+  return (int)b;
+}
+
+}  // namespace qopb
+
+using namespace qopb;
+
+#define OPT_TRY try {
+#define OPT_CATCH(ret) } catch (Fail &e) { log0(0, "QOP error: %s\n", e.msg.c_str()); return ret; }
+
+extern "C" {
+
+QOP_status_t QOP_init(QOP_layout_t *layout) {
+  Context &c = ctx();
+  if (c.inited) return QOP_FAIL;
+  if (!layout || layout->latdim != 4 || !layout->latsize) {
+    fprintf(stderr, "QOP_init: only 4-dimensional lattices are supported\n");
+    return QOP_FAIL;
+  }
+  Geom g{};
+  g.V = 1;
+  for (int i = 0; i < 4; i++) {
+    int L = layout->latsize[i];
+    if (L < 4 || (L & 1)) {
+      fprintf(stderr, "QOP_init: extent %d in direction %d must be even and >= 4\n", L, i);
+      return QOP_FAIL;
+    }
+    g.L[i] = L;
+    g.V *= L;
+  }
+  g.Vh = g.V / 2;
+  if (g.V >= (1LL << 31)) {
+    fprintf(stderr, "QOP_init: volume too large for one device\n");
+    return QOP_FAIL;
+  }
+  OPT_TRY
+  ensure_ready();
+  OPT_CATCH(QOP_FAIL)
+  c.g = g;
+  c.verbosity = 0;
+  c.proflevel = 0;
+  c.inited = 1;
+  return QOP_SUCCESS;
+}
+
+QOP_status_t QOP_finalize(void) {
+  Context &c = ctx();
+  if (!c.inited) return QOP_FAIL;
+  if (c.s) cudaStreamSynchronize(c.s);
+  c.inited = 0;
+  return QOP_SUCCESS;
+}
+
+int QOP_is_initialized(void) { return ctx().inited; }
+
+const char *QOP_version_str(void) { return "0.21.1-b200"; }
+int QOP_version_int(void) { return (0 * 1000 + 21) * 1000 + 1; }
+
+int QOP_verbose(int level) {
+  int old = ctx().verbosity;
+  ctx().verbosity = level;
+  return old;
+}
+int QOP_profcontrol(int level) {
+  int old = ctx().proflevel;
+  ctx().proflevel = level;
+  return old;
+}
+
+// single process: every site lives on node 0 (lib/common.c:134-139)
+int QOP_node_number_raw(int coords[]) { (void)coords; return 0; }
+
+// raw index of a site: even sites first (lib/layout_user.c:237-258)
+static int raw_index(const int x[]) {
+  const Geom &g = ctx().g;
+  i64 l = 0;
+  int s = 0;
+  for (int i = 0; i < 4; i++) { l = l * g.L[i] + x[i]; s += x[i]; }
+  return (int)((s & 1) ? (l + g.V) / 2 : l / 2);
+}
+int QOP_node_index_raw_V(int coords[], QOP_evenodd_t eo) { (void)eo; return ctx().inited ? raw_index(coords) : -1; }
+int QOP_node_index_raw_G(int coords[], QOP_evenodd_t eo) { (void)eo; return ctx().inited ? raw_index(coords) : -1; }
+int QOP_sites_on_node_raw_V(QOP_evenodd_t eo) { (void)eo; return (int)ctx().g.V; }
+int QOP_sites_on_node_raw_G(QOP_evenodd_t eo) { (void)eo; return (int)ctx().g.V; }
+
+// tags: st, ns, nm, cg, eigcg_nev, eigcg_m, eigcg_l (reference) and
+// prec_sloppy (64|32|16), ru_delta, chunk (B200 additions)
+QOP_status_t QOP_asqtad_invert_set_opts(QOP_opt_t opts[], int nopts) {
+  Options &o = ctx().opt;
+  int st = o.style, ns = o.nsvec, nm = o.nvec;
+  auto valid_nv = [](int nv, int s) { return nv == 1 || nv == 2 || nv == 4 || nv == 8 || (s == 1 && nv == 16); };
+  for (int i = 0; i < nopts; i++)
+    if (opts[i].tag && !strcmp(opts[i].tag, "st")) st = (int)opts[i].value;
+  if (st < 0 || st > 3) return QOP_FAIL;
+  if (!valid_nv(ns, st)) ns = ns < 1 ? 1 : 8;
+  if (!valid_nv(nm, st)) nm = nm < 1 ? 1 : 8;
+  Options n = o;
+  for (int i = 0; i < nopts; i++) {
+    const char *t = opts[i].tag;
+    double v = opts[i].value;
+    if (!t) continue;
+    if (!strcmp(t, "ns")) ns = (int)v;
+    else if (!strcmp(t, "nm")) nm = (int)v;
+    else if (!strcmp(t, "cg")) n.cgtype = (int)v;
+    else if (!strcmp(t, "eigcg_nev")) n.eigcg_nev = (int)v;
+    else if (!strcmp(t, "eigcg_m")) n.eigcg_m = (int)v;
+    else if (!strcmp(t, "eigcg_l")) n.eigcg_numax = (int)v;
+    else if (!strcmp(t, "prec_sloppy")) {
+      int p = (int)v;
+      if (p != 16 && p != 32 && p != 64) return QOP_FAIL;
+      n.sloppy_prec = p;
+    } else if (!strcmp(t, "ru_delta")) {
+      if (!(v > 0 && v < 1)) return QOP_FAIL;
+      n.ru_delta = v;
+    } else if (!strcmp(t, "chunk")) {
+      if (v < 1 || v > 1024) return QOP_FAIL;
+      n.chunk = (int)v;
+    }
+  }
+  if (!valid_nv(ns, st) || !valid_nv(nm, st)) return QOP_FAIL;
+  n.style = st; n.nsvec = ns; n.nvec = nm;
+  o = n;
+  return QOP_SUCCESS;
+}
+
+QOP_status_t QOP_hisq_invert_set_opts(QOP_opt_t opts[], int nopts) {
+  return QOP_asqtad_invert_set_opts(opts, nopts);
+}
+
+QOP_status_t QOP_hisq_links_set_opts(QOP_opt_t opts[], int nopts) {
+  Options &o = ctx().opt;
+  for (int i = 0; i < nopts; i++) {
+    const char *t = opts[i].tag;
+    double v = opts[i].value;
+    if (!t) continue;
+    if (!strcmp(t, "want_deps")) o.want_deps = (int)v;
+    else if (!strcmp(t, "want_aux")) o.want_aux = (int)v;
+    else if (!strcmp(t, "reunit_allow_svd")) o.reunit_allow_svd = (int)v;
+    else if (!strcmp(t, "reunit_svd_only")) o.reunit_svd_only = (int)v;
+    else if (!strcmp(t, "reunit_svd_rel_error")) o.reunit_svd_rel_error = v;
+    else if (!strcmp(t, "reunit_svd_abs_error")) o.reunit_svd_abs_error = v;
+    else if (!strcmp(t, "svd_values_info")) o.svd_values_info = (int)v;
+    else if (!strcmp(t, "use_fat7_lepage")) o.use_fat7_lepage = (int)v;
+  }
+  return QOP_SUCCESS;
+}
+
+}  // extern "C"

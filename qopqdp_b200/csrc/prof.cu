@@ -1,0 +1,104 @@
+// prof.cu -- per-kernel-class device timing with CUDA events on the library
+// stream (QOPB_prof_begin / QOPB_prof_end), plus QOPB_stream.
+#include "qopb.h"
+#include "prof.cuh"
+#include <vector>
+#include <string>
+
+namespace qopb {
+
+namespace {
+struct Cls { std::string name; double bytes; int launches = 0; double ms = 0; };
+struct Rec { int cls; cudaEvent_t a, b; };
+struct Prof {
+  bool active = false;
+  std::vector<Cls> cls;
+  std::vector<cudaEvent_t> pool;   // free events
+  std::vector<Rec> recs;
+  size_t cap = 1 << 16;            // at most this many recorded launches
+};
+Prof g_prof;
+
+cudaEvent_t take_event() {
+  if (g_prof.pool.empty()) {
+    for (int i = 0; i < 256; i++) {
+      cudaEvent_t e;
+      if (cudaEventCreate(&e) != cudaSuccess) { cudaGetLastError(); break; }
+      g_prof.pool.push_back(e);
+    }
+    if (g_prof.pool.empty()) return nullptr;
+  }
+  cudaEvent_t e = g_prof.pool.back();
+  g_prof.pool.pop_back();
+  return e;
+}
+}  // namespace
+
+int prof_start(const char *name, double bytes) {
+  if (!g_prof.active || g_prof.recs.size() >= g_prof.cap) return -1;
+  int c = -1;
+  for (size_t i = 0; i < g_prof.cls.size(); i++)
+    if (g_prof.cls[i].name == name && g_prof.cls[i].bytes == bytes) { c = (int)i; break; }
+  if (c < 0) {
+    g_prof.cls.push_back(Cls{name, bytes});
+    c = (int)g_prof.cls.size() - 1;
+  }
+  cudaEvent_t a = take_event(), b = take_event();
+  if (!a || !b) return -1;
+  cudaEventRecord(a, ctx().s);
+  g_prof.recs.push_back(Rec{c, a, b});
+  return (int)g_prof.recs.size() - 1;
+}
+
+void prof_stop(int idx) {
+  if (idx < 0) return;
+  cudaEventRecord(g_prof.recs[idx].b, ctx().s);
+}
+
+bool prof_active() { return g_prof.active; }
+
+}  // namespace qopb
+
+using namespace qopb;
+
+extern "C" void *QOPB_stream(void) {
+  try {
+    ensure_ready();
+  } catch (Fail &) {
+    return nullptr;
+  }
+  return (void *)ctx().s;
+}
+
+extern "C" int QOPB_prof_begin(void) {
+  g_prof.recs.clear();
+  g_prof.cls.clear();
+  g_prof.active = true;
+  return 0;
+}
+
+extern "C" int QOPB_prof_end(QOPB_kstat_t *out, int max) {
+  g_prof.active = false;
+  if (ctx().s) cudaStreamSynchronize(ctx().s);
+  for (auto &r : g_prof.recs) {
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, r.a, r.b) == cudaSuccess) {
+      g_prof.cls[r.cls].ms += ms;
+      g_prof.cls[r.cls].launches += 1;
+    } else {
+      cudaGetLastError();
+    }
+    g_prof.pool.push_back(r.a);
+    g_prof.pool.push_back(r.b);
+  }
+  g_prof.recs.clear();
+  int n = (int)g_prof.cls.size();
+  for (int i = 0; i < n && i < max && out; i++) {
+    memset(out[i].name, 0, sizeof(out[i].name));
+    strncpy(out[i].name, g_prof.cls[i].name.c_str(), sizeof(out[i].name) - 1);
+    out[i].launches = g_prof.cls[i].launches;
+    out[i].total_ms = g_prof.cls[i].ms;
+    out[i].bytes_per_launch = g_prof.cls[i].bytes;
+  }
+  return n;
+}

@@ -1,0 +1,209 @@
+// qopb.h -- internal declarations of the B200 asqtad/HISQ library.
+//
+// HBM layout (all fields checkerboarded, structure-of-arrays):
+//   site index i in parity p: i = lex(x)/2 with lex = ((x0*L1+x1)*L2+x2)*L3+x3,
+//   which is the reference raw index minus p*Vh (lib/layout_user.c:237-258),
+//   so a raw parity half maps to a device parity block without reordering.
+//   vector  : [parity][colour c][site i]            complex  (T2)
+//   matrix  : [parity][element e=3a+b][site i]      complex
+//   links   : [parity][slot k][element e][site i]   complex, slot k is the
+//             reference's dbllinks order: 4mu+{fat fwd, long fwd, fat bck,
+//             long bck}, shifts {+1,+3,-1,-3} along mu (16 slots; 8 without
+//             Naik: 2mu+{fwd,bck}); links are stored times 1/2 as the reference
+//             does (lib/asqtad_dslash_p.c:201-206).
+// Consecutive threads take consecutive sites, so every link, mass-term and
+// output access is a unit-stride coalesced load/store; neighbour gathers are
+// unit stride within a row of x3 and hit L2 otherwise.
+#pragma once
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <type_traits>
+#include <stdexcept>
+#include "qop.h"
+#include "qop_b200.h"
+
+namespace qopb {
+
+typedef long long i64;
+
+// ---------------------------------------------------------------- errors
+struct Fail {
+  QOP_status_t status;
+  std::string msg;
+  Fail(QOP_status_t s, std::string m) : status(s), msg(std::move(m)) {}
+};
+void check_cuda(cudaError_t e, const char *what, const char *file, int line);
+#define QCHECK(x) ::qopb::check_cuda((x), #x, __FILE__, __LINE__)
+#define QLAUNCH() ::qopb::check_cuda(cudaGetLastError(), "kernel launch", __FILE__, __LINE__)
+[[noreturn]] void fail(QOP_status_t s, const char *fmt, ...);
+
+// ---------------------------------------------------------------- geometry
+struct Geom {
+  int L[4];
+  i64 V, Vh;
+};
+
+// ---------------------------------------------------------------- complex
+template <typename T> struct Cx;
+template <> struct Cx<float> { typedef float2 t; };
+template <> struct Cx<double> { typedef double2 t; };
+template <typename T> using c2 = typename Cx<T>::t;
+
+template <typename T> __host__ __device__ inline c2<T> mk(T r, T i) { c2<T> z; z.x = r; z.y = i; return z; }
+template <typename T> __host__ __device__ inline c2<T> cadd(c2<T> a, c2<T> b) { return mk<T>(a.x + b.x, a.y + b.y); }
+template <typename T> __host__ __device__ inline c2<T> csub(c2<T> a, c2<T> b) { return mk<T>(a.x - b.x, a.y - b.y); }
+template <typename T> __host__ __device__ inline c2<T> cmul(c2<T> a, c2<T> b) {
+  return mk<T>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+template <typename T> __host__ __device__ inline c2<T> cconjmul(c2<T> a, c2<T> b) {  // conj(a) b
+  return mk<T>(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x);
+}
+template <typename T> __host__ __device__ inline c2<T> cscale(T s, c2<T> a) { return mk<T>(s * a.x, s * a.y); }
+// acc += a*b
+template <typename T> __host__ __device__ inline void cfma(c2<T> &acc, c2<T> a, c2<T> b) {
+  acc.x += a.x * b.x - a.y * b.y;
+  acc.y += a.x * b.y + a.y * b.x;
+}
+
+// host-side double complex used for solver scalars
+struct dcx {
+  double re, im;
+};
+inline dcx operator+(dcx a, dcx b) { return {a.re + b.re, a.im + b.im}; }
+inline dcx operator-(dcx a, dcx b) { return {a.re - b.re, a.im - b.im}; }
+inline dcx operator*(dcx a, dcx b) { return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
+inline dcx operator*(double s, dcx a) { return {s * a.re, s * a.im}; }
+inline dcx cdiv(dcx a, dcx b) {
+  double d = b.re * b.re + b.im * b.im;
+  return {(a.re * b.re + a.im * b.im) / d, (a.im * b.re - a.re * b.im) / d};
+}
+inline double norm2(dcx a) { return a.re * a.re + a.im * a.im; }
+
+// ---------------------------------------------------------------- context
+struct Options {
+  // QOP_asqtad_invert_set_opts (lib/asqtad_invert.c:69-113)
+  int style = 1, nsvec = 8, nvec = 8, cgtype = 0;
+  int eigcg_nev = 10, eigcg_m = 100, eigcg_numax = 200;
+  // B200 additions: sloppy precision of the inner Krylov solve
+  // (64 = exact reference algorithm in the handle's precision)
+  int sloppy_prec = 64;
+  double ru_delta = 0.1;         // reliable-update threshold on |r|
+  int chunk = 16;                // iterations launched per host check
+  // QOP_hisq_links_set_opts (lib/hisq_links.c:4-78)
+  int want_deps = 0, want_aux = 1, reunit_allow_svd = 1, reunit_svd_only = 0;
+  double reunit_svd_rel_error = 1e-8, reunit_svd_abs_error = 1e-8;
+  int svd_values_info = 1, use_fat7_lepage = 0;
+};
+
+struct Context {
+  int inited = 0;
+  int verbosity = 0;
+  int proflevel = 0;
+  Geom g{};
+  int device = 0;
+  cudaStream_t s = nullptr;
+  Options opt;
+  // reduction scratch: per-block partials + completion counter + result
+  double *d_part = nullptr;
+  unsigned *d_count = nullptr;
+  double *d_res = nullptr;
+  double *h_res = nullptr;   // pinned
+  int red_blocks = 0;
+};
+Context &ctx();
+void require_init(const char *fn);
+void ensure_ready();   // lazily creates stream and scratch on the current device
+
+// stream-ordered device allocation, throws QOP_MEM_ERROR on failure
+void *dmalloc(size_t bytes);
+void dfree(void *p);
+template <typename T> T *dalloc(i64 n) { return (T *)dmalloc(sizeof(T) * (size_t)n); }
+void dzero(void *p, size_t bytes);
+void sync();
+
+int grid_for(i64 n, int block);
+
+// ---------------------------------------------------------------- handles
+template <typename T> struct VecT {       // QOP_*_ColorVector
+  c2<T> *d = nullptr;                     // [2][3][Vh]
+};
+template <typename T> struct GaugeT {     // QOP_*_GaugeField
+  c2<T> *d = nullptr;                     // [4 mu][2][9][Vh]
+  int *r0 = nullptr; QOP_Complex *bc = nullptr; int *signmask = nullptr;
+};
+struct SloppyLinks;                       // reduced-precision copies (mixed.cu)
+template <typename T> struct FlaT {       // QOP_*_FermionLinksAsqtad
+  int nlinks = 16;
+  c2<T> *d = nullptr;                     // [2][nlinks][9][Vh], x 1/2, double stored
+  SloppyLinks *sl = nullptr;
+  void *shadow32 = nullptr;               // FlaT<float>* copy used by mixed solves
+};
+template <typename T> struct HisqT {      // QOP_*_FermionLinksHisq
+  int n_naiks = 1;
+  FlaT<T> *fn[QOP_MAX_NAIK] = {};
+  FlaT<T> *fn_deps = nullptr;
+  GaugeT<T> *U = nullptr, *V = nullptr, *W = nullptr;   // auxiliary links (want_aux)
+};
+
+inline i64 vec_elems(const Geom &g) { return 2 * 3 * g.Vh; }
+inline i64 par_off(const Geom &g, int p) { return (i64)p * 3 * g.Vh; }
+
+// subset helpers: a parity block of a vector is contiguous
+struct Range { i64 off, n; };   // in complex elements
+inline Range vrange(const Geom &g, int eo) {
+  if (eo == QOP_EVEN) return {0, 3 * g.Vh};
+  if (eo == QOP_ODD) return {3 * g.Vh, 3 * g.Vh};
+  return {0, 6 * g.Vh};
+}
+inline int opp(int eo) { return eo == QOP_EVEN ? QOP_ODD : eo == QOP_ODD ? QOP_EVEN : QOP_EVENODD; }
+
+// ---------------------------------------------------------------- BLAS (blas.cu)
+template <typename T> struct Blas {
+  static void zero(c2<T> *v, Range r);
+  static void copy(c2<T> *d, const c2<T> *s, Range r);
+  static void scale(c2<T> *d, double a, const c2<T> *s, Range r);                 // d = a s
+  static void cscale(c2<T> *d, dcx a, const c2<T> *s, Range r);                   // d = a s
+  static void axpy(c2<T> *y, double a, const c2<T> *x, Range r);                  // y += a x
+  static void caxpy(c2<T> *y, dcx a, const c2<T> *x, Range r);                    // y += a x
+  static void xpay(c2<T> *y, const c2<T> *x, double a, Range r);                  // y = x + a y
+  static void axpby(c2<T> *z, double a, const c2<T> *x, double b, const c2<T> *y, Range r); // z = a x + b y
+  static void caxpby(c2<T> *z, dcx a, const c2<T> *x, const c2<T> *y, Range r);   // z = a x + y
+  static double norm2(const c2<T> *v, Range r);
+  static double redot(const c2<T> *a, const c2<T> *b, Range r);
+  static dcx cdot(const c2<T> *a, const c2<T> *b, Range r);                       // sum conj(a) b
+  // x += a p ; r -= a Ap ; returns |r|^2
+  static double cg_update(c2<T> *x, c2<T> *r, double a, const c2<T> *p, const c2<T> *Ap, Range q);
+  // sum over sites of |r|^2/|x|^2 (1 where |x| = 0), single parity or both
+  static double relnorm_sum(const c2<T> *r, const c2<T> *x, int eo);
+};
+// convert between precisions (d = s over range)
+template <typename TD, typename TS> void convert(c2<TD> *d, const c2<TS> *s, Range r);
+
+// ---------------------------------------------------------------- dslash (dslash.cu)
+template <typename T> struct Dslash {
+  // reference semantics of QOP_asqtad_dslash_qdp (lib/asqtad_dslash_p.c:1048-1092)
+  static void apply(FlaT<T> *f, double mass, c2<T> *out, const c2<T> *in, int eo_out, int eo_in);
+  // out_p = hop_p(in)  [+ epilogues]; parity p in {0,1}
+  static void hop(FlaT<T> *f, c2<T> *out, const c2<T> *in, int p);
+  static void dslash_dir(FlaT<T> *f, int dir, int fb, double wtfat, double wtlong,
+                         c2<T> *out, const c2<T> *in, int eo_out);
+  // ddagd (asqtad_dslash_p.c:1106-1138): out_eo = m^2 in - D_eo,oe D_oe,eo in;
+  // tmp receives D_oe in on the opposite parity; returns |tmp|^2 + m^2 |in|^2
+  static double ddagd(FlaT<T> *f, double mass, c2<T> *out, const c2<T> *in, int eo,
+                      c2<T> *tmp, bool want_norm);
+};
+
+// link construction (links.cu)
+template <typename T> void double_store(FlaT<T> *f);
+template <typename T> FlaT<T> *fla_from_fwd(const c2<T> *fat, const c2<T> *lng);   // fields [4][2][9][Vh], unscaled
+template <typename TD, typename TS> FlaT<TD> *fla_convert(FlaT<TS> *src);
+template <typename T> void fla_destroy(FlaT<T> *f);
+
+void log0(int level, const char *fmt, ...);
+double wtime();
+
+}  // namespace qopb

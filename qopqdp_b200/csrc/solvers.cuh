@@ -1,0 +1,41 @@
+// solvers.cuh -- Krylov solvers and inverter drivers (solvers.cu, mixed.cu).
+#pragma once
+#include "qopb.h"
+
+namespace qopb {
+
+// A = m^2 - D_eo,oe D_oe,eo on parity eo (QOP_asqtad_invert_d2 / _d2_norm2,
+// lib/asqtad_invert_p.c:102-114)
+template <typename T> struct LinOp {
+  FlaT<T> *f;
+  double mass;
+  int eo;
+  c2<T> *tmp;   // full-volume scratch; its opposite-parity half holds D_oe in
+  void d2(c2<T> *out, const c2<T> *in) { Dslash<T>::ddagd(f, mass, out, in, eo, tmp, false); }
+  double d2n(c2<T> *out, const c2<T> *in) { return Dslash<T>::ddagd(f, mass, out, in, eo, tmp, true); }
+};
+
+template <typename T>
+void cg(LinOp<T> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t *ra, c2<T> *out, const c2<T> *in, c2<T> *p, int eo);
+template <typename T>
+void cgms(LinOp<T> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t **ra, const double *shifts, int ns, c2<T> **out,
+          const c2<T> *in, c2<T> *p, int eo);
+
+template <typename T>
+void invert(QOP_info_t *info, FlaT<T> *f, QOP_invert_arg_t *ia, QOP_resid_arg_t *ra, double mass, c2<T> *out,
+            const c2<T> *in);
+template <typename T>
+void solve_multi(QOP_info_t *info, FlaT<T> *f, QOP_invert_arg_t *ia, QOP_resid_arg_t **ra, const double *masses,
+                 c2<T> **out, c2<T> **in, int nsolve);
+template <typename T>
+void invert_multi(QOP_info_t *info, FlaT<T> *f, QOP_invert_arg_t *ia, QOP_resid_arg_t **ra[], double *masses[],
+                  int nmass[], c2<T> **out[], c2<T> *in[], int nsrc);
+
+// B200 mixed-precision inner solve (mixed.cu): multi-shift CG on A + shift_i
+// with the Krylov iteration in reduced precision (FP32 or FP16 storage with
+// FP32 arithmetic) and FP64 reliable updates of the true residual of the
+// base system.  Returns false when the path is not applicable.
+bool mixed_cgms(LinOp<double> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t **ra, const double *shifts, int ns,
+                c2<double> **out, const c2<double> *in, int eo, int prec);
+
+}  // namespace qopb

@@ -1,0 +1,380 @@
+"""ctypes mirror of the QOP C interface exported by libqop_b200.so.
+
+The structs below are the reference's include/qop_int.h structs, member for
+member.  `Qop(prec)` binds the F3 ('F', float32) or D3 ('D', float64) entry
+points and accepts numpy arrays in the reference raw layout:
+
+    vector : float array of shape (V, 3, 2)      (QLA_ColorVector per site)
+    links  : 4 float arrays of shape (V, 3, 3, 2) (QLA_ColorMatrix per site)
+
+in raw site order (even sites first, lib/layout_user.c:237-258).  The
+library is loaded from the package directory; there is no fallback.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libqop_b200.so")
+
+QOP_SUCCESS, QOP_FAIL, QOP_BC_ERROR, QOP_MEM_ERROR = 0, 1, 2, 3
+QOP_EVEN, QOP_ODD, QOP_EVENODD = 0, 1, 2
+QOP_UNITARIZE_U3, QOP_UNITARIZE_SU3 = 0, 1
+QOP_UNITARIZE_NONE, QOP_UNITARIZE_RATIONAL, QOP_UNITARIZE_ANALYTIC = 0, 3, 5
+QOP_MAX_NAIK = 20
+
+
+class QOP_layout_t(C.Structure):
+    _fields_ = [("node_number", C.c_void_p), ("node_index", C.c_void_p), ("latdim", C.c_int),
+                ("latsize", C.POINTER(C.c_int)), ("machdim", C.c_int), ("machsize", C.POINTER(C.c_int)),
+                ("this_node", C.c_int), ("sites_on_node", C.c_int)]
+
+
+class QOP_Complex(C.Structure):
+    _fields_ = [("re", C.c_double), ("im", C.c_double)]
+
+
+class QOP_bc_t(C.Structure):
+    _fields_ = [("phase", C.POINTER(QOP_Complex))]
+
+
+class QOP_staggered_sign_t(C.Structure):
+    _fields_ = [("signmask", C.POINTER(C.c_int))]
+
+
+class QOP_opt_t(C.Structure):
+    _fields_ = [("tag", C.c_char_p), ("value", C.c_double), ("extra", C.c_void_p)]
+
+
+class QOP_info_t(C.Structure):
+    _fields_ = [("final_sec", C.c_double), ("final_flop", C.c_double), ("status", C.c_int),
+                ("count1", C.c_int), ("count2", C.c_int)]
+
+
+class QOP_invert_arg_t(C.Structure):
+    _fields_ = [("mixed_rsq", C.c_double), ("max_iter", C.c_int), ("restart", C.c_int),
+                ("max_restarts", C.c_int), ("evenodd", C.c_int)]
+
+    @classmethod
+    def default(cls):
+        # QOP_INVERT_ARG_DEFAULT (include/qop_int.h:126)
+        return cls(1e9, 2000, 1000, 5, QOP_EVENODD)
+
+
+class QOP_resid_arg_t(C.Structure):
+    _fields_ = [("rsqmin", C.c_double), ("final_rsq", C.c_double), ("relmin", C.c_double),
+                ("final_rel", C.c_double), ("final_iter", C.c_int), ("final_restart", C.c_int)]
+
+    @classmethod
+    def default(cls):
+        # QOP_RESID_ARG_DEFAULT (include/qop_int.h:137)
+        return cls(1e-6, 0, 0, 0, 0, 0)
+
+
+class QOP_asqtad_coeffs_t(C.Structure):
+    _fields_ = [(n, C.c_double) for n in
+                ("one_link", "three_staple", "five_staple", "seven_staple", "lepage", "naik")]
+
+
+class QOP_hisq_coeffs_t(C.Structure):
+    _fields_ = [("n_naiks", C.c_int), ("eps_naik", C.c_double * QOP_MAX_NAIK), ("ugroup", C.c_int),
+                ("umethod", C.c_int)] + [(n, C.c_double) for n in (
+                    "fat7_one_link", "fat7_three_staple", "fat7_five_staple", "fat7_seven_staple", "fat7_lepage",
+                    "asqtad_one_link", "asqtad_three_staple", "asqtad_five_staple", "asqtad_seven_staple",
+                    "asqtad_lepage", "asqtad_naik", "difference_one_link", "difference_naik")]
+
+
+_lib = None
+
+
+def load_library(path=None):
+    """Load libqop_b200.so once; raises if it is missing (no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = path or LIB_PATH
+    if not os.path.exists(path):
+        raise RuntimeError("libqop_b200.so not built (%s); run python -m qopqdp_b200.build" % path)
+    lib = C.CDLL(path)
+    vp, ip = C.c_void_p, C.c_int
+    lib.QOP_init.argtypes = [C.POINTER(QOP_layout_t)]
+    lib.QOP_init.restype = ip
+    lib.QOP_finalize.restype = ip
+    lib.QOP_is_initialized.restype = ip
+    lib.QOP_version_str.restype = C.c_char_p
+    lib.QOP_version_int.restype = ip
+    lib.QOP_verbose.argtypes = [ip]
+    lib.QOP_verbose.restype = ip
+    lib.QOP_node_index_raw_V.argtypes = [C.POINTER(C.c_int), ip]
+    lib.QOP_node_index_raw_V.restype = ip
+    lib.QOP_sites_on_node_raw_V.argtypes = [ip]
+    lib.QOP_sites_on_node_raw_V.restype = ip
+    for f in ("QOP_asqtad_invert_set_opts", "QOP_hisq_links_set_opts", "QOP_hisq_invert_set_opts"):
+        getattr(lib, f).argtypes = [C.POINTER(QOP_opt_t), ip]
+        getattr(lib, f).restype = ip
+    for pc, real in (("F3", C.c_float), ("D3", C.c_double)):
+        rp = C.POINTER(real)
+        rpp = C.POINTER(rp)
+        info = C.POINTER(QOP_info_t)
+
+        def sig(name, args, res=None):
+            fn = getattr(lib, "QOP_%s_%s" % (pc, name))
+            fn.argtypes = args
+            fn.restype = res
+
+        sig("create_V_from_raw", [rp, ip], vp)
+        sig("extract_V_to_raw", [rp, vp, ip])
+        sig("destroy_V", [vp])
+        sig("create_G_from_raw", [rpp, ip], vp)
+        sig("extract_G_to_raw", [rpp, vp, ip])
+        sig("destroy_G", [vp])
+        sig("rephase_G", [vp, C.POINTER(C.c_int), C.POINTER(QOP_bc_t), C.POINTER(QOP_staggered_sign_t)])
+        sig("asqtad_create_L_from_raw", [rpp, rpp, ip], vp)
+        sig("asqtad_create_L_from_G", [info, C.POINTER(QOP_asqtad_coeffs_t), vp], vp)
+        sig("asqtad_create_L_from_G2", [info, C.POINTER(QOP_asqtad_coeffs_t), vp, vp], vp)
+        sig("asqtad_load_L_from_raw", [vp, rpp, rpp, ip])
+        sig("asqtad_extract_L_to_raw", [rpp, rpp, vp, ip])
+        sig("asqtad_destroy_L", [vp])
+        sig("asqtad_rephase_L", [vp, C.POINTER(C.c_int), C.POINTER(QOP_bc_t), C.POINTER(QOP_staggered_sign_t)])
+        sig("asqtad_dslash", [info, vp, real, vp, vp, ip, ip])
+        sig("asqtad_dslash_dir", [info, vp, ip, ip, C.c_double, C.c_double, vp, vp, ip])
+        sig("asqtad_diaginv", [info, vp, real, vp, vp, ip])
+        sig("asqtad_ddagd", [info, vp, real, vp, vp, ip])
+        sig("asqtad_ddagd_norm2", [info, vp, real, vp, vp, ip], real)
+        sig("asqtad_invert", [info, vp, C.POINTER(QOP_invert_arg_t), C.POINTER(QOP_resid_arg_t), real, vp, vp])
+        sig("asqtad_invert_multi", [info, vp, C.POINTER(QOP_invert_arg_t),
+                                    C.POINTER(C.POINTER(C.POINTER(QOP_resid_arg_t))), C.POINTER(rp),
+                                    C.POINTER(C.c_int), C.POINTER(C.POINTER(vp)), C.POINTER(vp), ip])
+        sig("hisq_create_L_from_G", [info, C.POINTER(QOP_hisq_coeffs_t), vp], vp)
+        sig("hisq_destroy_L", [vp])
+        sig("get_asqtad_links_from_hisq", [vp], C.POINTER(vp))
+        sig("get_asqtad_deps_links_from_hisq", [vp], vp)
+    lib.QOP_FD3_asqtad_create_L_from_L.argtypes = [vp]
+    lib.QOP_FD3_asqtad_create_L_from_L.restype = vp
+    _lib = lib
+    return lib
+
+
+def exported_symbols(header=None):
+    """Function names declared in include/qop.h (and qop_b200.h)."""
+    import re
+    root = os.path.dirname(_HERE)
+    names = []
+    for h in ("qop.h", "qop_b200.h"):
+        p = os.path.join(root, "include", h)
+        if not os.path.exists(p):
+            continue
+        txt = open(p).read()
+        if h == "qop.h":
+            body = txt.split("QOPB_DECLARE_PC(PC, REAL)")[1].split("QOPB_DECLARE_PC(F3")[0]
+            pcs = re.findall(r"QOP_##PC##_(\w+)\(", body)
+            for pc in ("F3", "D3"):
+                names += ["QOP_%s_%s" % (pc, n) for n in pcs]
+            txt = txt.replace(body, "")
+        names += re.findall(r"^\s*[\w\s\*]+?\b(QOPB?_\w+)\s*\(", txt, re.M)
+    return sorted(set(n for n in names if not n.startswith("QOPB_DECLARE") and n != "QOPB_GEN"))
+
+
+def _c_opts(opts):
+    arr = (QOP_opt_t * len(opts))()
+    keep = []
+    for i, (k, v) in enumerate(opts.items()):
+        b = k.encode()
+        keep.append(b)
+        arr[i].tag = b
+        arr[i].value = float(v)
+    return arr, keep
+
+
+class Qop:
+    """Bindings for one precision: prec 'F' (QOP_F3_*) or 'D' (QOP_D3_*)."""
+
+    def __init__(self, prec="D"):
+        self.lib = load_library()
+        self.prec = prec
+        self.pc = "F3" if prec == "F" else "D3"
+        self.real = C.c_float if prec == "F" else C.c_double
+        self.dtype = np.float32 if prec == "F" else np.float64
+
+    def f(self, name):
+        return getattr(self.lib, "QOP_%s_%s" % (self.pc, name))
+
+    # ------------------------------------------------------------ library
+    def init(self, L):
+        ls = (C.c_int * 4)(*L)
+        lay = QOP_layout_t()
+        lay.latdim = 4
+        lay.latsize = ls
+        lay.machdim = -1
+        st = self.lib.QOP_init(C.byref(lay))
+        return st
+
+    def finalize(self):
+        return self.lib.QOP_finalize()
+
+    def set_opts(self, **opts):
+        arr, _keep = _c_opts(opts)
+        return self.lib.QOP_asqtad_invert_set_opts(arr, len(opts))
+
+    def set_hisq_opts(self, **opts):
+        arr, _keep = _c_opts(opts)
+        return self.lib.QOP_hisq_links_set_opts(arr, len(opts))
+
+    # ------------------------------------------------------------ arrays
+    def _arr(self, a):
+        a = np.ascontiguousarray(a, dtype=self.dtype)
+        return a, a.ctypes.data_as(C.POINTER(self.real))
+
+    def _arr4(self, links):
+        keep, ptrs = [], (C.POINTER(self.real) * 4)()
+        for i in range(4):
+            a, p = self._arr(links[i])
+            keep.append(a)
+            ptrs[i] = p
+        return keep, ptrs
+
+    # ------------------------------------------------------------ fields
+    def create_V(self, raw, eo=QOP_EVENODD):
+        a, p = self._arr(raw)
+        h = self.f("create_V_from_raw")(p, eo)
+        if not h:
+            raise RuntimeError("create_V_from_raw failed")
+        return h
+
+    def extract_V(self, h, V, eo=QOP_EVENODD, into=None):
+        out = into if into is not None else np.zeros((V, 3, 2), dtype=self.dtype)
+        assert out.dtype == self.dtype and out.flags.c_contiguous
+        self.f("extract_V_to_raw")(out.ctypes.data_as(C.POINTER(self.real)), h, eo)
+        return out
+
+    def destroy_V(self, h):
+        self.f("destroy_V")(h)
+
+    def create_G(self, links, eo=QOP_EVENODD):
+        keep, ptrs = self._arr4(links)
+        h = self.f("create_G_from_raw")(ptrs, eo)
+        if not h:
+            raise RuntimeError("create_G_from_raw failed")
+        return h
+
+    def extract_G(self, h, V, eo=QOP_EVENODD):
+        outs = [np.zeros((V, 3, 3, 2), dtype=self.dtype) for _ in range(4)]
+        ptrs = (C.POINTER(self.real) * 4)(*[o.ctypes.data_as(C.POINTER(self.real)) for o in outs])
+        self.f("extract_G_to_raw")(ptrs, h, eo)
+        return outs
+
+    def destroy_G(self, h):
+        self.f("destroy_G")(h)
+
+    @staticmethod
+    def _phases(r0, bc, signmask):
+        r0c = (C.c_int * 4)(*r0)
+        ph = (QOP_Complex * 4)(*[QOP_Complex(complex(z).real, complex(z).imag) for z in bc])
+        bct = QOP_bc_t(ph)
+        sm = (C.c_int * 4)(*signmask)
+        sgn = QOP_staggered_sign_t(sm)
+        return r0c, ph, bct, sm, sgn
+
+    def rephase_G(self, h, r0=(0, 0, 0, 0), bc=(1, 1, 1, -1), signmask=(0, 1, 3, 7)):
+        r0c, ph, bct, sm, sgn = self._phases(r0, bc, signmask)
+        self.f("rephase_G")(h, r0c, C.byref(bct), C.byref(sgn))
+
+    # ------------------------------------------------------------ links
+    def create_L_from_raw(self, fat, lng, eo=QOP_EVENODD):
+        kf, pf = self._arr4(fat)
+        if lng is not None:
+            kl, pl = self._arr4(lng)
+        else:
+            pl = None
+        h = self.f("asqtad_create_L_from_raw")(pf, pl, eo)
+        if not h:
+            raise RuntimeError("asqtad_create_L_from_raw failed")
+        return h
+
+    def create_L_from_G(self, coeffs, gauge, info=None):
+        info = info or QOP_info_t()
+        c = QOP_asqtad_coeffs_t(*coeffs)
+        h = self.f("asqtad_create_L_from_G")(C.byref(info), C.byref(c), gauge)
+        if not h:
+            raise RuntimeError("asqtad_create_L_from_G failed (status %d)" % info.status)
+        return h
+
+    def extract_L(self, h, V, naik=True, eo=QOP_EVENODD):
+        fat = [np.zeros((V, 3, 3, 2), dtype=self.dtype) for _ in range(4)]
+        lng = [np.zeros((V, 3, 3, 2), dtype=self.dtype) for _ in range(4)] if naik else None
+        pf = (C.POINTER(self.real) * 4)(*[o.ctypes.data_as(C.POINTER(self.real)) for o in fat])
+        pl = (C.POINTER(self.real) * 4)(*[o.ctypes.data_as(C.POINTER(self.real)) for o in lng]) if naik else None
+        self.f("asqtad_extract_L_to_raw")(pf, pl, h, eo)
+        return fat, lng
+
+    def load_L_from_raw(self, h, fat, lng, eo=QOP_EVENODD):
+        kf, pf = self._arr4(fat)
+        pl = self._arr4(lng)[1] if lng is not None else None
+        self.f("asqtad_load_L_from_raw")(h, pf, pl, eo)
+
+    def destroy_L(self, h):
+        self.f("asqtad_destroy_L")(h)
+
+    def rephase_L(self, h, r0=(0, 0, 0, 0), bc=(1, 1, 1, -1), signmask=(0, 1, 3, 7)):
+        r0c, ph, bct, sm, sgn = self._phases(r0, bc, signmask)
+        self.f("asqtad_rephase_L")(h, r0c, C.byref(bct), C.byref(sgn))
+
+    def hisq_create_L_from_G(self, hc, gauge, info=None):
+        info = info or QOP_info_t()
+        h = self.f("hisq_create_L_from_G")(C.byref(info), C.byref(hc), gauge)
+        if not h:
+            raise RuntimeError("hisq_create_L_from_G failed (status %d)" % info.status)
+        return h
+
+    def hisq_asqtad_links(self, hh, k=0):
+        return self.f("get_asqtad_links_from_hisq")(hh)[k]
+
+    def hisq_destroy_L(self, hh):
+        self.f("hisq_destroy_L")(hh)
+
+    # ------------------------------------------------------------ operators
+    def dslash(self, fla, mass, out, inp, eo_out, eo_in, info=None):
+        info = info or QOP_info_t()
+        self.f("asqtad_dslash")(C.byref(info), fla, self.real(mass), out, inp, eo_out, eo_in)
+        return info
+
+    def dslash_dir(self, fla, mu, fb, wtfat, wtlong, out, inp, eo_out, info=None):
+        info = info or QOP_info_t()
+        self.f("asqtad_dslash_dir")(C.byref(info), fla, mu, fb, wtfat, wtlong, out, inp, eo_out)
+        return info
+
+    def diaginv(self, fla, mass, out, inp, eo, info=None):
+        info = info or QOP_info_t()
+        self.f("asqtad_diaginv")(C.byref(info), fla, self.real(mass), out, inp, eo)
+        return info
+
+    def ddagd(self, fla, mass, out, inp, eo, info=None):
+        info = info or QOP_info_t()
+        self.f("asqtad_ddagd")(C.byref(info), fla, self.real(mass), out, inp, eo)
+        return info
+
+    def ddagd_norm2(self, fla, mass, out, inp, eo, info=None):
+        info = info or QOP_info_t()
+        return self.f("asqtad_ddagd_norm2")(C.byref(info), fla, self.real(mass), out, inp, eo)
+
+    def invert(self, fla, mass, out, inp, inv_arg, res_arg, info=None):
+        info = info or QOP_info_t()
+        self.f("asqtad_invert")(C.byref(info), fla, C.byref(inv_arg), C.byref(res_arg), self.real(mass), out, inp)
+        return info
+
+    def invert_multi(self, fla, masses, outs, ins, inv_arg, res_args, info=None):
+        """masses[s][j], outs[s][j] (handles), ins[s] (handles), res_args[s][j]."""
+        info = info or QOP_info_t()
+        nsrc = len(ins)
+        RA = C.POINTER(QOP_resid_arg_t)
+        ra_rows = [(RA * len(r))(*[C.pointer(x) for x in r]) for r in res_args]
+        ra = (C.POINTER(RA) * nsrc)(*[C.cast(r, C.POINTER(RA)) for r in ra_rows])
+        m_rows = [(self.real * len(m))(*m) for m in masses]
+        mp = (C.POINTER(self.real) * nsrc)(*[C.cast(m, C.POINTER(self.real)) for m in m_rows])
+        nm = (C.c_int * nsrc)(*[len(m) for m in masses])
+        o_rows = [(C.c_void_p * len(o))(*o) for o in outs]
+        op = (C.POINTER(C.c_void_p) * nsrc)(*[C.cast(o, C.POINTER(C.c_void_p)) for o in o_rows])
+        ip_ = (C.c_void_p * nsrc)(*ins)
+        self.f("asqtad_invert_multi")(C.byref(info), fla, C.byref(inv_arg), ra, mp, nm, op, ip_, nsrc)
+        return info

@@ -1,0 +1,157 @@
+"""CPU tests of the oracle (no GPU).
+
+The reference ships no golden vectors and cannot be built here (it needs the
+external QDP/C, QLA and QMP libraries), so the oracle is pinned to the
+reference's own tests and to the identities the algorithm guarantees:
+  * examples/asqtad_test.c:37-81 check_op: Dslash rebuilt from the unscaled
+    links with plain shifts agrees to <= 1e-10 (squared, relative);
+  * examples/asqtad_test.c:84-130 check_resids: the eo solve's true residual
+    |in - (1/m)(m^2 - D D) out|^2/|in|^2 meets rsqmin;
+  * layout (lib/layout_user.c:237-258), rephase (lib/common_p.c:455-526),
+    U(3) projection (W^+W = 1), gauge covariance, anti-hermiticity of the hop.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from helpers import gauge, asqtad_links, hisq_links, eo_residual, full_residual, half
+from qopqdp_b200 import lattice as LT
+
+LATTICES = [(4, 4, 4, 4), (4, 4, 4, 8), (6, 4, 4, 4)]
+
+
+@pytest.mark.parametrize("L", LATTICES)
+def test_raw_index_matches_layout_formula(L):
+    lat = O.Lattice(L)
+    xs = LT.raw_coords(L)
+    V = int(np.prod(L))
+    assert sorted(LT.raw_index(L, xs)) == list(range(V))
+    import ctypes as C
+    for idx in (0, 1, V // 2 - 1, V // 2, V - 1):
+        x = (C.c_int * 4)(*[int(v) for v in xs[idx]])
+        assert O.lib().or_raw_index(lat.h, x) == idx
+    # even sites first
+    assert (xs[: V // 2].sum(axis=1) % 2 == 0).all() and (xs[V // 2:].sum(axis=1) % 2 == 1).all()
+
+
+@pytest.mark.parametrize("L", LATTICES)
+@pytest.mark.parametrize("naik", [True, False])
+def test_check_op_identity(L, naik):
+    fat, lng = asqtad_links(L, 0.3, 7, naik)
+    fo = O.Fla(O.Lattice(L), fat, lng)
+    src = LT.gaussian_vector(L, 1)
+    for m in (0.1, 0.0):
+        d2 = fo.check_op(m, src)
+        assert d2 <= 1e-28, d2          # the reference test demands <= 1e-10
+
+
+def test_check_op_hisq():
+    L = (4, 4, 4, 8)
+    fat, lng, W, _ = hisq_links(L, 0.5, 9)
+    fo = O.Fla(O.Lattice(L), fat, lng)
+    assert fo.check_op(0.05, LT.gaussian_vector(L, 2)) <= 1e-28
+    # the analytic projection (hisq_reunit_utilities_p.c:99-297) loses a few
+    # digits where fat7 links have nearly degenerate V^+V eigenvalues
+    for mu in range(4):
+        w = LT.to_complex(W[mu])
+        assert np.abs(np.einsum("vij,vkj->vik", w, w.conj()) - np.eye(3)).max() < 1e-9
+
+
+def test_u3_projection_fixes_unitary_and_polar_factor():
+    rng = np.random.default_rng(0)
+    import ctypes as C
+    for _ in range(20):
+        a = rng.standard_normal((3, 3)) + 1j * rng.standard_normal((3, 3))
+        Vr = LT.from_complex(a).ravel()
+        Wr = np.zeros(18)
+        O.lib().or_u3_un_analytic(O._p(Vr), O._p(Wr), 1, 1e-8, 1e-8)
+        W = LT.to_complex(Wr.reshape(3, 3, 2))
+        u, s, vh = np.linalg.svd(a)
+        assert np.abs(W - u @ vh).max() < 1e-10        # polar factor V (V^+V)^-1/2
+        Wr2 = np.zeros(18)
+        O.lib().or_u3_un_analytic(O._p(LT.from_complex(W).ravel()), O._p(Wr2), 1, 1e-8, 1e-8)
+        assert np.abs(LT.to_complex(Wr2.reshape(3, 3, 2)) - W).max() < 1e-12
+    # near-singular input takes the eigen-decomposition fallback
+    a = rng.standard_normal((3, 3)) + 1j * rng.standard_normal((3, 3))
+    a[2] = a[0] * (1 + 1e-9)
+    Wr = np.zeros(18)
+    assert O.lib().or_u3_un_analytic(O._p(LT.from_complex(a).ravel()), O._p(Wr), 1, 1e-8, 1e-8) == 1
+
+
+def test_rephase_G_signs_and_boundary():
+    L = (4, 4, 4, 8)
+    U = LT.random_gauge(L, 0.3, 3)
+    R = O.Lattice(L).rephase_G(U, (0, 0, 0, 0), (1, 1, 1, -1), (0, 1, 3, 7))
+    xs = LT.raw_coords(L)
+    for mu, mask in enumerate((0, 1, 3, 7)):
+        s = np.zeros(len(xs), dtype=np.int64)
+        for j in range(4):
+            if (mask >> j) & 1:
+                s += xs[:, j]
+        f = np.where(s % 2 == 1, -1.0, 1.0)
+        if mu == 3:
+            f = f * np.where(xs[:, 3] == L[3] - 1, -1.0, 1.0)
+        np.testing.assert_array_equal(R[mu], U[mu] * f[:, None, None, None])
+
+
+def test_hop_is_antihermitian_and_gauge_covariant():
+    L = (4, 4, 4, 4)
+    fat, lng = asqtad_links(L, 0.3, 7)
+    fo = O.Fla(O.Lattice(L), fat, lng)
+    x = LT.to_complex(LT.gaussian_vector(L, 5))
+    y = LT.to_complex(LT.gaussian_vector(L, 6))
+    Dy = LT.to_complex(fo.dslash(0.0, LT.from_complex(y), 2, 2))
+    Dx = LT.to_complex(fo.dslash(0.0, LT.from_complex(x), 2, 2))
+    lhs = np.vdot(x, Dy)
+    rhs = -np.vdot(Dx, y)
+    assert abs(lhs - rhs) <= 1e-12 * abs(lhs)
+    # gauge covariance: U -> g(x) U g(x+mu)^+ on the base links, psi -> g psi
+    Ug = [LT.to_complex(u) for u in gauge(L, 0.3, 7)]
+    gx = LT.to_complex(LT.random_gauge(L, 1.0, 99)[0])
+    xs = LT.raw_coords(L)
+    Ut = []
+    for mu in range(4):
+        y_ = xs.copy()
+        y_[:, mu] = (y_[:, mu] + 1) % L[mu]
+        nb = LT.raw_index(L, y_)
+        Ut.append(LT.from_complex(np.einsum("vij,vjk,vlk->vil", gx, Ug[mu], gx[nb].conj())))
+    lat = O.Lattice(L)
+    f2, l2 = lat.make_imp_links(LT.ASQTAD_BENCH_COEFFS, Ut)
+    fo2 = O.Fla(lat, f2, l2)
+    psi = LT.to_complex(LT.gaussian_vector(L, 8))
+    a = LT.to_complex(fo2.dslash(0.1, LT.from_complex(np.einsum("vij,vj->vi", gx, psi)), 2, 2))
+    b = np.einsum("vij,vj->vi", gx, LT.to_complex(fo.dslash(0.1, LT.from_complex(psi), 2, 2)))
+    assert np.abs(a - b).max() <= 1e-12 * np.abs(b).max()
+
+
+@pytest.mark.parametrize("eo", [0, 1])
+def test_check_resids_eo_solve(eo):
+    L = (4, 4, 4, 8)
+    fat, lng = asqtad_links(L, 0.3, 7)
+    fo = O.Fla(O.Lattice(L), fat, lng)
+    src = LT.gaussian_vector(L, 20)
+    ia, ra = O.InvertArg(1e9, 2000, 1000, 5, eo), O.ResidArg(1e-20, 0, 0, 0, 0, 0)
+    out, flop = fo.invert(0.1, src, ia, ra)
+    true = eo_residual(fo, 0.1, out, src, L, eo)
+    assert true <= 1e-20 * 1.01 and abs(true - ra.final_rsq) <= 1e-3 * true
+    assert not half(out, L, 1 - eo).any()
+    # restarting from the solution needs (almost) no iterations
+    ra2 = O.ResidArg(1e-20, 0, 0, 0, 0, 0)
+    fo.invert(0.1, src, O.InvertArg(1e9, 2000, 1000, 5, eo), ra2, out=out)
+    assert ra2.final_iter <= 2
+    assert flop == 0.5 * (60 + 2 * 8 * 9 * 16) * ra.final_iter * int(np.prod(L))
+
+
+def test_evenodd_solve_and_multimass():
+    L = (4, 4, 4, 8)
+    fat, lng, _, _ = hisq_links(L, 0.5, 9)
+    fo = O.Fla(O.Lattice(L), fat, lng)
+    src = LT.gaussian_vector(L, 21)
+    ra = O.ResidArg(1e-18, 0, 0, 0, 0, 0)
+    out, _ = fo.invert(0.05, src, O.InvertArg(1e9, 2000, 1000, 5, 2), ra)
+    assert full_residual(fo, 0.05, out, src) <= 1e-18 * 1.01
+    ms = [0.02, 0.05, 0.2]
+    ras = [[O.ResidArg(1e-18, 0, 0, 0, 0, 0) for _ in ms]]
+    outs, _ = fo.invert_multi([ms], [src], O.InvertArg(1e9, 8000, 1000, 20, 0), ras)
+    for j, m in enumerate(ms):
+        assert eo_residual(fo, m, outs[0][j], src, L, 0) <= 1e-18 * 1.05
