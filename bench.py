@@ -1,0 +1,403 @@
+#!/usr/bin/env python
+"""Benchmark of the asqtad/HISQ eo-preconditioned solve on one B200 (or N
+independent replicas).
+
+Workload (one "step" = one solve): HISQ links built on the device from a
+seeded gauge field U = exp(i 0.5 H) on a 32^3 x 64 lattice (t antiperiodic,
+staggered signs), mass 0.01, one Gaussian source on even sites, solved with
+QOP_D3_asqtad_invert (evenodd = EVEN) to |b - A x| / |b| <= 1e-10
+(rsqmin = 1e-20), using the mixed-precision reliable-update solver
+(FP16 storage, FP32 arithmetic, FP64 reliable updates).
+
+Reported: solves/s (device-resident inputs, CUDA events on the library
+stream, max over ranks), e2e solves/s through the C ABI from pinned host
+buffers, p50/p99 latency, the same solve with plain FP64 CG, Dslash GB/s
+and the roofline of the dominant kernel, and the oracle's CPU time.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+"""
+import argparse
+import json
+import os
+import re
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PEAK_FALLBACK_GBS = 6650.0
+BENCH_ITERS_FILE = os.path.join(ROOT, "profiles", "bench_iterations.json")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--lattice", default="32,32,32,64")
+    ap.add_argument("--mass", type=float, default=0.01)
+    ap.add_argument("--tol", type=float, default=1e-10, help="|r|/|b| target")
+    ap.add_argument("--eps", type=float, default=0.5)
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--prec", type=int, default=16, choices=[16, 32, 64], help="sloppy precision")
+    ap.add_argument("--fp64-steps", type=int, default=1)
+    ap.add_argument("--cpu-iters", type=int, default=12, help="CG iterations timed on the host")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--quick", action="store_true", help="skip FP64 baseline and e2e (development)")
+    return ap.parse_args()
+
+
+def rank_info():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)),
+            int(os.environ.get("WORLD_SIZE", 1)))
+
+
+def workload_name(a, L):
+    return "hisq_%s_m%g_tol%g_eps%g_seed%d" % ("x".join(map(str, L)), a.mass, a.tol, a.eps, a.seed)
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return PEAK_FALLBACK_GBS, "fallback"
+
+
+def ncu_traffic(kernel_class, L):
+    """DRAM bytes per launch from the committed ncu summary, if one exists."""
+    p = os.path.join(ROOT, "profiles", "ncu_%s_%s.md" % (kernel_class, "x".join(map(str, L))))
+    if not os.path.exists(p):
+        return None
+    m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", open(p).read())
+    return float(m.group(1)) if m else None
+
+
+class Clocks:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+
+    def __init__(self, gpu):
+        self.gpu, self.samples, self.stop, self.t = gpu, [], False, None
+
+    def _run(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        while not self.stop:
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + q,
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            time.sleep(0.2)
+
+    def __enter__(self):
+        self.t = threading.Thread(target=self._run, daemon=True)
+        self.t.start()
+        return self
+
+    def __exit__(self, *exc):
+        self.stop = True
+        self.t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if "Active" in s[3 + k]
+                          and not s[3 + k].startswith("Not")})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+# ---------------------------------------------------------------- reference arm
+def cpu_iteration_time(fat, lng, L, src, mass, iters, threads):
+    """Seconds per CG iteration of the oracle (the reference algorithm restated
+    in C, FP64, OpenMP) on the host cores: a bounded run of `iters`."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.set_threads(threads)
+    lat = O.Lattice(L)
+    fo = O.Fla(lat, fat, lng)
+    ia = O.InvertArg(1e9, iters, iters, 0, 0)
+    ra = O.ResidArg(1e-30, 0, 0, 0, 0, 0)
+    t0 = time.perf_counter()
+    fo.invert(mass, src, ia, ra)
+    dt = time.perf_counter() - t0
+    return dt / max(ra.final_iter, 1), ra.final_iter, O.get_threads()
+
+
+def run_reference(a):
+    rank, _, world = rank_info()
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from qopqdp_b200 import lattice as LT
+    L = tuple(int(x) for x in a.lattice.split(","))
+    threads = os.cpu_count() or 1
+    O.set_threads(threads)
+    U = LT.random_gauge(L, a.eps, a.seed, device="cpu")
+    lat = O.Lattice(L)
+    U = lat.rephase_G(U, LT.BENCH_R0, LT.BENCH_BC, LT.BENCH_SIGNMASK)
+    fat, lng, _, _ = lat.hisq_links(LT.hisq_coeff_vector(LT.hisq_bench_coeffs()), U)
+    del U
+    src = LT.gaussian_vector(L, a.seed)
+    iters_db = json.load(open(BENCH_ITERS_FILE)) if os.path.exists(BENCH_ITERS_FILE) else {}
+    key = workload_name(a, L)
+    n_solve = iters_db.get(key, {}).get("fp64_iters")
+    per = []
+    for k in range(a.warmup + a.steps):
+        s, it, th = cpu_iteration_time(fat, lng, L, src, a.mass, a.cpu_iters, threads)
+        if k >= a.warmup:
+            per.append(s)
+    s_it = float(np.median(per))
+    if n_solve:
+        value = 1.0 / (s_it * n_solve)
+        sample = ("%d CG iterations of the FP64 reference algorithm per step on %d host threads; solves/s "
+                  "extrapolated with the full solve's %d iterations (FP64 solve of this workload)" %
+                  (a.cpu_iters, th, n_solve))
+    else:
+        value = None
+        sample = "%d CG iterations per step; full-solve iteration count not recorded" % a.cpu_iters
+    line = {"metric": "mixed-prec CG solves/s @1e-10 (HISQ eo solve)", "value": value, "unit": "solves/s",
+            "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": 1e3 / value if value else None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": key, "lattice": L, "mass": a.mass, "tol": a.tol},
+            "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": th, "kind": "port", "sample": sample,
+                             "sec_per_iter": s_it},
+            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- device arm
+def run_b200(a):
+    rank, local, world = rank_info()
+    import torch
+    import ctypes as C
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    from qopqdp_b200 import lattice as LT
+    from qopqdp_b200.qop import (Qop, QOP_invert_arg_t, QOP_resid_arg_t, QOP_info_t, QOP_EVEN, load_library)
+    lib = load_library()
+    lib.QOPB_stream.restype = C.c_void_p
+
+    class KStat(C.Structure):
+        _fields_ = [("name", C.c_char * 32), ("launches", C.c_int), ("total_ms", C.c_double),
+                    ("bytes_per_launch", C.c_double)]
+
+    lib.QOPB_prof_end.argtypes = [C.POINTER(KStat), C.c_int]
+    lib.QOPB_launch_count.restype = C.c_ulonglong
+
+    def prof_end():
+        buf = (KStat * 32)()
+        n = lib.QOPB_prof_end(buf, 32)
+        return {buf[i].name.decode(): (buf[i].launches, buf[i].total_ms, buf[i].bytes_per_launch)
+                for i in range(min(n, 32))}
+
+    L = tuple(int(x) for x in a.lattice.split(","))
+    V = int(np.prod(L))
+    q = Qop("D")
+    assert q.init(L) == 0
+    t_setup = time.perf_counter()
+    U = LT.random_gauge(L, a.eps, a.seed, device="cuda")
+    G = q.create_G(U)
+    del U
+    q.rephase_G(G, LT.BENCH_R0, LT.BENCH_BC, LT.BENCH_SIGNMASK)
+    q.set_hisq_opts(want_aux=0)
+    info = QOP_info_t()
+    H = q.hisq_create_L_from_G(LT.hisq_bench_coeffs(), G, info)
+    q.destroy_G(G)
+    fla = q.hisq_asqtad_links(H, 0)
+    src = LT.gaussian_vector(L, a.seed)
+    t_setup = time.perf_counter() - t_setup
+    stream = torch.cuda.ExternalStream(lib.QOPB_stream())
+    rsq = a.tol * a.tol
+    big = 1 << 30
+
+    def solve(hout, hin, prec):
+        q.set_opts(prec_sloppy=prec)
+        q.dslash(fla, 0.0, hout, hout, QOP_EVEN, QOP_EVEN)          # zero initial guess
+        ia = QOP_invert_arg_t(1e9, 200000, 200000, 10, QOP_EVEN)
+        ra = QOP_resid_arg_t(rsq, 0, 0, 0, 0, 0)
+        inf = q.invert(fla, a.mass, hout, hin, ia, ra)
+        return ra, inf
+
+    def ev():
+        e = torch.cuda.Event(enable_timing=True)
+        e.record(stream)
+        return e
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    hin = q.create_V(src, QOP_EVEN)
+    hout = q.create_V(np.zeros_like(src))
+    for _ in range(a.warmup):
+        ra, _ = solve(hout, hin, a.prec)
+    # ---------------- timed region (device-resident inputs)
+    lat_ms, iters, rsqs = [], [], []
+    lib.QOPB_prof_begin()
+    barrier()
+    n_launch0 = lib.QOPB_launch_count()
+    with Clocks(local) as clk:
+        e0 = ev()
+        for _ in range(a.steps):
+            s0 = ev()
+            ra, _ = solve(hout, hin, a.prec)
+            s1 = ev()
+            s1.synchronize()
+            lat_ms.append(s0.elapsed_time(s1))
+            iters.append(ra.final_iter)
+            rsqs.append(ra.final_rsq)
+        e1 = ev()
+        barrier()
+    n_launch = lib.QOPB_launch_count() - n_launch0
+    kst = prof_end()
+    total_ms = max_over_ranks(e0.elapsed_time(e1))
+    value = a.steps * world / (total_ms / 1e3)
+    # independent FP64 check of the last solution's residual (not timed)
+    sol = q.extract_V(hout, V)
+    # ---------------- plain FP64 GPU CG (the reference algorithm in FP64)
+    fp64 = {}
+    if not a.quick and a.fp64_steps > 0:
+        t64, it64 = [], []
+        lib.QOPB_prof_begin()
+        for _ in range(a.fp64_steps):
+            s0 = ev()
+            r64, _ = solve(hout, hin, 64)
+            s1 = ev()
+            s1.synchronize()
+            t64.append(s0.elapsed_time(s1))
+            it64.append(r64.final_iter)
+        k64 = prof_end()
+        fp64 = {"solves_per_s": 1e3 / float(np.mean(t64)), "ms_per_solve": float(np.mean(t64)),
+                "iters": int(np.median(it64)), "final_rsq": r64.final_rsq}
+        h = k64.get("hop_f64")
+        if h and h[1] > 0:
+            fp64["hop_f64_gbs"] = h[0] * h[2] / (h[1] * 1e-3) / 1e9
+    # ---------------- e2e through the C ABI from pinned host buffers
+    e2e = None
+    if not a.quick:
+        src_pin = torch.empty(src.shape, dtype=torch.float64, pin_memory=True).numpy()
+        src_pin[...] = src
+        dst_pin = torch.empty(src.shape, dtype=torch.float64, pin_memory=True).numpy()
+        barrier()
+        e_ms = []
+        t0 = time.perf_counter()
+        for _ in range(a.steps):
+            s0 = ev()
+            h_in = q.create_V(src_pin, QOP_EVEN)                   # H2D: even half
+            solve(hout, h_in, a.prec)
+            q.extract_V(hout, V, QOP_EVEN, into=dst_pin)           # D2H: even half
+            q.destroy_V(h_in)
+            s1 = ev()
+            s1.synchronize()
+            e_ms.append(s0.elapsed_time(s1))
+        barrier()
+        e_tot = max_over_ranks(sum(e_ms))
+        half = (V // 2) * 3 * 2 * 8
+        e2e = {"value": a.steps * world / (e_tot / 1e3), "unit": "solves/s", "h2d_bytes_per_step": half,
+               "d2h_bytes_per_step": half, "wall_s": time.perf_counter() - t0}
+    # ---------------- roofline of the dominant kernel
+    peak, peak_kind = measured_peak()
+    dom = max(kst.items(), key=lambda kv: kv[1][1]) if kst else None
+    roof = None
+    kernels = {}
+    for name, (n, ms, b) in kst.items():
+        kernels[name] = {"launches": n, "total_ms": ms, "avg_us": 1e3 * ms / max(n, 1),
+                         "gbs": n * b / (ms * 1e-3) / 1e9 if ms > 0 else None, "bytes_per_launch": b}
+    if dom:
+        name, (n, ms, b) = dom
+        ach = n * b / (ms * 1e-3) / 1e9
+        roof = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                "peak_kind": peak_kind, "kernel": name, "traffic": ncu_traffic(name, L),
+                "bytes_per_launch": b}
+    # ---------------- CPU baseline (oracle) on rank 0, N = 1
+    cpu = None
+    n_fp64 = fp64.get("iters")
+    if rank == 0 and world == 1 and not a.no_cpu:
+        fat, lng = q.extract_L(fla, V)
+        threads = os.cpu_count() or 1
+        s_it, nit, th = cpu_iteration_time(fat, lng, L, src, a.mass, a.cpu_iters, threads)
+        n_ref = n_fp64 or int(np.median(iters))
+        cpu = {"value": 1.0 / (s_it * n_ref), "unit": "solves/s", "cores": th, "kind": "port",
+               "sample": "%d CG iterations of the oracle (FP64 reference algorithm, C/OpenMP) on %d host threads, "
+                         "%.3f s/iteration, extrapolated to the %d iterations of the FP64 solve" %
+                         (nit, th, s_it, n_ref), "sec_per_iter": s_it}
+        del fat, lng
+    if rank == 0:
+        if n_fp64:
+            os.makedirs(os.path.dirname(BENCH_ITERS_FILE), exist_ok=True)
+            db = json.load(open(BENCH_ITERS_FILE)) if os.path.exists(BENCH_ITERS_FILE) else {}
+            db[workload_name(a, L)] = {"fp64_iters": n_fp64, "mixed_iters": int(np.median(iters))}
+            try:
+                json.dump(db, open(BENCH_ITERS_FILE, "w"), indent=1, sort_keys=True)
+            except OSError:
+                pass
+        lat_sorted = np.sort(lat_ms)
+        line = {
+            "metric": "mixed-prec CG solves/s @1e-10 (HISQ eo solve)",
+            "value": value, "unit": "solves/s", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": total_ms / a.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f16" if a.prec == 16 else ("f32" if a.prec == 32 else "f64"),
+            "data": "synthetic",
+            "config": {"workload": workload_name(a, L), "lattice": L, "mass": a.mass, "tol": a.tol,
+                       "eps": a.eps, "precision": "FP%d storage / FP32 arith / FP64 reliable updates" % a.prec,
+                       "parallelism": "replicas x%d" % world,
+                       "l2": "inputs larger than L2 (links %.1f GB FP64)" % (V * 16 * 18 * 8 / 1e9)},
+            "p50_ms": float(np.percentile(lat_sorted, 50)), "p99_ms": float(np.percentile(lat_sorted, 99)),
+            "iters": int(np.median(iters)), "final_rsq": float(max(rsqs)),
+            "fp64_cg": fp64,
+            "speedup_vs_fp64": (value / world) / fp64["solves_per_s"] if fp64 else None,
+            "roofline": roof, "kernels": kernels, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": int(n_launch),
+            "clocks": clk.summary(), "setup_s": t_setup,
+        }
+        print(json.dumps(line), flush=True)
+    q.destroy_V(hin)
+    q.destroy_V(hout)
+    q.hisq_destroy_L(H)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_b200(a)
+
+
+if __name__ == "__main__":
+    main()

@@ -30,6 +30,9 @@ typedef struct {
 int QOPB_prof_begin(void);
 int QOPB_prof_end(QOPB_kstat_t *out, int max);
 
+/* Number of kernels the library has launched since it was loaded. */
+unsigned long long QOPB_launch_count(void);
+
 #ifdef __cplusplus
 }
 #endif

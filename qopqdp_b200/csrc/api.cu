@@ -111,6 +111,7 @@ template <typename T, typename R> void load_L_raw(FlaT<T> *f, R *fat[], R *lng[]
     if (dl) raw_to_dev<T, R>(dl + (i64)mu * 18 * g.Vh, lng[mu], 9, eo);
   }
   fla_load_fwd<T>(f, df, dl, 0.5);
+  sloppy_invalidate((void *)f);
   if (f->shadow32) { fla_destroy((FlaT<float> *)f->shadow32); f->shadow32 = nullptr; }
   dfree(df); if (dl) dfree(dl);
   sync();
@@ -263,6 +264,7 @@ template <typename T, typename R> void invert_multi_api(QOP_info_t *info, FlaT<T
                                               QOP_staggered_sign_t *sign) {                                       \
     TRY require_init(__func__); FlaT<T> *f = il<T>(fla); need_handle<T>(f, "FermionLinksAsqtad");                  \
     fla_rephase<T>(f, r0, bc ? bc->phase : nullptr, sign ? sign->signmask : nullptr);                               \
+    sloppy_invalidate((void *)f);                                                                                   \
     if (f->shadow32) { fla_destroy((FlaT<float> *)f->shadow32); f->shadow32 = nullptr; }                            \
     sync(); CATCHV(nullptr)                                                                                         \
   }                                                                                                                 \

@@ -18,6 +18,10 @@ void check_cuda(cudaError_t e, const char *what, const char *file, int line) {
   throw Fail(e == cudaErrorMemoryAllocation ? QOP_MEM_ERROR : QOP_FAIL, buf);
 }
 
+static unsigned long long g_launches = 0;
+void count_launches(int n) { g_launches += (unsigned long long)n; }
+unsigned long long launch_count() { return g_launches; }
+
 void fail(QOP_status_t s, const char *fmt, ...) {
   char buf[512];
   va_list ap;
@@ -54,7 +58,8 @@ void ensure_ready() {
   int sms = 0;
   QCHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device));
   c.red_blocks = sms * 8;
-  QCHECK(cudaMalloc(&c.d_part, sizeof(double) * 8 * c.red_blocks));
+  c.part_cap = (size_t)8 * c.red_blocks;
+  QCHECK(cudaMalloc(&c.d_part, sizeof(double) * c.part_cap));
   QCHECK(cudaMalloc(&c.d_count, sizeof(unsigned) * 4));
   QCHECK(cudaMemset(c.d_count, 0, sizeof(unsigned) * 4));
   QCHECK(cudaMalloc(&c.d_res, sizeof(double) * 64));
@@ -124,6 +129,14 @@ QOP_status_t QOP_init(QOP_layout_t *layout) {
   }
   OPT_TRY
   ensure_ready();
+  // fused reductions run one block per 64+ sites with up to 4 sums each
+  size_t need = (size_t)4 * (g.Vh / 64 + 64);
+  if (need > c.part_cap) {
+    QCHECK(cudaStreamSynchronize(c.s));
+    QCHECK(cudaFree(c.d_part));
+    QCHECK(cudaMalloc(&c.d_part, sizeof(double) * need));
+    c.part_cap = need;
+  }
   OPT_CATCH(QOP_FAIL)
   c.g = g;
   c.verbosity = 0;
@@ -141,6 +154,8 @@ QOP_status_t QOP_finalize(void) {
 }
 
 int QOP_is_initialized(void) { return ctx().inited; }
+
+unsigned long long QOPB_launch_count(void) { return launch_count(); }
 
 const char *QOP_version_str(void) { return "0.21.1-b200"; }
 int QOP_version_int(void) { return (0 * 1000 + 21) * 1000 + 1; }
@@ -198,6 +213,9 @@ QOP_status_t QOP_asqtad_invert_set_opts(QOP_opt_t opts[], int nopts) {
       int p = (int)v;
       if (p != 16 && p != 32 && p != 64) return QOP_FAIL;
       n.sloppy_prec = p;
+    } else if (!strcmp(t, "half_format")) {
+      if (v < 0 || v > 2) return QOP_FAIL;
+      n.half_format = (int)v;
     } else if (!strcmp(t, "ru_delta")) {
       if (!(v > 0 && v < 1)) return QOP_FAIL;
       n.ru_delta = v;

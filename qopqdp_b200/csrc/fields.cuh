@@ -26,5 +26,6 @@ template <typename T> HisqT<T> *hisq_from_G(QOP_info_t *info, const QOP_hisq_coe
 template <typename T> void hisq_destroy(HisqT<T> *h);
 template <typename T> FlaT<T> *fla_scaled_copy(FlaT<T> *src, double s);
 template <typename T> void fla_peq(FlaT<T> *f, FlaT<T> *g);
+void sloppy_invalidate(void *fla_any);   // drop reduced-precision copies (mixed.cu)
 
 }  // namespace qopb

@@ -443,8 +443,6 @@ void double_store(FlaT<T> *f) {
   QLAUNCH();
 }
 
-void sloppy_invalidate(void *fla_any);   // mixed.cu
-
 template <typename T>
 void fla_load_fwd(FlaT<T> *f, const c2<T> *fat, const c2<T> *lng, double scale) {
   const Geom &g = ctx().g;

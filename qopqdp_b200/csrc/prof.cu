@@ -55,6 +55,13 @@ void prof_stop(int idx) {
   cudaEventRecord(g_prof.recs[idx].b, ctx().s);
 }
 
+// the launch behind record idx did no work (e.g. it found a stop flag set):
+// keep it out of the per-class averages
+void prof_discard(int idx) {
+  if (idx < 0 || idx >= (int)g_prof.recs.size()) return;
+  g_prof.recs[idx].cls = -1;
+}
+
 bool prof_active() { return g_prof.active; }
 
 }  // namespace qopb
@@ -82,6 +89,11 @@ extern "C" int QOPB_prof_end(QOPB_kstat_t *out, int max) {
   if (ctx().s) cudaStreamSynchronize(ctx().s);
   for (auto &r : g_prof.recs) {
     float ms = 0;
+    if (r.cls < 0) {
+      g_prof.pool.push_back(r.a);
+      g_prof.pool.push_back(r.b);
+      continue;
+    }
     if (cudaEventElapsedTime(&ms, r.a, r.b) == cudaSuccess) {
       g_prof.cls[r.cls].ms += ms;
       g_prof.cls[r.cls].launches += 1;

@@ -5,6 +5,7 @@
 namespace qopb {
 int prof_start(const char *name, double bytes);   // -1 when inactive
 void prof_stop(int idx);
+void prof_discard(int idx);
 bool prof_active();
 
 struct ProfScope {

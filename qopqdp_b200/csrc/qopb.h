@@ -38,7 +38,11 @@ struct Fail {
 };
 void check_cuda(cudaError_t e, const char *what, const char *file, int line);
 #define QCHECK(x) ::qopb::check_cuda((x), #x, __FILE__, __LINE__)
-#define QLAUNCH() ::qopb::check_cuda(cudaGetLastError(), "kernel launch", __FILE__, __LINE__)
+// every kernel launch is followed by QLAUNCH (or QLAUNCHN for n launches),
+// which checks the launch and counts it (QOPB_launch_count)
+void count_launches(int n);
+#define QLAUNCHN(n) (::qopb::count_launches(n), ::qopb::check_cuda(cudaGetLastError(), "kernel launch", __FILE__, __LINE__))
+#define QLAUNCH() QLAUNCHN(1)
 [[noreturn]] void fail(QOP_status_t s, const char *fmt, ...);
 
 // ---------------------------------------------------------------- geometry
@@ -91,6 +95,7 @@ struct Options {
   // B200 additions: sloppy precision of the inner Krylov solve
   // (64 = exact reference algorithm in the handle's precision)
   int sloppy_prec = 64;
+  int half_format = 0;           // 16-bit storage: 0 int16 fixed point, 1 IEEE FP16, 2 FP16 links
   double ru_delta = 0.1;         // reliable-update threshold on |r|
   int chunk = 16;                // iterations launched per host check
   // QOP_hisq_links_set_opts (lib/hisq_links.c:4-78)
@@ -113,6 +118,7 @@ struct Context {
   double *d_res = nullptr;
   double *h_res = nullptr;   // pinned
   int red_blocks = 0;
+  size_t part_cap = 0;       // doubles in d_part
 };
 Context &ctx();
 void require_init(const char *fn);
