@@ -7,7 +7,8 @@ seeded gauge field U = exp(i 0.5 H) on a 32^3 x 64 lattice (t antiperiodic,
 staggered signs), mass 0.01, one Gaussian source on even sites, solved with
 QOP_D3_asqtad_invert (evenodd = EVEN) to |b - A x| / |b| <= 1e-10
 (rsqmin = 1e-20), using the mixed-precision reliable-update solver
-(FP16 storage, FP32 arithmetic, FP64 reliable updates).
+(16-bit fixed-point storage with per-site / per-link FP32 scales, FP32
+arithmetic, FP64 reductions and reliable updates).
 
 Reported: solves/s (device-resident inputs, CUDA events on the library
 stream, max over ranks), e2e solves/s through the C ABI from pinned host
@@ -46,6 +47,7 @@ def parse():
     ap.add_argument("--eps", type=float, default=0.5)
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--prec", type=int, default=16, choices=[16, 32, 64], help="sloppy precision")
+    ap.add_argument("--ru-delta", type=float, default=0.3, help="reliable-update threshold on |r|")
     ap.add_argument("--fp64-steps", type=int, default=1)
     ap.add_argument("--cpu-iters", type=int, default=12, help="CG iterations timed on the host")
     ap.add_argument("--no-cpu", action="store_true")
@@ -71,12 +73,16 @@ def measured_peak():
 
 
 def ncu_traffic(kernel_class, L):
-    """DRAM bytes per launch from the committed ncu summary, if one exists."""
-    p = os.path.join(ROOT, "profiles", "ncu_%s_%s.md" % (kernel_class, "x".join(map(str, L))))
-    if not os.path.exists(p):
-        return None
-    m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", open(p).read())
-    return float(m.group(1)) if m else None
+    """DRAM bytes per launch from the committed ncu summary of this kernel
+    class (captured on a smaller lattice and scaled by the sites one launch
+    processes; traffic per site is volume independent once the fields exceed
+    L2), or None when no capture is committed."""
+    import glob
+    for p in sorted(glob.glob(os.path.join(ROOT, "profiles", "ncu_%s_*.md" % kernel_class))):
+        m = re.search(r"dram_bytes_per_site:\s*([0-9.eE+]+)", open(p).read())
+        if m:
+            return float(m.group(1)) * int(np.prod(L)) // 2
+    return None
 
 
 class Clocks:
@@ -234,7 +240,7 @@ def run_b200(a):
     big = 1 << 30
 
     def solve(hout, hin, prec):
-        q.set_opts(prec_sloppy=prec)
+        q.set_opts(prec_sloppy=prec, half_format=0, ru_delta=a.ru_delta)
         q.dslash(fla, 0.0, hout, hout, QOP_EVEN, QOP_EVEN)          # zero initial guess
         ia = QOP_invert_arg_t(1e9, 200000, 200000, 10, QOP_EVEN)
         ra = QOP_resid_arg_t(rsq, 0, 0, 0, 0, 0)
@@ -368,10 +374,10 @@ def run_b200(a):
             "metric": "mixed-prec CG solves/s @1e-10 (HISQ eo solve)",
             "value": value, "unit": "solves/s", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": total_ms / a.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f16" if a.prec == 16 else ("f32" if a.prec == 32 else "f64"),
+            "vs_baseline": None, "dtype": "f32" if a.prec < 64 else "f64",
             "data": "synthetic",
             "config": {"workload": workload_name(a, L), "lattice": L, "mass": a.mass, "tol": a.tol,
-                       "eps": a.eps, "precision": "FP%d storage / FP32 arith / FP64 reliable updates" % a.prec,
+                       "eps": a.eps, "precision": ("int16 fixed-point" if a.prec == 16 else "FP%d" % a.prec) + " storage, FP32 arithmetic, FP64 reductions and reliable updates (delta %g)" % a.ru_delta,
                        "parallelism": "replicas x%d" % world,
                        "l2": "inputs larger than L2 (links %.1f GB FP64)" % (V * 16 * 18 * 8 / 1e9)},
             "p50_ms": float(np.percentile(lat_sorted, 50)), "p99_ms": float(np.percentile(lat_sorted, 99)),

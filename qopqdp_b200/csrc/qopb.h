@@ -96,7 +96,7 @@ struct Options {
   // (64 = exact reference algorithm in the handle's precision)
   int sloppy_prec = 64;
   int half_format = 0;           // 16-bit storage: 0 int16 fixed point, 1 IEEE FP16, 2 FP16 links
-  double ru_delta = 0.1;         // reliable-update threshold on |r|
+  double ru_delta = 0.3;         // reliable-update threshold on |r| (0.3-0.5 measured best)
   int chunk = 16;                // iterations launched per host check
   // QOP_hisq_links_set_opts (lib/hisq_links.c:4-78)
   int want_deps = 0, want_aux = 1, reunit_allow_svd = 1, reunit_svd_only = 0;
