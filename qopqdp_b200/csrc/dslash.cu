@@ -230,6 +230,30 @@ double Dslash<T>::ddagd(FlaT<T> *f, double mass, c2<T> *out, const c2<T> *in, in
   return (double)((T)c.h_res[0] + m2 * (T)c.h_res[1]);
 }
 
+template <typename T>
+void Dslash<T>::ddagd_norm2_ws(FlaT<T> *f, double mass, c2<T> *out, const c2<T> *in, int eo, c2<T> *tmp_block,
+                               double *part, unsigned *count, double *res) {
+  Context &c = ctx();
+  const Geom &g = c.g;
+  const int p = eo, q = 1 - eo;
+  const T m2 = (T)mass * (T)mass;
+  const i64 lk_par = (i64)f->nlinks * 9 * g.Vh;
+  const int grid = grid_for(g.Vh, HOP_BLOCK);
+  // t = D_qp in (sum |t|^2 -> res[0]); out_p = m^2 in_p - D_pq t (sum |in_p|^2 -> res[1])
+  if (f->nlinks == 16) {
+    k_hop<T, 16, HOP_SET, 1><<<grid, HOP_BLOCK, 0, c.s>>>(tmp_block, in + par_off(g, p), f->d + q * lk_par, nullptr,
+                                                          (T)0, g, q, part, count, res);
+    k_hop<T, 16, HOP_M2_MINUS, 2><<<grid, HOP_BLOCK, 0, c.s>>>(out + par_off(g, p), tmp_block, f->d + p * lk_par,
+                                                               in + par_off(g, p), m2, g, p, part, count, res + 1);
+  } else {
+    k_hop<T, 8, HOP_SET, 1><<<grid, HOP_BLOCK, 0, c.s>>>(tmp_block, in + par_off(g, p), f->d + q * lk_par, nullptr,
+                                                         (T)0, g, q, part, count, res);
+    k_hop<T, 8, HOP_M2_MINUS, 2><<<grid, HOP_BLOCK, 0, c.s>>>(out + par_off(g, p), tmp_block, f->d + p * lk_par,
+                                                              in + par_off(g, p), m2, g, p, part, count, res + 1);
+  }
+  QLAUNCHN(2);
+}
+
 template struct Dslash<float>;
 template struct Dslash<double>;
 

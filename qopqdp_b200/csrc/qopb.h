@@ -201,6 +201,11 @@ template <typename T> struct Dslash {
   // tmp receives D_oe in on the opposite parity; returns |tmp|^2 + m^2 |in|^2
   static double ddagd(FlaT<T> *f, double mass, c2<T> *out, const c2<T> *in, int eo,
                       c2<T> *tmp, bool want_norm);
+  // the same operator with caller-provided scratch: tmp_block is one parity
+  // block ([3][Vh]), part/count/res the reduction partials, ticket and the
+  // two sums; launches only, no allocation and no synchronisation
+  static void ddagd_norm2_ws(FlaT<T> *f, double mass, c2<T> *out, const c2<T> *in, int eo, c2<T> *tmp_block,
+                             double *part, unsigned *count, double *res);
 };
 
 // link construction (links.cu)
