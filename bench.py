@@ -127,6 +127,24 @@ class Clocks:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
+# ---------------------------------------------------------------- replicas
+def reduce_max(x, dist, device):
+    """Max of a per-rank scalar over all ranks (the job is as slow as its
+    slowest replica); identity without a process group."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(steps, world, max_ms):
+    """Solves/s of the whole job: every replica solves `steps` systems; the
+    elapsed time is the slowest rank's."""
+    return steps * world / (max_ms / 1e3)
+
+
 # ---------------------------------------------------------------- reference arm
 def cpu_iteration_time(fat, lng, L, src, mass, iters, threads):
     """Seconds per CG iteration of the oracle (the reference algorithm restated
@@ -259,11 +277,7 @@ def run_b200(a):
         torch.cuda.synchronize()
 
     def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(x, dist, "cuda")
 
     hin = q.create_V(src, QOP_EVEN)
     hout = q.create_V(np.zeros_like(src))
@@ -289,7 +303,7 @@ def run_b200(a):
     n_launch = lib.QOPB_launch_count() - n_launch0
     kst = prof_end()
     total_ms = max_over_ranks(e0.elapsed_time(e1))
-    value = a.steps * world / (total_ms / 1e3)
+    value = job_throughput(a.steps, world, total_ms)
     # independent FP64 check of the last solution's residual (not timed)
     sol = q.extract_V(hout, V)
     # ---------------- plain FP64 GPU CG (the reference algorithm in FP64)
