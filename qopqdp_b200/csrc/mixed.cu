@@ -86,78 +86,73 @@ struct SpF16 {
   }
 };
 
-// 16-bit fixed point: an int16 q stands for q * s / 32767 with a float scale
-// s per site (vectors) or per link (links), 15 bits of mantissa relative to
-// the largest component.  Decoding avoids integer->float conversion
-// instructions: the bit pattern 0x4B400000 + q is the float 1.5*2^23 + q
-// exactly, so q*c = fma(bits, c, -1.5*2^23*c).
-__device__ __forceinline__ float q16_lo(unsigned w, float c, float b) {
-  return fmaf(__int_as_float(0x4B400000 + (((int)(w << 16)) >> 16)), c, b);
+// 16-bit fixed point: a component x is stored as u = q + 32768 with
+// q = round(32767 x / s) in [-32767, 32767] and a float scale s per site
+// (vectors) or per link (links): 15 bits of mantissa relative to the largest
+// component.  Decoding needs no integer->float conversion: byte-permuting u
+// under the exponent 0x4B gives the float 2^23 + u exactly, and subtracting
+// 2^23 + 32768 gives q exactly; the scale is applied afterwards.
+__device__ __forceinline__ float u16_lo(unsigned w) {
+  return __int_as_float(__byte_perm(w, 0x4B000000u, 0x7610)) - 8421376.0f;
 }
-__device__ __forceinline__ float q16_hi(unsigned w, float c, float b) {
-  return fmaf(__int_as_float(0x4B400000 + (((int)w) >> 16)), c, b);
+__device__ __forceinline__ float u16_hi(unsigned w) {
+  return __int_as_float(__byte_perm(w, 0x4B000000u, 0x7632)) - 8421376.0f;
 }
-__device__ __forceinline__ unsigned q16_pack(float x, float y, float inv) {
+__device__ __forceinline__ unsigned u16_pack(float x, float y, float inv) {
   int a = __float2int_rn(x * inv), b = __float2int_rn(y * inv);
-  a = max(-32767, min(32767, a));
-  b = max(-32767, min(32767, b));
-  return ((unsigned)a & 0xffffu) | ((unsigned)b << 16);
+  a = max(-32767, min(32767, a)) + 32768;
+  b = max(-32767, min(32767, b)) + 32768;
+  return (unsigned)a | ((unsigned)b << 16);
+}
+__device__ __forceinline__ float absmax3(const float2 v[3]) {
+  return fmaxf(fmaxf(fmaxf(fabsf(v[0].x), fabsf(v[0].y)), fmaxf(fabsf(v[1].x), fabsf(v[1].y))),
+               fmaxf(fabsf(v[2].x), fabsf(v[2].y)));
 }
 
-// int16 vector parity block: [Vh] x 16 bytes = {int16 re/im x 3 colours; float s}
+// int16 vector parity block: [Vh] x 16 bytes = {u16 re/im x 3 colours; float s}
 struct SpQ16 {
   typedef uint4 elem;
   static i64 block(i64 Vh) { return Vh; }
   static const char *name() { return "q16"; }
   static constexpr int site_bytes = 16;
+  // integer-valued components and the factor c = s/32767 that scales them
+  __device__ static float raw(uint4 u, float2 q[3]) {
+    q[0] = make_float2(u16_lo(u.x), u16_hi(u.x));
+    q[1] = make_float2(u16_lo(u.y), u16_hi(u.y));
+    q[2] = make_float2(u16_lo(u.z), u16_hi(u.z));
+    return __uint_as_float(u.w) * (1.0f / 32767.0f);
+  }
   __device__ static void load(const uint4 *b, int i, i64, float2 v[3]) {
-    uint4 u = b[i];
-    const float c = __uint_as_float(u.w) * (1.0f / 32767.0f), o = -12582912.0f * c;
-    v[0] = make_float2(q16_lo(u.x, c, o), q16_hi(u.x, c, o));
-    v[1] = make_float2(q16_lo(u.y, c, o), q16_hi(u.y, c, o));
-    v[2] = make_float2(q16_lo(u.z, c, o), q16_hi(u.z, c, o));
+    const float c = raw(b[i], v);
+#pragma unroll
+    for (int k = 0; k < 3; k++) v[k] = make_float2(v[k].x * c, v[k].y * c);
   }
   __device__ static void store(uint4 *b, int i, i64, float2 v[3]) {
-    float m = fmaxf(fmaxf(fmaxf(fabsf(v[0].x), fabsf(v[0].y)), fmaxf(fabsf(v[1].x), fabsf(v[1].y))),
-                    fmaxf(fabsf(v[2].x), fabsf(v[2].y)));
+    const float m = absmax3(v);
     const float inv = m > 0.f ? 32767.0f / m : 0.f;
     uint4 u;
-    u.x = q16_pack(v[0].x, v[0].y, inv);
-    u.y = q16_pack(v[1].x, v[1].y, inv);
-    u.z = q16_pack(v[2].x, v[2].y, inv);
+    u.x = u16_pack(v[0].x, v[0].y, inv);
+    u.y = u16_pack(v[1].x, v[1].y, inv);
+    u.z = u16_pack(v[2].x, v[2].y, inv);
     u.w = __float_as_uint(m);
     b[i] = u;
-    const float c = m * (1.0f / 32767.0f), o = -12582912.0f * c;
-    v[0] = make_float2(q16_lo(u.x, c, o), q16_hi(u.x, c, o));
-    v[1] = make_float2(q16_lo(u.y, c, o), q16_hi(u.y, c, o));
-    v[2] = make_float2(q16_lo(u.z, c, o), q16_hi(u.z, c, o));
+    load(&u, 0, 0, v);
   }
 };
 
 struct LinksSloppy { const void *a, *b, *c; };   // one parity
 
-// int16 links: a = [nl][Vh] uint4 (elements 0-3), b = [nl][Vh] uint4 (4-7),
-// c = [nl][Vh] uint2 {element 8, float scale}: 40 bytes per link
-struct LkQ16 {
+// int16 links, blocked for bulk copies: for every block of QB = 128 sites
+// and every slot k, 5120 contiguous bytes = A[128] uint4 (elements 0-3),
+// B[128] uint4 (elements 4-7), C[128] uint2 {element 8, float scale}; the
+// slots of a block follow each other, so the links of 4 slots for 128 sites
+// are one 20 KB contiguous span.  40 bytes per link.
+constexpr int QB = 128;
+constexpr int QSLOT = QB * 40;          // bytes per (block, slot)
+struct LkQ16B {
   static const char *name() { return "q16"; }
   static constexpr int link_bytes = 40;
-  __device__ static void load(const LinksSloppy &L, int k, int i, i64 Vh, float2 U[9]) {
-    i64 o = (i64)k * Vh + i;
-    uint4 a = ((const uint4 *)L.a)[o], b = ((const uint4 *)L.b)[o];
-    uint2 t = ((const uint2 *)L.c)[o];
-    const float c = __uint_as_float(t.y) * (1.0f / 32767.0f), z = -12582912.0f * c;
-    U[0] = make_float2(q16_lo(a.x, c, z), q16_hi(a.x, c, z));
-    U[1] = make_float2(q16_lo(a.y, c, z), q16_hi(a.y, c, z));
-    U[2] = make_float2(q16_lo(a.z, c, z), q16_hi(a.z, c, z));
-    U[3] = make_float2(q16_lo(a.w, c, z), q16_hi(a.w, c, z));
-    U[4] = make_float2(q16_lo(b.x, c, z), q16_hi(b.x, c, z));
-    U[5] = make_float2(q16_lo(b.y, c, z), q16_hi(b.y, c, z));
-    U[6] = make_float2(q16_lo(b.z, c, z), q16_hi(b.z, c, z));
-    U[7] = make_float2(q16_lo(b.w, c, z), q16_hi(b.w, c, z));
-    U[8] = make_float2(q16_lo(t.x, c, z), q16_hi(t.x, c, z));
-  }
 };
-
 // FP32 links: a = [nl][9][Vh] float2
 struct LkF32 {
   static const char *name() { return "f32"; }
@@ -353,31 +348,257 @@ __global__ void k_links_f16(uint4 *A, uint4 *B, __half2 *C, const double2 *src, 
   C[s] = h[8];
 }
 
-__global__ void k_links_q16(uint4 *A, uint4 *B, uint2 *C, const double2 *src, int nl, i64 Vh) {
-  i64 s = blockIdx.x * (i64)blockDim.x + threadIdx.x;   // over [2][nl][Vh]
-  if (s >= 2 * nl * Vh) return;
-  i64 i = s % Vh, pk = s / Vh;
-  const double2 *b = src + pk * 9 * Vh + i;
+// blocked int16 links: dst is [2 parities][nblk][nl slots][QSLOT bytes];
+// sites beyond Vh in the last block are zero links
+__global__ void k_links_q16b(unsigned char *dst, const double2 *src, int nl, i64 Vh, i64 nblk) {
+  i64 s = blockIdx.x * (i64)blockDim.x + threadIdx.x;   // over [2][nblk][nl][QB]
+  if (s >= 2 * nblk * nl * QB) return;
+  const int t = (int)(s % QB);
+  const i64 r = s / QB;
+  const int k = (int)(r % nl);
+  const i64 pb = r / nl, b = pb % nblk, p = pb / nblk;
+  const i64 i = b * QB + t;
   float2 e[9];
   float m = 0.f;
 #pragma unroll
-  for (int k = 0; k < 9; k++) {
-    double2 v = b[k * Vh];
-    e[k] = make_float2((float)v.x, (float)v.y);
-    m = fmaxf(m, fmaxf(fabsf(e[k].x), fabsf(e[k].y)));
+  for (int j = 0; j < 9; j++) {
+    e[j] = make_float2(0.f, 0.f);
+    if (i < Vh) {
+      double2 v = src[((p * nl + k) * 9 + j) * Vh + i];
+      e[j] = make_float2((float)v.x, (float)v.y);
+    }
+    m = fmaxf(m, fmaxf(fabsf(e[j].x), fabsf(e[j].y)));
   }
   const float inv = m > 0.f ? 32767.0f / m : 0.f;
-  A[s] = make_uint4(q16_pack(e[0].x, e[0].y, inv), q16_pack(e[1].x, e[1].y, inv), q16_pack(e[2].x, e[2].y, inv),
-                    q16_pack(e[3].x, e[3].y, inv));
-  B[s] = make_uint4(q16_pack(e[4].x, e[4].y, inv), q16_pack(e[5].x, e[5].y, inv), q16_pack(e[6].x, e[6].y, inv),
-                    q16_pack(e[7].x, e[7].y, inv));
-  C[s] = make_uint2(q16_pack(e[8].x, e[8].y, inv), __float_as_uint(m));
+  unsigned char *base = dst + (size_t)r * QSLOT;
+  reinterpret_cast<uint4 *>(base)[t] =
+      make_uint4(u16_pack(e[0].x, e[0].y, inv), u16_pack(e[1].x, e[1].y, inv), u16_pack(e[2].x, e[2].y, inv),
+                 u16_pack(e[3].x, e[3].y, inv));
+  reinterpret_cast<uint4 *>(base + 16 * QB)[t] =
+      make_uint4(u16_pack(e[4].x, e[4].y, inv), u16_pack(e[5].x, e[5].y, inv), u16_pack(e[6].x, e[6].y, inv),
+                 u16_pack(e[7].x, e[7].y, inv));
+  reinterpret_cast<uint2 *>(base + 32 * QB)[t] = make_uint2(u16_pack(e[8].x, e[8].y, inv), __float_as_uint(m));
+}
+
+// ---------------------------------------------------------------- TMA-staged hop
+// Variant 1 (TMA): link data of GRP slots x 128 sites (GRP x 5 KB,
+// contiguous in the blocked layout) is fetched by one cp.async.bulk into
+// shared memory against an mbarrier; two buffers alternate so the next
+// group's links stream in while the current group is computed.  Neighbour
+// sites are read with ordinary loads (L1/L2 hits) issued before the group's
+// barrier wait.  Every wait is bounded: on timeout the kernel raises
+// MIX_ERROR and skips the work.
+// Variant 2 (LDG): the same blocked layout read with plain coalesced loads,
+// the raw words of BATCH slots loaded before any of them is decoded so that
+// BATCH x 56 bytes per thread are in flight.
+enum { MIX_ERROR = 3 };
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, uint64_t *bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+               ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t *bar, unsigned phase) {
+  unsigned ok;
+  asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+               : "=r"(ok) : "r"(smem_u32(bar)), "r"(phase) : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned phase) {
+  for (int it = 0; it < (1 << 22); it++)
+    if (mbar_try(bar, phase)) return true;
+  return false;
+}
+
+// neighbour of (x0..x3) = lex in parity p along mu by d, as a checkerboard index
+struct NbrGeom { int L[4]; int str[4]; };
+__device__ __forceinline__ int nbr_fast(const NbrGeom &n, const int x[4], int lex, int mu, int d) {
+  int t = x[mu] + d;
+  int off = d * n.str[mu];
+  if (t >= n.L[mu]) off -= n.L[mu] * n.str[mu];
+  else if (t < 0) off += n.L[mu] * n.str[mu];
+  return (lex + off) >> 1;
+}
+
+// a += (link scale x site scale) x (integer link) (integer site): one slot
+__device__ __forceinline__ void q16_slot(const uint4 ua, const uint4 ub, const uint2 uc, const uint4 nb, float2 a[3]) {
+  float2 v[3];
+  const float cv = SpQ16::raw(nb, v);
+  const float sc = __uint_as_float(uc.y) * (1.0f / 32767.0f) * cv;
+  float2 U[9];
+  U[0] = make_float2(u16_lo(ua.x), u16_hi(ua.x)); U[1] = make_float2(u16_lo(ua.y), u16_hi(ua.y));
+  U[2] = make_float2(u16_lo(ua.z), u16_hi(ua.z)); U[3] = make_float2(u16_lo(ua.w), u16_hi(ua.w));
+  U[4] = make_float2(u16_lo(ub.x), u16_hi(ub.x)); U[5] = make_float2(u16_lo(ub.y), u16_hi(ub.y));
+  U[6] = make_float2(u16_lo(ub.z), u16_hi(ub.z)); U[7] = make_float2(u16_lo(ub.w), u16_hi(ub.w));
+  U[8] = make_float2(u16_lo(uc.x), u16_hi(uc.x));
+#pragma unroll
+  for (int r = 0; r < 3; r++) {
+    float2 t = make_float2(0.f, 0.f);
+    cfmaf(t, U[3 * r], v[0]);
+    cfmaf(t, U[3 * r + 1], v[1]);
+    cfmaf(t, U[3 * r + 2], v[2]);
+    a[r].x = fmaf(sc, t.x, a[r].x);
+    a[r].y = fmaf(sc, t.y, a[r].y);
+  }
+}
+
+// KIND epilogue shared by both variants; returns the value to reduce
+template <int KIND>
+__device__ __forceinline__ double q16_epilogue(uint4 *out, const uint4 *same, int i, i64 Vh, float m2, float2 a[3]) {
+  if (KIND == 1) {
+    SpQ16::store(out, i, Vh, a);
+    return (double)a[0].x * a[0].x + (double)a[0].y * a[0].y + (double)a[1].x * a[1].x + (double)a[1].y * a[1].y +
+           (double)a[2].x * a[2].x + (double)a[2].y * a[2].y;
+  }
+  float2 sv[3];
+  SpQ16::load(same, i, Vh, sv);
+#pragma unroll
+  for (int c = 0; c < 3; c++) a[c] = make_float2(m2 * sv[c].x - a[c].x, m2 * sv[c].y - a[c].y);
+  SpQ16::store(out, i, Vh, a);
+  return (double)sv[0].x * sv[0].x + (double)sv[0].y * sv[0].y + (double)sv[1].x * sv[1].x +
+         (double)sv[1].y * sv[1].y + (double)sv[2].x * sv[2].x + (double)sv[2].y * sv[2].y;
+}
+
+template <int KIND>
+__device__ __forceinline__ void q16_finish(double (&acc1)[1], double *part, unsigned *count, MixState *st) {
+  if (grid_sum<1>(acc1, part, count, &st->red)) {
+    if (KIND == 1) {
+      st->dp2 = st->red;
+    } else if (st->flag != MIX_ERROR) {
+      double pAp = st->dp2 + st->m2 * st->red;   // <p, A p> = |D p|^2 + m^2 |p|^2
+      if (!(pAp > 0)) st->flag = MIX_BREAK;
+      else st->alpha = st->rsq / pAp;
+    }
+  }
+}
+
+template <int NL, int KIND, int GRP>
+__global__ void __launch_bounds__(QB)
+k_mix_hop_q16(uint4 *__restrict__ out, const uint4 *__restrict__ src, const unsigned char *__restrict__ lk,
+              const uint4 *__restrict__ same, Geom g, NbrGeom ng, int p, MixState *st, double *part,
+              unsigned *count) {
+  if (st->flag) return;
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ __align__(8) uint64_t bar[2];
+  constexpr int NG = NL / GRP;
+  constexpr int GB = GRP * QSLOT;
+  const int tid = threadIdx.x;
+  const i64 Vh = g.Vh;
+  const int i = blockIdx.x * QB + tid;
+  const unsigned char *gl = lk + (size_t)blockIdx.x * NL * QSLOT;
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  __syncthreads();
+  if (tid == 0) {
+#pragma unroll
+    for (int gi = 0; gi < 2 && gi < NG; gi++) {
+      mbar_expect_tx(&bar[gi], GB);
+      bulk_g2s(smem + gi * GB, gl + gi * GB, GB, &bar[gi]);
+    }
+  }
+  const bool live = i < Vh;
+  int x[4] = {0, 0, 0, 0}, lex = 0;
+  if (live) {
+    site_coords(g, i, p, x);
+    lex = ((x[0] * g.L[1] + x[1]) * g.L[2] + x[2]) * g.L[3] + x[3];
+  }
+  float2 a[3] = {make_float2(0, 0), make_float2(0, 0), make_float2(0, 0)};
+  bool ok = true;
+  int issued[2] = {NG > 0 ? 1 : 0, NG > 1 ? 1 : 0}, waited[2] = {0, 0};   // thread 0 bookkeeping
+#pragma unroll
+  for (int gi = 0; gi < NG; gi++) {
+    const int buf = gi & 1;
+    uint4 nb[GRP];
+#pragma unroll
+    for (int s = 0; s < GRP; s++) {
+      const int k = gi * GRP + s;
+      nb[s] = live ? src[nbr_fast(ng, x, lex, slot_mu<NL>(k), slot_disp<NL>(k))] : make_uint4(0, 0, 0, 0);
+    }
+    const bool arrived = mbar_wait_bounded(&bar[buf], (gi >> 1) & 1);
+    if (!arrived) ok = false;
+    else waited[buf]++;
+    if (arrived && live) {
+      const unsigned char *sb = smem + buf * GB;
+#pragma unroll
+      for (int s = 0; s < GRP; s++) {
+        const unsigned char *ls = sb + s * QSLOT;
+        q16_slot(reinterpret_cast<const uint4 *>(ls)[tid], reinterpret_cast<const uint4 *>(ls + 16 * QB)[tid],
+                 reinterpret_cast<const uint2 *>(ls + 32 * QB)[tid], nb[s], a);
+      }
+    }
+    if (gi + 2 < NG) {
+      __syncthreads();                 // every thread is done with this buffer
+      if (tid == 0 && ok) {
+        mbar_expect_tx(&bar[buf], GB);
+        bulk_g2s(smem + buf * GB, gl + (gi + 2) * GB, GB, &bar[buf]);
+        issued[buf]++;
+      }
+    }
+  }
+  if (!ok) {
+    st->flag = MIX_ERROR;
+    if (tid == 0)   // let copies still in flight land before the block exits (bounded)
+      for (int b2 = 0; b2 < 2; b2++)
+        while (waited[b2] < issued[b2] && mbar_wait_bounded(&bar[b2], waited[b2] & 1)) waited[b2]++;
+  }
+  double acc1[1] = {0.0};
+  if (live) acc1[0] = q16_epilogue<KIND>(out, same, i, Vh, (float)st->m2, a);
+  q16_finish<KIND>(acc1, part, count, st);
+}
+
+template <int NL, int KIND, int BATCH>
+__global__ void __launch_bounds__(QB)
+k_mix_hop_q16r(uint4 *__restrict__ out, const uint4 *__restrict__ src, const unsigned char *__restrict__ lk,
+               const uint4 *__restrict__ same, Geom g, NbrGeom ng, int p, MixState *st, double *part,
+               unsigned *count) {
+  if (st->flag) return;
+  const int tid = threadIdx.x;
+  const i64 Vh = g.Vh;
+  const int i = blockIdx.x * QB + tid;
+  const unsigned char *gl = lk + (size_t)blockIdx.x * NL * QSLOT;
+  double acc1[1] = {0.0};
+  if (i < Vh) {
+    int x[4];
+    site_coords(g, i, p, x);
+    const int lex = ((x[0] * g.L[1] + x[1]) * g.L[2] + x[2]) * g.L[3] + x[3];
+    float2 a[3] = {make_float2(0, 0), make_float2(0, 0), make_float2(0, 0)};
+#pragma unroll
+    for (int k0 = 0; k0 < NL; k0 += BATCH) {
+      uint4 ua[BATCH], ub[BATCH], nb[BATCH];
+      uint2 uc[BATCH];
+#pragma unroll
+      for (int s = 0; s < BATCH; s++) {
+        const int k = k0 + s;
+        const unsigned char *ls = gl + k * QSLOT;
+        ua[s] = __ldcs(reinterpret_cast<const uint4 *>(ls) + tid);
+        ub[s] = __ldcs(reinterpret_cast<const uint4 *>(ls + 16 * QB) + tid);
+        uc[s] = __ldcs(reinterpret_cast<const uint2 *>(ls + 32 * QB) + tid);
+        nb[s] = src[nbr_fast(ng, x, lex, slot_mu<NL>(k), slot_disp<NL>(k))];
+      }
+#pragma unroll
+      for (int s = 0; s < BATCH; s++) q16_slot(ua[s], ub[s], uc[s], nb[s], a);
+    }
+    acc1[0] = q16_epilogue<KIND>(out, same, i, Vh, (float)st->m2, a);
+  }
+  q16_finish<KIND>(acc1, part, count, st);
 }
 
 struct SloppyLinks {
   int nl = 0;
   void *a16 = nullptr, *b16 = nullptr, *c16 = nullptr;   // IEEE FP16 copy
-  void *aq = nullptr, *bq = nullptr, *cq = nullptr;      // int16 fixed-point copy
+  void *aq = nullptr;                                    // int16 fixed-point copy (blocked)
   FlaT<float> *f32 = nullptr;                            // FP32 copy
 };
 
@@ -388,7 +609,7 @@ void sloppy_invalidate(void *fla_any) {
   if (it == g_sloppy.end()) return;
   SloppyLinks *s = it->second;
   if (s->a16) { dfree(s->a16); dfree(s->b16); dfree(s->c16); }
-  if (s->aq) { dfree(s->aq); dfree(s->bq); dfree(s->cq); }
+  if (s->aq) dfree(s->aq);
   if (s->f32) fla_destroy<float>(s->f32);
   delete s;
   g_sloppy.erase(it);
@@ -411,11 +632,10 @@ static SloppyLinks *sloppy_get(FlaT<double> *f, int lkfmt) {
     QLAUNCH();
   }
   if (lkfmt == LK_Q16 && !s->aq) {
-    s->aq = dmalloc(sizeof(uint4) * n);
-    s->bq = dmalloc(sizeof(uint4) * n);
-    s->cq = dmalloc(sizeof(uint2) * n);
-    k_links_q16<<<grid_for(n, 256), 256, 0, ctx().s>>>((uint4 *)s->aq, (uint4 *)s->bq, (uint2 *)s->cq, f->d,
-                                                       f->nlinks, g.Vh);
+    const i64 nblk = (g.Vh + QB - 1) / QB;
+    s->aq = dmalloc((size_t)2 * nblk * f->nlinks * QSLOT);
+    const i64 nt = 2 * nblk * f->nlinks * QB;
+    k_links_q16b<<<grid_for(nt, 256), 256, 0, ctx().s>>>((unsigned char *)s->aq, f->d, f->nlinks, g.Vh, nblk);
     QLAUNCH();
   }
   if (lkfmt == LK_F32 && !s->f32) s->f32 = fla_convert<float, double>(f);
@@ -427,9 +647,44 @@ static LinksSloppy links_parity(SloppyLinks *s, int lkfmt, int p) {
   const i64 o = (i64)p * s->nl * Vh;
   if (lkfmt == LK_F16)
     return LinksSloppy{(const uint4 *)s->a16 + o, (const uint4 *)s->b16 + o, (const __half2 *)s->c16 + o};
-  if (lkfmt == LK_Q16)
-    return LinksSloppy{(const uint4 *)s->aq + o, (const uint4 *)s->bq + o, (const uint2 *)s->cq + o};
+  if (lkfmt == LK_Q16) {
+    const i64 nblk = (Vh + QB - 1) / QB;
+    return LinksSloppy{(const unsigned char *)s->aq + (size_t)p * nblk * s->nl * QSLOT, nullptr, nullptr};
+  }
   return LinksSloppy{s->f32->d + (i64)p * s->nl * 9 * Vh, nullptr, nullptr};
+}
+
+// int16 hop launch: variant 0 = plain loads, 4 slots batched (default);
+// 1 / 2 = TMA bulk staging with 2- / 4-slot groups; 3 / 4 = plain loads
+// with 2 / 8 slots batched
+template <int KIND>
+static void launch_q16(int variant, int nl, int grid, uint4 *out, const uint4 *src, const unsigned char *lk,
+                       const uint4 *same, const Geom &g, const NbrGeom &ng, int par, MixState *st) {
+  Context &c = ctx();
+#define Q16_ARGS out, src, lk, same, g, ng, par, st, c.d_part, c.d_count
+  switch (variant) {
+    case 1:
+      if (nl == 16) k_mix_hop_q16<16, KIND, 2><<<grid, QB, 4 * QSLOT, c.s>>>(Q16_ARGS);
+      else k_mix_hop_q16<8, KIND, 2><<<grid, QB, 4 * QSLOT, c.s>>>(Q16_ARGS);
+      break;
+    case 2:
+      if (nl == 16) k_mix_hop_q16<16, KIND, 4><<<grid, QB, 8 * QSLOT, c.s>>>(Q16_ARGS);
+      else k_mix_hop_q16<8, KIND, 4><<<grid, QB, 8 * QSLOT, c.s>>>(Q16_ARGS);
+      break;
+    case 3:
+      if (nl == 16) k_mix_hop_q16r<16, KIND, 2><<<grid, QB, 0, c.s>>>(Q16_ARGS);
+      else k_mix_hop_q16r<8, KIND, 2><<<grid, QB, 0, c.s>>>(Q16_ARGS);
+      break;
+    case 4:
+      if (nl == 16) k_mix_hop_q16r<16, KIND, 8><<<grid, QB, 0, c.s>>>(Q16_ARGS);
+      else k_mix_hop_q16r<8, KIND, 8><<<grid, QB, 0, c.s>>>(Q16_ARGS);
+      break;
+    default:
+      if (nl == 16) k_mix_hop_q16r<16, KIND, 4><<<grid, QB, 0, c.s>>>(Q16_ARGS);
+      else k_mix_hop_q16r<8, KIND, 4><<<grid, QB, 0, c.s>>>(Q16_ARGS);
+      break;
+  }
+#undef Q16_ARGS
 }
 
 // ---------------------------------------------------------------- driver
@@ -457,7 +712,10 @@ static void run_mixed(LinOp<double> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t *r
   MixState *dst = dalloc<MixState>(1);
   MixState h{};
   const LinksSloppy lk_p = links_parity(sl, lkfmt, p), lk_q = links_parity(sl, lkfmt, q);
-  const int gridh = grid_for(Vh, 128), gridv = grid_for(Vh, 256);
+  const int gridh = grid_for(Vh, 128), gridv = grid_for(Vh, 256), gridq = (int)((Vh + QB - 1) / QB);
+  NbrGeom ng;
+  for (int d = 0; d < 4; d++) ng.L[d] = g.L[d];
+  ng.str[3] = 1; ng.str[2] = g.L[3]; ng.str[1] = g.L[2] * g.L[3]; ng.str[0] = g.L[1] * g.L[2] * g.L[3];
   const int nl = sl->nl;
   const double hop_bytes = (double)Vh * (nl * Lk::link_bytes + 2 * Sp::site_bytes);
   char hname[32];
@@ -490,14 +748,24 @@ static void run_mixed(LinOp<double> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t *r
     for (int k = 0; k < chunk; k++) {
       {
         ProfScope ps1(hname, hop_bytes);
-        if (nl == 16) k_mix_hop<Sp, Lk, 16, 1><<<gridh, 128, 0, c.s>>>(ts, ps, lk_q, nullptr, g, q, dst, c.d_part, c.d_count);
-        else k_mix_hop<Sp, Lk, 8, 1><<<gridh, 128, 0, c.s>>>(ts, ps, lk_q, nullptr, g, q, dst, c.d_part, c.d_count);
+        if constexpr (std::is_same<Lk, LkQ16B>::value) {
+          const unsigned char *lq = (const unsigned char *)lk_q.a;
+          launch_q16<1>(c.opt.hop_kernel, nl, gridq, ts, ps, lq, nullptr, g, ng, q, dst);
+        } else {
+          if (nl == 16) k_mix_hop<Sp, Lk, 16, 1><<<gridh, 128, 0, c.s>>>(ts, ps, lk_q, nullptr, g, q, dst, c.d_part, c.d_count);
+          else k_mix_hop<Sp, Lk, 8, 1><<<gridh, 128, 0, c.s>>>(ts, ps, lk_q, nullptr, g, q, dst, c.d_part, c.d_count);
+        }
         recs.push_back(ps1.idx);
       }
       {
         ProfScope ps2(hname, hop_bytes + (double)Vh * Sp::site_bytes);
-        if (nl == 16) k_mix_hop<Sp, Lk, 16, 2><<<gridh, 128, 0, c.s>>>(Aps, ts, lk_p, ps, g, p, dst, c.d_part, c.d_count);
-        else k_mix_hop<Sp, Lk, 8, 2><<<gridh, 128, 0, c.s>>>(Aps, ts, lk_p, ps, g, p, dst, c.d_part, c.d_count);
+        if constexpr (std::is_same<Lk, LkQ16B>::value) {
+          const unsigned char *lp = (const unsigned char *)lk_p.a;
+          launch_q16<2>(c.opt.hop_kernel, nl, gridq, Aps, ts, lp, ps, g, ng, p, dst);
+        } else {
+          if (nl == 16) k_mix_hop<Sp, Lk, 16, 2><<<gridh, 128, 0, c.s>>>(Aps, ts, lk_p, ps, g, p, dst, c.d_part, c.d_count);
+          else k_mix_hop<Sp, Lk, 8, 2><<<gridh, 128, 0, c.s>>>(Aps, ts, lk_p, ps, g, p, dst, c.d_part, c.d_count);
+        }
         recs.push_back(ps2.idx);
       }
       k_mix_update<Sp><<<gridv, 256, 0, c.s>>>(xs, rs, ps, Aps, Vh, dst, c.d_part, c.d_count);
@@ -512,6 +780,10 @@ static void run_mixed(LinOp<double> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t *r
     int hops_ran = 2 * ran + (h.flag == MIX_BREAK ? 2 : 0);
     for (size_t k = hops_ran; k < recs.size(); k++) prof_discard(recs[k]);
     if (h.flag == MIX_RUN) continue;
+    if (h.flag == MIX_ERROR) {
+      dfree(rs); dfree(ps); dfree(Aps); dfree(ts); dfree(xs); dfree(r); dfree(Ax); dfree(dst);
+      fail(QOP_FAIL, "mixed solver: a bulk copy into shared memory did not complete in time");
+    }
     stalls = ran == 0 ? stalls + 1 : 0;           // repeated breakdown without progress
     // reliable update: fold the sloppy solution into FP64, true residual
     k_fold_x<<<grid_for(3 * Vh, 256), 256, 0, c.s>>>(x + is.off, xs, 3 * Vh);
@@ -558,7 +830,7 @@ bool mixed_cgms(LinOp<double> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t **ra, co
   switch (ctx().opt.half_format) {
     case 1: run_mixed<SpF16, LkF16>(L, ia, ra[0], out[0], in, eo, sloppy_get(L.f, LK_F16), LK_F16); break;
     case 2: run_mixed<SpQ16, LkF16>(L, ia, ra[0], out[0], in, eo, sloppy_get(L.f, LK_F16), LK_F16); break;
-    default: run_mixed<SpQ16, LkQ16>(L, ia, ra[0], out[0], in, eo, sloppy_get(L.f, LK_Q16), LK_Q16); break;
+    default: run_mixed<SpQ16, LkQ16B>(L, ia, ra[0], out[0], in, eo, sloppy_get(L.f, LK_Q16), LK_Q16); break;
   }
   return true;
 }
