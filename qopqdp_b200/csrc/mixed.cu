@@ -26,6 +26,7 @@
 #include "dslash.cuh"
 #include "prof.cuh"
 #include "fields.cuh"
+#include <algorithm>
 #include <map>
 #include <vector>
 #include <cmath>
@@ -299,6 +300,158 @@ k_mix_p(typename Sp::elem *__restrict__ p, const typename Sp::elem *__restrict__
   Sp::store(p, i, Vh, pv);
 }
 
+// ---------------------------------------------------------------- multi-shift
+// Shifted systems (A + sigma_s) x_s = b ride on the base recursion with the
+// multi-shift CG recurrences of lib/invert_cg_p.c:234-252 and :356-362:
+//   zeta_{k+1} = zeta_k zeta_{k-1} alpha_{k-1} /
+//                (alpha_k beta_{k-1} (zeta_{k-1} - zeta_k) + zeta_{k-1} alpha_{k-1} (1 + sigma alpha_k))
+//   alpha_s = alpha_k zeta_{k+1} / zeta_k,   beta_s = beta_k zeta_{k+1} alpha_s / (zeta_k alpha_k)
+//   x_s += alpha_s p_s,   p_s = zeta_{k+1} r + beta_s p_s
+// (alpha = step length, beta = direction coefficient; alpha_{-1} = -1,
+// beta_{-1} = 0, zeta_0 = zeta_{-1} = 1).  The scalars are FP64 in device
+// memory; a shift stops being updated once zeta^2 |r|^2 is below its target.
+constexpr int MS_MAX = 32;
+struct MsShift {
+  double sigma, z, zo, bo, stop;   // index 0 (base): bo = previous alpha
+  int active, pad;
+};
+struct MsVecs {
+  void *p[MS_MAX];
+  float2 *x[MS_MAX];
+};
+
+__device__ __forceinline__ void ms_step(const MsShift &s, double al, double be_old, double al_old, double &zn,
+                                        double &as) {
+  zn = s.z * s.zo * al_old;
+  const double c1 = al * be_old * (s.zo - s.z) + s.zo * al_old * (1.0 + s.sigma * al);
+  zn = c1 != 0.0 ? zn / c1 : 0.0;
+  if (s.z != 0.0) as = al * zn / s.z;
+  else zn = as = 0.0;
+}
+
+// base: x += alpha p, r -= alpha Ap, |r|^2; shifts: x_s += alpha_s p_s.
+// Every block derives alpha_s from the state as it was at launch; the last
+// block (after all others have read it) advances the recurrences in place.
+template <class Sp>
+__global__ void __launch_bounds__(256)
+k_ms_update(float2 *__restrict__ xs, typename Sp::elem *__restrict__ r, const typename Sp::elem *__restrict__ p,
+            const typename Sp::elem *__restrict__ Ap, i64 Vh, MixState *st, double *part, unsigned *count,
+            MsShift *sh, int ns, MsVecs mv) {
+  typedef typename Sp::elem E;
+  if (st->flag) return;
+  __shared__ float al_s[MS_MAX];
+  const double al = st->alpha, be_old = st->beta, al_old = sh[0].bo;
+  if (threadIdx.x < MS_MAX) {
+    const int s = threadIdx.x;
+    float v = 0.f;
+    if (s > 0 && s < ns && sh[s].active) {
+      double zn, as;
+      ms_step(sh[s], al, be_old, al_old, zn, as);
+      v = (float)as;
+    }
+    al_s[s] = v;
+  }
+  __syncthreads();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double acc1[1] = {0.0};
+  if (i < Vh) {
+    const float alf = (float)al;
+    float2 pv[3], av[3], rv[3];
+    Sp::load(p, i, Vh, pv);
+    Sp::load(Ap, i, Vh, av);
+    Sp::load(r, i, Vh, rv);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      float2 xv = xs[c * Vh + i];
+      xv.x = fmaf(alf, pv[c].x, xv.x);
+      xv.y = fmaf(alf, pv[c].y, xv.y);
+      xs[c * Vh + i] = xv;
+      rv[c].x = fmaf(-alf, av[c].x, rv[c].x);
+      rv[c].y = fmaf(-alf, av[c].y, rv[c].y);
+    }
+    Sp::store(r, i, Vh, rv);
+    acc1[0] = (double)rv[0].x * rv[0].x + (double)rv[0].y * rv[0].y + (double)rv[1].x * rv[1].x +
+              (double)rv[1].y * rv[1].y + (double)rv[2].x * rv[2].x + (double)rv[2].y * rv[2].y;
+    for (int s = 1; s < ns; s++) {
+      const float a = al_s[s];
+      if (a == 0.f) continue;
+      float2 ps[3];
+      Sp::load(reinterpret_cast<const E *>(mv.p[s]), i, Vh, ps);
+      float2 *xp = mv.x[s];
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        float2 xv = xp[c * Vh + i];
+        xv.x = fmaf(a, ps[c].x, xv.x);
+        xv.y = fmaf(a, ps[c].y, xv.y);
+        xp[c * Vh + i] = xv;
+      }
+    }
+  }
+  if (grid_sum<1>(acc1, part, count, &st->red)) {
+    const double rn = st->red;
+    for (int s = 1; s < ns; s++) {
+      MsShift &q = sh[s];
+      if (!q.active) continue;
+      double zn, as;
+      ms_step(q, al, be_old, al_old, zn, as);
+      q.zo = q.z;
+      q.z = zn;
+      q.bo = as;
+      if (zn * zn * rn <= q.stop) q.active = 0;
+    }
+    sh[0].bo = al;
+    st->iter += 1;
+    st->rsq_old = st->rsq;
+    st->rsq = rn;
+    st->beta = rn / st->rsq_old;
+    if (rn > st->maxr2) st->maxr2 = rn;
+    if (rn < st->delta2 * st->maxr2 || rn <= st->stop || st->iter >= st->max_iter) st->flag = MIX_UPDATE;
+  }
+}
+
+// p = r + beta p;  p_s = zeta_s r + beta_s p_s for the shifts still active
+template <class Sp>
+__global__ void __launch_bounds__(256)
+k_ms_p(typename Sp::elem *__restrict__ p, const typename Sp::elem *__restrict__ r, i64 Vh, MixState *st,
+       const MsShift *sh, int ns, MsVecs mv) {
+  typedef typename Sp::elem E;
+  if (st->flag) return;
+  __shared__ float pz[MS_MAX], pb[MS_MAX];
+  const double be = st->beta, al = st->alpha;
+  if (threadIdx.x < MS_MAX) {
+    const int s = threadIdx.x;
+    float z = 0.f, b = 0.f;
+    if (s > 0 && s < ns && sh[s].active) {
+      const MsShift q = sh[s];
+      const double d = q.zo * al;
+      z = (float)q.z;
+      b = d != 0.0 ? (float)(be * q.z * q.bo / d) : 0.f;
+    }
+    pz[s] = z;
+    pb[s] = b;
+  }
+  __syncthreads();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= Vh) return;
+  const float bef = (float)be;
+  float2 pv[3], rv[3];
+  Sp::load(p, i, Vh, pv);
+  Sp::load(r, i, Vh, rv);
+#pragma unroll
+  for (int c = 0; c < 3; c++) pv[c] = make_float2(fmaf(bef, pv[c].x, rv[c].x), fmaf(bef, pv[c].y, rv[c].y));
+  Sp::store(p, i, Vh, pv);
+  for (int s = 1; s < ns; s++) {
+    const float z = pz[s], b = pb[s];
+    if (z == 0.f && b == 0.f) continue;
+    E *q = reinterpret_cast<E *>(mv.p[s]);
+    Sp::load(q, i, Vh, pv);
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+      pv[c] = make_float2(fmaf(b, pv[c].x, z * rv[c].x), fmaf(b, pv[c].y, z * rv[c].y));
+    Sp::store(q, i, Vh, pv);
+  }
+}
+
 // FP64 [3][Vh] parity block -> sloppy
 template <class Sp>
 __global__ void k_to_sloppy(typename Sp::elem *d, const double2 *s, i64 Vh) {
@@ -350,7 +503,55 @@ __global__ void k_links_f16(uint4 *A, uint4 *B, __half2 *C, const double2 *src, 
 
 // blocked int16 links: dst is [2 parities][nblk][nl slots][QSLOT bytes];
 // sites beyond Vh in the last block are zero links
-__global__ void k_links_q16b(unsigned char *dst, const double2 *src, int nl, i64 Vh, i64 nblk) {
+// Long (Naik) links of asqtad and HISQ are c times a unitary matrix with one
+// |c| for the whole lattice (naik/2 times products of U(3) links, times the
+// +-1 phases).  With RECON they are stored as their first two rows divided by
+// |c| (int16, no per-link scale) and the phase of det(L/|c|): 28 bytes
+// A[128] uint4 (elements 0-3), B[128] uint2 (elements 4-5), C[128] float.
+// The third row is det * conj(row0 x row1).  Fat links keep the 40-byte
+// form.  In the blocked layout slots then alternate fat (5120 bytes per 128
+// sites) and long (3584 bytes).
+constexpr int QSLOTL = QB * 28;
+__host__ __device__ constexpr int q16_slot_off(int k, bool recon) {
+  return recon ? (k >> 1) * (QSLOT + QSLOTL) + (k & 1) * QSLOT : k * QSLOT;
+}
+__host__ __device__ constexpr int q16_block_bytes(int nl, bool recon) {
+  return recon ? (nl / 2) * (QSLOT + QSLOTL) : nl * QSLOT;
+}
+
+// largest unitarity defect |L L^+ / c^2 - 1| and the range of row-0 norms c
+// over all long links; decides whether RECON is exact enough
+__global__ void k_long_check(const double2 *src, int nl, i64 Vh, unsigned long long *defect,
+                             unsigned long long *cmax, unsigned long long *cmin) {
+  i64 s = blockIdx.x * (i64)blockDim.x + threadIdx.x;   // over [2][nl/2 long slots][Vh]
+  if (s >= 2 * (nl / 2) * Vh) return;
+  const i64 i = s % Vh, r = s / Vh;
+  const int k = 2 * (int)(r % (nl / 2)) + 1, p = (int)(r / (nl / 2));
+  double2 e[9];
+  for (int j = 0; j < 9; j++) e[j] = src[(((i64)p * nl + k) * 9 + j) * Vh + i];
+  double c2 = e[0].x * e[0].x + e[0].y * e[0].y + e[1].x * e[1].x + e[1].y * e[1].y + e[2].x * e[2].x +
+              e[2].y * e[2].y;
+  double d = 0;
+  for (int a = 0; a < 3; a++)
+    for (int b = 0; b < 3; b++) {
+      double re = 0, im = 0;
+      for (int j = 0; j < 3; j++) {
+        double2 x = e[3 * a + j], y = e[3 * b + j];
+        re += x.x * y.x + x.y * y.y;
+        im += x.y * y.x - x.x * y.y;
+      }
+      re = re / c2 - (a == b ? 1.0 : 0.0);
+      im = im / c2;
+      d = fmax(d, fmax(fabs(re), fabs(im)));
+    }
+  const double c = sqrt(c2);
+  atomicMax(defect, (unsigned long long)__double_as_longlong(d));
+  atomicMax(cmax, (unsigned long long)__double_as_longlong(c));
+  atomicMin(cmin, (unsigned long long)__double_as_longlong(c));
+}
+
+__global__ void k_links_q16b(unsigned char *dst, const double2 *src, int nl, i64 Vh, i64 nblk, int recon,
+                             double c_long) {
   i64 s = blockIdx.x * (i64)blockDim.x + threadIdx.x;   // over [2][nblk][nl][QB]
   if (s >= 2 * nblk * nl * QB) return;
   const int t = (int)(s % QB);
@@ -358,6 +559,27 @@ __global__ void k_links_q16b(unsigned char *dst, const double2 *src, int nl, i64
   const int k = (int)(r % nl);
   const i64 pb = r / nl, b = pb % nblk, p = pb / nblk;
   const i64 i = b * QB + t;
+  unsigned char *blk = dst + (size_t)pb * q16_block_bytes(nl, recon != 0);
+  if (recon && (k & 1)) {
+    double2 e[9];
+    for (int j = 0; j < 9; j++)
+      e[j] = i < Vh ? src[((p * nl + k) * 9 + j) * Vh + i] : make_double2(j % 4 == 0 ? c_long : 0.0, 0.0);
+    const double2 d = cadd<double>(
+        csub<double>(cmul<double>(e[0], csub<double>(cmul<double>(e[4], e[8]), cmul<double>(e[5], e[7]))),
+                     cmul<double>(e[1], csub<double>(cmul<double>(e[3], e[8]), cmul<double>(e[5], e[6])))),
+        cmul<double>(e[2], csub<double>(cmul<double>(e[3], e[7]), cmul<double>(e[4], e[6]))));
+    const float phase = (float)atan2(d.y, d.x);   // arg det(L/|c|) = arg det(L)
+    const float inv = (float)(32767.0 / c_long);
+    float2 f[6];
+    for (int j = 0; j < 6; j++) f[j] = make_float2((float)e[j].x, (float)e[j].y);
+    unsigned char *base = blk + q16_slot_off(k, true);
+    reinterpret_cast<uint4 *>(base)[t] =
+        make_uint4(u16_pack(f[0].x, f[0].y, inv), u16_pack(f[1].x, f[1].y, inv), u16_pack(f[2].x, f[2].y, inv),
+                   u16_pack(f[3].x, f[3].y, inv));
+    reinterpret_cast<uint2 *>(base + 16 * QB)[t] = make_uint2(u16_pack(f[4].x, f[4].y, inv), u16_pack(f[5].x, f[5].y, inv));
+    reinterpret_cast<float *>(base + 24 * QB)[t] = phase;
+    return;
+  }
   float2 e[9];
   float m = 0.f;
 #pragma unroll
@@ -370,7 +592,7 @@ __global__ void k_links_q16b(unsigned char *dst, const double2 *src, int nl, i64
     m = fmaxf(m, fmaxf(fabsf(e[j].x), fabsf(e[j].y)));
   }
   const float inv = m > 0.f ? 32767.0f / m : 0.f;
-  unsigned char *base = dst + (size_t)r * QSLOT;
+  unsigned char *base = blk + q16_slot_off(k, recon != 0);
   reinterpret_cast<uint4 *>(base)[t] =
       make_uint4(u16_pack(e[0].x, e[0].y, inv), u16_pack(e[1].x, e[1].y, inv), u16_pack(e[2].x, e[2].y, inv),
                  u16_pack(e[3].x, e[3].y, inv));
@@ -558,16 +780,47 @@ k_mix_hop_q16(uint4 *__restrict__ out, const uint4 *__restrict__ src, const unsi
   q16_finish<KIND>(acc1, part, count, st);
 }
 
-template <int NL, int KIND, int BATCH>
-__global__ void __launch_bounds__(QB)
+// one long slot stored as two rows + det phase: a += (|c|/32767 x site scale) U v
+__device__ __forceinline__ void q16_slot_recon(const uint4 ua, const uint2 ub, const float phase, const uint4 nb,
+                                               const float cl, float2 a[3]) {
+  float2 v[3];
+  const float cv = SpQ16::raw(nb, v);
+  const float sc = cl * (1.0f / 32767.0f) * cv;
+  float2 U[9];
+  U[0] = make_float2(u16_lo(ua.x), u16_hi(ua.x)); U[1] = make_float2(u16_lo(ua.y), u16_hi(ua.y));
+  U[2] = make_float2(u16_lo(ua.z), u16_hi(ua.z)); U[3] = make_float2(u16_lo(ua.w), u16_hi(ua.w));
+  U[4] = make_float2(u16_lo(ub.x), u16_hi(ub.x)); U[5] = make_float2(u16_lo(ub.y), u16_hi(ub.y));
+  float sn, cs;
+  __sincosf(phase, &sn, &cs);
+  const float2 z = make_float2(cs * (1.0f / 32767.0f), sn * (1.0f / 32767.0f));
+  // row 2 = det * conj(row0 x row1), in units of the stored integers
+  const float2 c0 = csub<float>(cmul<float>(U[1], U[5]), cmul<float>(U[2], U[4]));
+  const float2 c1 = csub<float>(cmul<float>(U[2], U[3]), cmul<float>(U[0], U[5]));
+  const float2 c2 = csub<float>(cmul<float>(U[0], U[4]), cmul<float>(U[1], U[3]));
+  U[6] = cmul<float>(z, make_float2(c0.x, -c0.y));
+  U[7] = cmul<float>(z, make_float2(c1.x, -c1.y));
+  U[8] = cmul<float>(z, make_float2(c2.x, -c2.y));
+#pragma unroll
+  for (int r = 0; r < 3; r++) {
+    float2 t = make_float2(0.f, 0.f);
+    cfmaf(t, U[3 * r], v[0]);
+    cfmaf(t, U[3 * r + 1], v[1]);
+    cfmaf(t, U[3 * r + 2], v[2]);
+    a[r].x = fmaf(sc, t.x, a[r].x);
+    a[r].y = fmaf(sc, t.y, a[r].y);
+  }
+}
+
+template <int NL, int KIND, int BATCH, bool RECON, int MINB = 1>
+__global__ void __launch_bounds__(QB, MINB)
 k_mix_hop_q16r(uint4 *__restrict__ out, const uint4 *__restrict__ src, const unsigned char *__restrict__ lk,
                const uint4 *__restrict__ same, Geom g, NbrGeom ng, int p, MixState *st, double *part,
-               unsigned *count) {
+               unsigned *count, float c_long) {
   if (st->flag) return;
   const int tid = threadIdx.x;
   const i64 Vh = g.Vh;
   const int i = blockIdx.x * QB + tid;
-  const unsigned char *gl = lk + (size_t)blockIdx.x * NL * QSLOT;
+  const unsigned char *gl = lk + (size_t)blockIdx.x * q16_block_bytes(NL, RECON);
   double acc1[1] = {0.0};
   if (i < Vh) {
     int x[4];
@@ -581,14 +834,25 @@ k_mix_hop_q16r(uint4 *__restrict__ out, const uint4 *__restrict__ src, const uns
 #pragma unroll
       for (int s = 0; s < BATCH; s++) {
         const int k = k0 + s;
-        const unsigned char *ls = gl + k * QSLOT;
+        const unsigned char *ls = gl + q16_slot_off(k, RECON);
         ua[s] = __ldcs(reinterpret_cast<const uint4 *>(ls) + tid);
-        ub[s] = __ldcs(reinterpret_cast<const uint4 *>(ls + 16 * QB) + tid);
-        uc[s] = __ldcs(reinterpret_cast<const uint2 *>(ls + 32 * QB) + tid);
+        if (RECON && (k & 1)) {
+          uint2 w = __ldcs(reinterpret_cast<const uint2 *>(ls + 16 * QB) + tid);
+          ub[s] = make_uint4(w.x, w.y, 0u, 0u);
+          uc[s] = make_uint2(__float_as_uint(__ldcs(reinterpret_cast<const float *>(ls + 24 * QB) + tid)), 0u);
+        } else {
+          ub[s] = __ldcs(reinterpret_cast<const uint4 *>(ls + 16 * QB) + tid);
+          uc[s] = __ldcs(reinterpret_cast<const uint2 *>(ls + 32 * QB) + tid);
+        }
         nb[s] = src[nbr_fast(ng, x, lex, slot_mu<NL>(k), slot_disp<NL>(k))];
       }
 #pragma unroll
-      for (int s = 0; s < BATCH; s++) q16_slot(ua[s], ub[s], uc[s], nb[s], a);
+      for (int s = 0; s < BATCH; s++) {
+        if (RECON && ((k0 + s) & 1))
+          q16_slot_recon(ua[s], make_uint2(ub[s].x, ub[s].y), __uint_as_float(uc[s].x), nb[s], c_long, a);
+        else
+          q16_slot(ua[s], ub[s], uc[s], nb[s], a);
+      }
     }
     acc1[0] = q16_epilogue<KIND>(out, same, i, Vh, (float)st->m2, a);
   }
@@ -599,6 +863,9 @@ struct SloppyLinks {
   int nl = 0;
   void *a16 = nullptr, *b16 = nullptr, *c16 = nullptr;   // IEEE FP16 copy
   void *aq = nullptr;                                    // int16 fixed-point copy (blocked)
+  int recon = 0;                                         // long links as 2 rows + det phase
+  double c_long = 0;                                     // |c| of the long links when recon
+  int recon_mode = -1;                                   // recon option the copy was built for
   FlaT<float> *f32 = nullptr;                            // FP32 copy
 };
 
@@ -631,12 +898,41 @@ static SloppyLinks *sloppy_get(FlaT<double> *f, int lkfmt) {
                                                        f->nlinks, g.Vh);
     QLAUNCH();
   }
+  // the TMA variants need equal slot sizes: reconstruction only with the
+  // plain-load kernels, and only if the long links pass the unitarity check
+  const int want_recon = (ctx().opt.recon_long && ctx().opt.hop_kernel != 1 && ctx().opt.hop_kernel != 2) ? 1 : 0;
+  if (lkfmt == LK_Q16 && s->aq && s->recon_mode != want_recon) { dfree(s->aq); s->aq = nullptr; }
   if (lkfmt == LK_Q16 && !s->aq) {
     const i64 nblk = (g.Vh + QB - 1) / QB;
-    s->aq = dmalloc((size_t)2 * nblk * f->nlinks * QSLOT);
+    int recon = 0;
+    double c_long = 0;
+    if (want_recon && f->nlinks == 16) {
+      unsigned long long *st = dalloc<unsigned long long>(3);
+      unsigned long long init[3] = {0ull, 0ull, 0ull};
+      const double big = 1e300;
+      memcpy(&init[2], &big, 8);
+      QCHECK(cudaMemcpyAsync(st, init, sizeof init, cudaMemcpyHostToDevice, ctx().s));
+      const i64 nc = 2 * (f->nlinks / 2) * g.Vh;
+      k_long_check<<<grid_for(nc, 256), 256, 0, ctx().s>>>(f->d, f->nlinks, g.Vh, st, st + 1, st + 2);
+      QLAUNCH();
+      unsigned long long h[3];
+      QCHECK(cudaMemcpyAsync(h, st, sizeof h, cudaMemcpyDeviceToHost, ctx().s));
+      sync();
+      dfree(st);
+      double defect, cmax, cmin;
+      memcpy(&defect, &h[0], 8); memcpy(&cmax, &h[1], 8); memcpy(&cmin, &h[2], 8);
+      // exact to well below the 2^-15 storage precision
+      if (cmax > 0 && defect < 1e-7 && (cmax - cmin) <= 1e-7 * cmax) { recon = 1; c_long = cmax; }
+      log0(QOP_VERB_MED, "sloppy links: long-link defect %g, |c| in [%g, %g] -> recon %d\n", defect, cmin, cmax, recon);
+    }
+    s->aq = dmalloc((size_t)2 * nblk * q16_block_bytes(f->nlinks, recon != 0));
     const i64 nt = 2 * nblk * f->nlinks * QB;
-    k_links_q16b<<<grid_for(nt, 256), 256, 0, ctx().s>>>((unsigned char *)s->aq, f->d, f->nlinks, g.Vh, nblk);
+    k_links_q16b<<<grid_for(nt, 256), 256, 0, ctx().s>>>((unsigned char *)s->aq, f->d, f->nlinks, g.Vh, nblk, recon,
+                                                          c_long);
     QLAUNCH();
+    s->recon = recon;
+    s->c_long = c_long;
+    s->recon_mode = want_recon;
   }
   if (lkfmt == LK_F32 && !s->f32) s->f32 = fla_convert<float, double>(f);
   return s;
@@ -649,20 +945,43 @@ static LinksSloppy links_parity(SloppyLinks *s, int lkfmt, int p) {
     return LinksSloppy{(const uint4 *)s->a16 + o, (const uint4 *)s->b16 + o, (const __half2 *)s->c16 + o};
   if (lkfmt == LK_Q16) {
     const i64 nblk = (Vh + QB - 1) / QB;
-    return LinksSloppy{(const unsigned char *)s->aq + (size_t)p * nblk * s->nl * QSLOT, nullptr, nullptr};
+    return LinksSloppy{(const unsigned char *)s->aq + (size_t)p * nblk * q16_block_bytes(s->nl, s->recon != 0),
+                       nullptr, nullptr};
   }
   return LinksSloppy{s->f32->d + (i64)p * s->nl * 9 * Vh, nullptr, nullptr};
 }
 
-// int16 hop launch: variant 0 = plain loads, 4 slots batched (default);
+// int16 hop launch: variant 0 = plain loads, 4 slots batched;
 // 1 / 2 = TMA bulk staging with 2- / 4-slot groups; 3 / 4 = plain loads
-// with 2 / 8 slots batched
+// with 2 / 8 slots batched; 5-10 = plain loads with the registers capped
+// for B resident blocks per SM (5: 2 slots, B 10 = 48 registers, the
+// default; 6: 2, 12 (spills); 7: 4, 8; 8: 2, 8; 9: 1, 10; 10: 2, 9).
+// Without a cap the compiler takes ~150 registers and 3 blocks fit per SM;
+// at 32^3x64 variant 5 runs a hop in 131 us against 149 us for variant 3.
 template <int KIND>
-static void launch_q16(int variant, int nl, int grid, uint4 *out, const uint4 *src, const unsigned char *lk,
-                       const uint4 *same, const Geom &g, const NbrGeom &ng, int par, MixState *st) {
+static void launch_q16(int variant, int nl, bool recon, float c_long, int grid, uint4 *out, const uint4 *src,
+                       const unsigned char *lk, const uint4 *same, const Geom &g, const NbrGeom &ng, int par,
+                       MixState *st) {
   Context &c = ctx();
 #define Q16_ARGS out, src, lk, same, g, ng, par, st, c.d_part, c.d_count
+#define Q16R(NLV, B)                                                                        \
+  do {                                                                                      \
+    if (recon) k_mix_hop_q16r<NLV, KIND, B, true><<<grid, QB, 0, c.s>>>(Q16_ARGS, c_long);  \
+    else k_mix_hop_q16r<NLV, KIND, B, false><<<grid, QB, 0, c.s>>>(Q16_ARGS, c_long);       \
+  } while (0)
+#define Q16RM(B, M)                                                                                       \
+  do {                                                                                                    \
+    if (nl != 16) k_mix_hop_q16r<8, KIND, B, false, M><<<grid, QB, 0, c.s>>>(Q16_ARGS, c_long);          \
+    else if (recon) k_mix_hop_q16r<16, KIND, B, true, M><<<grid, QB, 0, c.s>>>(Q16_ARGS, c_long);        \
+    else k_mix_hop_q16r<16, KIND, B, false, M><<<grid, QB, 0, c.s>>>(Q16_ARGS, c_long);                  \
+  } while (0)
   switch (variant) {
+    case 5: Q16RM(2, 10); break;   // register cap for 10 resident blocks
+    case 6: Q16RM(2, 12); break;
+    case 7: Q16RM(4, 8); break;
+    case 8: Q16RM(2, 8); break;
+    case 9: Q16RM(1, 10); break;
+    case 10: Q16RM(2, 9); break;
     case 1:
       if (nl == 16) k_mix_hop_q16<16, KIND, 2><<<grid, QB, 4 * QSLOT, c.s>>>(Q16_ARGS);
       else k_mix_hop_q16<8, KIND, 2><<<grid, QB, 4 * QSLOT, c.s>>>(Q16_ARGS);
@@ -672,35 +991,48 @@ static void launch_q16(int variant, int nl, int grid, uint4 *out, const uint4 *s
       else k_mix_hop_q16<8, KIND, 4><<<grid, QB, 8 * QSLOT, c.s>>>(Q16_ARGS);
       break;
     case 3:
-      if (nl == 16) k_mix_hop_q16r<16, KIND, 2><<<grid, QB, 0, c.s>>>(Q16_ARGS);
-      else k_mix_hop_q16r<8, KIND, 2><<<grid, QB, 0, c.s>>>(Q16_ARGS);
+      if (nl == 16) Q16R(16, 2);
+      else k_mix_hop_q16r<8, KIND, 2, false><<<grid, QB, 0, c.s>>>(Q16_ARGS, c_long);
       break;
     case 4:
-      if (nl == 16) k_mix_hop_q16r<16, KIND, 8><<<grid, QB, 0, c.s>>>(Q16_ARGS);
-      else k_mix_hop_q16r<8, KIND, 8><<<grid, QB, 0, c.s>>>(Q16_ARGS);
+      if (nl == 16) Q16R(16, 8);
+      else k_mix_hop_q16r<8, KIND, 8, false><<<grid, QB, 0, c.s>>>(Q16_ARGS, c_long);
       break;
     default:
-      if (nl == 16) k_mix_hop_q16r<16, KIND, 4><<<grid, QB, 0, c.s>>>(Q16_ARGS);
-      else k_mix_hop_q16r<8, KIND, 4><<<grid, QB, 0, c.s>>>(Q16_ARGS);
+      if (nl == 16) Q16R(16, 4);
+      else k_mix_hop_q16r<8, KIND, 4, false><<<grid, QB, 0, c.s>>>(Q16_ARGS, c_long);
       break;
   }
+#undef Q16RM
+#undef Q16R
 #undef Q16_ARGS
 }
 
 // ---------------------------------------------------------------- driver
+// Shifted systems solved alongside the base one: sigma[0] = 0 is the base,
+// stop[s] the absolute target on zeta_s^2 |r|^2, x[s] the FP64 solutions
+// (x[0] is the base solution argument of run_mixed).
+struct MsArgs {
+  int ns;
+  const double *sigma, *stop;
+  c2<double> **x;
+};
+
 template <class Sp, class Lk>
 static void run_mixed(LinOp<double> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t *ra, c2<double> *x,
-                      const c2<double> *b, int eo, SloppyLinks *sl, int lkfmt) {
+                      const c2<double> *b, int eo, SloppyLinks *sl, int lkfmt, const MsArgs *ms = nullptr) {
   typedef typename Sp::elem E;
   Context &c = ctx();
   const Geom &g = c.g;
   const i64 Vh = g.Vh;
   const int p = eo, q = 1 - eo;
   const Range is = vrange(g, eo);
+  const int ns = ms ? ms->ns : 1;
   const double b2 = Blas<double>::norm2(b, is);
   ra->final_rel = 0;
   ra->final_restart = 0;
   Blas<double>::zero(x, is);
+  for (int s = 1; s < ns; s++) Blas<double>::zero(ms->x[s], is);
   if (b2 == 0.0) { ra->final_rsq = 0; ra->final_iter = 0; return; }
   const double stop = ra->rsqmin * b2;
   const i64 nb = Sp::block(Vh);
@@ -711,13 +1043,37 @@ static void run_mixed(LinOp<double> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t *r
   Blas<double>::copy(r, b, is);
   MixState *dst = dalloc<MixState>(1);
   MixState h{};
+  MsShift *dsh = nullptr;
+  MsVecs mv{};
+  if (ns > 1) {
+    std::vector<MsShift> hs(ns);
+    for (int s = 0; s < ns; s++) hs[s] = MsShift{ms->sigma[s], 1.0, 1.0, -1.0, ms->stop[s], 1, 0};
+    dsh = dalloc<MsShift>(ns);
+    QCHECK(cudaMemcpyAsync(dsh, hs.data(), sizeof(MsShift) * ns, cudaMemcpyHostToDevice, c.s));
+    for (int s = 1; s < ns; s++) {
+      mv.p[s] = dalloc<E>(nb);
+      mv.x[s] = dalloc<float2>(3 * Vh);
+      dzero(mv.x[s], sizeof(float2) * 3 * Vh);
+    }
+  }
+  auto release = [&]() {
+    dfree(rs); dfree(ps); dfree(Aps); dfree(ts); dfree(xs); dfree(r); dfree(Ax); dfree(dst);
+    for (int s = 1; s < ns; s++) { dfree(mv.p[s]); dfree(mv.x[s]); }
+    dfree(dsh);
+  };
   const LinksSloppy lk_p = links_parity(sl, lkfmt, p), lk_q = links_parity(sl, lkfmt, q);
   const int gridh = grid_for(Vh, 128), gridv = grid_for(Vh, 256), gridq = (int)((Vh + QB - 1) / QB);
   NbrGeom ng;
   for (int d = 0; d < 4; d++) ng.L[d] = g.L[d];
   ng.str[3] = 1; ng.str[2] = g.L[3]; ng.str[1] = g.L[2] * g.L[3]; ng.str[0] = g.L[1] * g.L[2] * g.L[3];
   const int nl = sl->nl;
-  const double hop_bytes = (double)Vh * (nl * Lk::link_bytes + 2 * Sp::site_bytes);
+  // compulsory bytes: links once (reconstructed long links 28 B), input and
+  // output sites once
+  const double link_site = (std::is_same<Lk, LkQ16B>::value && sl->recon) ? (nl / 2) * (40.0 + 28.0)
+                                                                           : (double)nl * Lk::link_bytes;
+  const double hop_bytes = (double)Vh * (link_site + 2 * Sp::site_bytes);
+  const bool recon = sl->recon != 0;
+  const float c_long = (float)sl->c_long;
   char hname[32];
   snprintf(hname, sizeof hname, "hop_%s_link%s", Sp::name(), Lk::name());
 
@@ -737,6 +1093,10 @@ static void run_mixed(LinOp<double> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t *r
   h.rsq_old = b2;
   k_copy_elems<E><<<grid_for(nb, 256), 256, 0, c.s>>>(ps, rs, nb);
   QLAUNCH();
+  for (int s = 1; s < ns; s++) {
+    k_copy_elems<E><<<grid_for(nb, 256), 256, 0, c.s>>>((E *)mv.p[s], rs, nb);
+    QLAUNCH();
+  }
   QCHECK(cudaMemcpyAsync(dst, &h, sizeof h, cudaMemcpyHostToDevice, c.s));
   int nru = 0, stalls = 0;
   double r2 = b2;
@@ -750,7 +1110,7 @@ static void run_mixed(LinOp<double> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t *r
         ProfScope ps1(hname, hop_bytes);
         if constexpr (std::is_same<Lk, LkQ16B>::value) {
           const unsigned char *lq = (const unsigned char *)lk_q.a;
-          launch_q16<1>(c.opt.hop_kernel, nl, gridq, ts, ps, lq, nullptr, g, ng, q, dst);
+          launch_q16<1>(c.opt.hop_kernel, nl, recon, c_long, gridq, ts, ps, lq, nullptr, g, ng, q, dst);
         } else {
           if (nl == 16) k_mix_hop<Sp, Lk, 16, 1><<<gridh, 128, 0, c.s>>>(ts, ps, lk_q, nullptr, g, q, dst, c.d_part, c.d_count);
           else k_mix_hop<Sp, Lk, 8, 1><<<gridh, 128, 0, c.s>>>(ts, ps, lk_q, nullptr, g, q, dst, c.d_part, c.d_count);
@@ -761,15 +1121,20 @@ static void run_mixed(LinOp<double> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t *r
         ProfScope ps2(hname, hop_bytes + (double)Vh * Sp::site_bytes);
         if constexpr (std::is_same<Lk, LkQ16B>::value) {
           const unsigned char *lp = (const unsigned char *)lk_p.a;
-          launch_q16<2>(c.opt.hop_kernel, nl, gridq, Aps, ts, lp, ps, g, ng, p, dst);
+          launch_q16<2>(c.opt.hop_kernel, nl, recon, c_long, gridq, Aps, ts, lp, ps, g, ng, p, dst);
         } else {
           if (nl == 16) k_mix_hop<Sp, Lk, 16, 2><<<gridh, 128, 0, c.s>>>(Aps, ts, lk_p, ps, g, p, dst, c.d_part, c.d_count);
           else k_mix_hop<Sp, Lk, 8, 2><<<gridh, 128, 0, c.s>>>(Aps, ts, lk_p, ps, g, p, dst, c.d_part, c.d_count);
         }
         recs.push_back(ps2.idx);
       }
-      k_mix_update<Sp><<<gridv, 256, 0, c.s>>>(xs, rs, ps, Aps, Vh, dst, c.d_part, c.d_count);
-      k_mix_p<Sp><<<gridv, 256, 0, c.s>>>(ps, rs, Vh, dst);
+      if (ns > 1) {
+        k_ms_update<Sp><<<gridv, 256, 0, c.s>>>(xs, rs, ps, Aps, Vh, dst, c.d_part, c.d_count, dsh, ns, mv);
+        k_ms_p<Sp><<<gridv, 256, 0, c.s>>>(ps, rs, Vh, dst, dsh, ns, mv);
+      } else {
+        k_mix_update<Sp><<<gridv, 256, 0, c.s>>>(xs, rs, ps, Aps, Vh, dst, c.d_part, c.d_count);
+        k_mix_p<Sp><<<gridv, 256, 0, c.s>>>(ps, rs, Vh, dst);
+      }
       QLAUNCHN(4);
     }
     (void)prof0;
@@ -781,13 +1146,17 @@ static void run_mixed(LinOp<double> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t *r
     for (size_t k = hops_ran; k < recs.size(); k++) prof_discard(recs[k]);
     if (h.flag == MIX_RUN) continue;
     if (h.flag == MIX_ERROR) {
-      dfree(rs); dfree(ps); dfree(Aps); dfree(ts); dfree(xs); dfree(r); dfree(Ax); dfree(dst);
+      release();
       fail(QOP_FAIL, "mixed solver: a bulk copy into shared memory did not complete in time");
     }
     stalls = ran == 0 ? stalls + 1 : 0;           // repeated breakdown without progress
     // reliable update: fold the sloppy solution into FP64, true residual
     k_fold_x<<<grid_for(3 * Vh, 256), 256, 0, c.s>>>(x + is.off, xs, 3 * Vh);
     QLAUNCH();
+    for (int s = 1; s < ns; s++) {
+      k_fold_x<<<grid_for(3 * Vh, 256), 256, 0, c.s>>>(ms->x[s] + is.off, mv.x[s], 3 * Vh);
+      QLAUNCH();
+    }
     L.d2(Ax, x);
     Blas<double>::axpby(r, 1.0, b, -1.0, Ax, is);
     r2 = Blas<double>::norm2(r, is);
@@ -796,6 +1165,7 @@ static void run_mixed(LinOp<double> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t *r
     if (r2 <= stop || h.iter + nru >= h.max_iter || stalls > 2) break;
     const bool broke = (h.flag == MIX_BREAK);
     const double rsq_prev = broke ? 0.0 : h.rsq_old;
+    if (ns > 1 && (broke || !(rsq_prev > 0))) break;   // shifted recurrences cannot restart
     refresh(r2);
     if (broke || !(rsq_prev > 0)) {
       // restart the recursion from the true residual
@@ -805,7 +1175,8 @@ static void run_mixed(LinOp<double> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t *r
       h.beta = r2 / rsq_prev;
       h.flag = MIX_RUN;
       QCHECK(cudaMemcpyAsync(dst, &h, sizeof h, cudaMemcpyHostToDevice, c.s));
-      k_mix_p<Sp><<<gridv, 256, 0, c.s>>>(ps, rs, Vh, dst);
+      if (ns > 1) k_ms_p<Sp><<<gridv, 256, 0, c.s>>>(ps, rs, Vh, dst, dsh, ns, mv);
+      else k_mix_p<Sp><<<gridv, 256, 0, c.s>>>(ps, rs, Vh, dst);
       QLAUNCH();
     }
     h.flag = MIX_RUN;
@@ -813,26 +1184,128 @@ static void run_mixed(LinOp<double> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t *r
   }
   ra->final_rsq = r2 / b2;
   ra->final_iter = h.iter + nru;
-  dfree(rs); dfree(ps); dfree(Aps); dfree(ts); dfree(xs); dfree(r); dfree(Ax); dfree(dst);
+  release();
   sync();
+}
+
+static void run_sloppy(LinOp<double> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t *ra, c2<double> *x,
+                       const c2<double> *b, int eo, int prec, const MsArgs *ms) {
+  if (prec == 32) {
+    run_mixed<SpF32, LkF32>(L, ia, ra, x, b, eo, sloppy_get(L.f, LK_F32), LK_F32, ms);
+    return;
+  }
+  // 16-bit storage: 0 = int16 fixed point (default), 1 = IEEE FP16,
+  // 2 = FP16 links with int16 vectors
+  switch (ctx().opt.half_format) {
+    case 1: run_mixed<SpF16, LkF16>(L, ia, ra, x, b, eo, sloppy_get(L.f, LK_F16), LK_F16, ms); break;
+    case 2: run_mixed<SpQ16, LkF16>(L, ia, ra, x, b, eo, sloppy_get(L.f, LK_F16), LK_F16, ms); break;
+    default: run_mixed<SpQ16, LkQ16B>(L, ia, ra, x, b, eo, sloppy_get(L.f, LK_Q16), LK_Q16, ms); break;
+  }
 }
 
 bool mixed_cgms(LinOp<double> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t **ra, const double *shifts, int ns,
                 c2<double> **out, const c2<double> *in, int eo, int prec) {
   if (ns != 1 || shifts[0] != 0.0) return false;   // multi-shift: reference CGMS in FP64
   if (prec != 16 && prec != 32) return false;
-  if (prec == 32) {
-    run_mixed<SpF32, LkF32>(L, ia, ra[0], out[0], in, eo, sloppy_get(L.f, LK_F32), LK_F32);
-    return true;
-  }
-  // 16-bit storage: 0 = int16 fixed point (default), 1 = IEEE FP16,
-  // 2 = FP16 links with int16 vectors
-  switch (ctx().opt.half_format) {
-    case 1: run_mixed<SpF16, LkF16>(L, ia, ra[0], out[0], in, eo, sloppy_get(L.f, LK_F16), LK_F16); break;
-    case 2: run_mixed<SpQ16, LkF16>(L, ia, ra[0], out[0], in, eo, sloppy_get(L.f, LK_F16), LK_F16); break;
-    default: run_mixed<SpQ16, LkQ16B>(L, ia, ra[0], out[0], in, eo, sloppy_get(L.f, LK_Q16), LK_Q16); break;
-  }
+  run_sloppy(L, ia, ra[0], out[0], in, eo, prec, nullptr);
   return true;
+}
+
+// Several masses on one parity with sloppy storage.  Phase 1: the solves
+// that share a source and start from zero run as one reduced-precision
+// multi-shift CG (reliable updates on the lightest mass, every heavier mass
+// stops when its implied residual zeta^2 |r|^2 reaches its target).  Phase 2:
+// every solve goes through the reference driver on its own (one mass, the
+// phase-1 vector as its starting guess), which refines it with the
+// single-mass mixed solver until its FP64 true residual meets its target and
+// applies the m * A^-1 normalisation.
+void solve_multi_mixed(QOP_info_t *info, FlaT<double> *f, QOP_invert_arg_t *ia, QOP_resid_arg_t **ra,
+                       const double *masses, c2<double> **out, c2<double> **in, int nsolve) {
+  const Geom &g = ctx().g;
+  const int eo = ia->evenodd, prec = ctx().opt.sloppy_prec;
+  const Range is = vrange(g, eo);
+  const double t0 = wtime();
+  const double nflop = 0.5 * (20 * 3 + 2 * 8 * 3 * 3 * f->nlinks), nflopm = 0.5 * 10 * 3;
+  const int max_iter = ia->max_iter;
+  double flop = 0;
+  int it1 = 0;
+  std::vector<char> seen(nsolve, 0);
+  for (int i = 0; i < nsolve; i++) {
+    if (seen[i]) continue;
+    std::vector<int> grp;
+    for (int j = i; j < nsolve; j++)
+      if (!seen[j] && in[j] == in[i]) { grp.push_back(j); seen[j] = 1; }
+    std::vector<double> m2;
+    bool ok = true;
+    for (int j : grp) {
+      m2.push_back(masses[j] * masses[j]);
+      if (ra[j]->relmin > 0) ok = false;   // Fermilab stopping: reference driver only
+    }
+    std::sort(m2.begin(), m2.end());
+    m2.erase(std::unique(m2.begin(), m2.end()), m2.end());
+    const int ns = (int)m2.size();
+    if (!ok || ns < 2 || ns > MS_MAX) continue;
+    for (int j : grp)
+      if (Blas<double>::norm2(out[j], is) != 0.0) ok = false;
+    const double b2 = Blas<double>::norm2(in[i], is);
+    if (!ok || b2 == 0.0) continue;
+    std::vector<double> sigma(ns), stop(ns, -1.0);
+    for (int s = 0; s < ns; s++) sigma[s] = m2[s] - m2[0];
+    for (int j : grp) {
+      const int s = (int)(std::lower_bound(m2.begin(), m2.end(), masses[j] * masses[j]) - m2.begin());
+      const double t = ra[j]->rsqmin * b2;
+      stop[s] = stop[s] < 0 ? t : std::min(stop[s], t);
+    }
+    std::vector<c2<double> *> xv(ns);
+    for (int s = 0; s < ns; s++) xv[s] = dalloc<c2<double>>(vec_elems(g));
+    c2<double> *tmp = dalloc<c2<double>>(vec_elems(g));
+    LinOp<double> L{f, std::sqrt(m2[0]), eo, tmp};
+    QOP_invert_arg_t ia1 = *ia;
+    QOP_resid_arg_t ra1 = QOP_RESID_ARG_DEFAULT;
+    ra1.rsqmin = stop[0] / b2;
+    const MsArgs msa{ns, sigma.data(), stop.data(), xv.data()};
+    run_sloppy(L, &ia1, &ra1, xv[0], in[i], eo, prec, &msa);
+    it1 += ra1.final_iter;
+    flop += (nflop + nflopm * (ns - 1)) * ra1.final_iter * (double)g.V;
+    if (ctx().verbosity >= QOP_VERB_MED) {
+      c2<double> *ax = dalloc<c2<double>>(vec_elems(g));
+      for (int s = 0; s < ns; s++) {
+        LinOp<double> Ls{f, std::sqrt(m2[s]), eo, tmp};
+        Ls.d2(ax, xv[s]);
+        Blas<double>::axpby(ax, 1.0, in[i], -1.0, ax, is);
+        log0(QOP_VERB_MED, "SOLVE(mixed multi-mass): mass %g true rsq %g target %g\n", std::sqrt(m2[s]),
+             Blas<double>::norm2(ax, is) / b2, stop[s] / b2);
+      }
+      dfree(ax);
+    }
+    for (int j : grp) {
+      const int s = (int)(std::lower_bound(m2.begin(), m2.end(), masses[j] * masses[j]) - m2.begin());
+      Blas<double>::copy(out[j], xv[s], is);
+    }
+    for (int s = 0; s < ns; s++) dfree(xv[s]);
+    dfree(tmp);
+  }
+  int it2 = 0, nres = 0;
+  for (int i = 0; i < nsolve; i++) {
+    QOP_info_t inf{};
+    QOP_invert_arg_t ia2 = *ia;
+    ia2.max_iter = std::max(1, max_iter - it1);
+    solve_multi<double>(&inf, f, &ia2, &ra[i], &masses[i], &out[i], &in[i], 1);
+    it2 += ra[i]->final_iter;
+    nres = std::max(nres, ra[i]->final_restart);
+    flop += inf.final_flop;
+  }
+  for (int i = 0; i < nsolve; i++) {
+    ra[i]->final_iter = it1 + it2;
+    ra[i]->final_restart = nres;
+  }
+  log0(QOP_VERB_LOW, "SOLVE(mixed multi-mass): multi-shift its %d, refinement its %d\n", it1, it2);
+  sync();
+  if (info) {
+    info->final_sec = wtime() - t0;
+    info->final_flop = flop;
+    info->status = QOP_SUCCESS;
+  }
 }
 
 }  // namespace qopb

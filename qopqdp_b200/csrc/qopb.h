@@ -98,7 +98,8 @@ struct Options {
   int half_format = 0;           // 16-bit storage: 0 int16 fixed point, 1 IEEE FP16, 2 FP16 links
   double ru_delta = 0.3;         // reliable-update threshold on |r| (0.3-0.5 measured best)
   int chunk = 16;                // iterations launched per host check
-  int hop_kernel = 3;            // int16 hop variant (mixed.cu launch_q16); 3 measured fastest
+  int hop_kernel = 5;            // int16 hop variant (mixed.cu launch_q16); 5 measured fastest
+  int recon_long = 1;            // int16 long links as two rows + det phase when exact
   // QOP_hisq_links_set_opts (lib/hisq_links.c:4-78)
   int want_deps = 0, want_aux = 1, reunit_allow_svd = 1, reunit_svd_only = 0;
   double reunit_svd_rel_error = 1e-8, reunit_svd_abs_error = 1e-8;

@@ -309,6 +309,12 @@ void solve_multi(QOP_info_t *info, FlaT<T> *f, QOP_invert_arg_t *ia, QOP_resid_a
     for (int i = 0; i < nsolve; i++) invert<T>(info, f, ia, ra[i], masses[i], out[i], in[i]);
     return;
   }
+  if constexpr (std::is_same<T, double>::value) {
+    if (ctx().opt.sloppy_prec < 64 && nsolve > 1) {
+      solve_multi_mixed(info, f, ia, ra, masses, out, in, nsolve);
+      return;
+    }
+  }
   const int opeo = opp(ineo);
   const Range is = vrange(g, ineo);
   double dtime = 0;

@@ -37,5 +37,9 @@ void invert_multi(QOP_info_t *info, FlaT<T> *f, QOP_invert_arg_t *ia, QOP_resid_
 // base system.  Returns false when the path is not applicable.
 bool mixed_cgms(LinOp<double> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t **ra, const double *shifts, int ns,
                 c2<double> **out, const c2<double> *in, int eo, int prec);
+// several masses on one parity with prec_sloppy < 64: reduced-precision
+// multi-shift CG per shared source, then per-solve refinement
+void solve_multi_mixed(QOP_info_t *info, FlaT<double> *f, QOP_invert_arg_t *ia, QOP_resid_arg_t **ra,
+                       const double *masses, c2<double> **out, c2<double> **in, int nsolve);
 
 }  // namespace qopb

@@ -69,3 +69,107 @@ def test_mixed_iterations_close_to_fp64():
     q.set_opts(prec_sloppy=64)
     assert its[32] <= 1.3 * its[64] + 20 and its[16] <= 2.0 * its[64] + 50, its
     q.destroy_L(fla)
+
+
+@pytest.mark.parametrize("kind", ["hisq", "random_long"])
+def test_long_link_reconstruction(kind):
+    """int16 long links stored as two rows + det phase (when they are |c| times
+    a unitary matrix) give the same convergence as full storage; links that
+    are not of that form fall back to full storage automatically."""
+    L = (4, 4, 4, 8)
+    V = int(np.prod(L))
+    q = gpu_lattice(L, "D")
+    fat, lng, _, _ = hisq_links(L, 0.5, 9)
+    if kind == "random_long":
+        rng = np.random.default_rng(5)
+        lng = tuple(0.05 * rng.standard_normal(a.shape) for a in lng)
+    fo = O.Fla(O.Lattice(L), fat, lng)
+    fla = q.create_L_from_raw(fat, lng)
+    src = LT.gaussian_vector(L, 300)
+    its = {}
+    for recon in (1, 0):
+        assert q.set_opts(prec_sloppy=16, recon_long=recon) == 0
+        ia = QOP_invert_arg_t(1e9, 20000, 20000, 5, 0)
+        ra = QOP_resid_arg_t(1e-20, 0, 0, 0, 0, 0)
+        hin, hout = q.create_V(src), q.create_V(np.zeros_like(src))
+        q.invert(fla, 0.05, hout, hin, ia, ra)
+        assert eo_residual(fo, 0.05, q.extract_V(hout, V), src, L, 0) <= 1.05e-20
+        its[recon] = ra.final_iter
+        q.destroy_V(hin)
+        q.destroy_V(hout)
+    q.set_opts(prec_sloppy=64, recon_long=1)
+    assert its[1] <= 1.1 * its[0] + 10, its
+    q.destroy_L(fla)
+
+
+def _run_multi(q, fla, masses, srcs, rsq, guess=None):
+    V = srcs[0].shape[0]
+    ras = [[QOP_resid_arg_t(rsq, 0, 0, 0, 0, 0) for _ in ms] for ms in masses]
+    hins = [q.create_V(s) for s in srcs]
+    houts = [[q.create_V(np.zeros_like(srcs[0]) if guess is None else guess) for _ in ms] for ms in masses]
+    ia = QOP_invert_arg_t(1e9, 20000, 20000, 20, 0)
+    info = q.invert_multi(fla, masses, houts, hins, ia, ras)
+    outs = [[q.extract_V(h, V) for h in row] for row in houts]
+    for h in hins:
+        q.destroy_V(h)
+    for row in houts:
+        for h in row:
+            q.destroy_V(h)
+    return info, ras, outs
+
+
+@pytest.mark.parametrize("prec", [16, 32])
+def test_mixed_multi_mass(prec):
+    """Several masses per source (EVEN parity): the sloppy multi-shift CG plus
+    per-mass refinement meets every FP64 tolerance, reports the true
+    residual, and agrees with the oracle's single-mass solves."""
+    L = (8, 8, 8, 8)
+    q = gpu_lattice(L, "D")
+    fat, lng, _, _ = hisq_links(L, 0.5, 9)
+    fo = O.Fla(O.Lattice(L), fat, lng)
+    fla = q.create_L_from_raw(fat, lng)
+    rsq = 1e-20
+    masses = [[0.02, 0.05, 0.1, 0.3, 1.0], [0.2, 0.04]]
+    srcs = [LT.gaussian_vector(L, 310 + s) for s in range(2)]
+    assert q.set_opts(prec_sloppy=prec) == 0
+    info, ras, outs = _run_multi(q, fla, masses, srcs, rsq)
+    assert q.set_opts(prec_sloppy=64) == 0
+    assert info.status == 0
+    for s, ms in enumerate(masses):
+        for j, m in enumerate(ms):
+            true = eo_residual(fo, m, outs[s][j], srcs[s], L, 0)
+            assert true <= rsq * 1.05, (s, m, true)
+            assert abs(ras[s][j].final_rsq - true) <= 0.05 * true + 1e-26
+            ref, _ = fo.invert(m, srcs[s], O.InvertArg(1e9, 20000, 20000, 5, 0), O.ResidArg(rsq, 0, 0, 0, 0, 0))
+            assert rel_norm_err(half(outs[s][j], L, 0), half(ref, L, 0)) <= max(1e-6, 30 * np.sqrt(rsq) / m ** 2)
+    q.destroy_L(fla)
+
+
+def test_mixed_multi_mass_iterations():
+    """One multi-mass solve costs fewer iterations than the separate
+    single-mass solves it replaces; a non-zero starting guess skips the
+    multi-shift phase and still converges."""
+    L = (8, 8, 8, 8)
+    V = int(np.prod(L))
+    q = gpu_lattice(L, "D")
+    fat, lng, _, _ = hisq_links(L, 0.5, 9)
+    fo = O.Fla(O.Lattice(L), fat, lng)
+    fla = q.create_L_from_raw(fat, lng)
+    rsq = 1e-20
+    ms = [0.01, 0.03, 0.1, 0.3]
+    src = LT.gaussian_vector(L, 320)
+    assert q.set_opts(prec_sloppy=16) == 0
+    _, ras, _ = _run_multi(q, fla, [ms], [src], rsq)
+    multi = ras[0][0].final_iter
+    sep = 0
+    for m in ms:
+        _, r1, _ = _run_multi(q, fla, [[m]], [src], rsq)
+        sep += r1[0][0].final_iter
+    guess = LT.gaussian_vector(L, 321) * 1e-3
+    _, rg, og = _run_multi(q, fla, [ms], [src], rsq, guess=guess)
+    assert q.set_opts(prec_sloppy=64) == 0
+    print("multi-mass iterations", multi, "separate", sep, "with guess", rg[0][0].final_iter)
+    assert multi < 0.9 * sep, (multi, sep)
+    for j, m in enumerate(ms):
+        assert eo_residual(fo, m, og[0][j], src, L, 0) <= rsq * 1.05
+    q.destroy_L(fla)
