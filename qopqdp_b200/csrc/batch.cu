@@ -1,0 +1,393 @@
+// batch.cu -- several independent systems A_j x_j = b_j, A_j = m_j^2 - D_eo D_oe
+// on one parity, solved together (B200 addition; the reference solves the
+// systems of QOP_asqtad_invert_multi one restart at a time,
+// lib/asqtad_invert_p.c:332-647).
+//
+// Each system runs its own reduced-precision reliable-update CG (int16
+// links and site vectors, FP32 arithmetic, FP64 scalars and reductions,
+// FP64 true-residual updates; the single-system method of mixed.cu), but the
+// hop kernel reads every link once for all systems of a launch: the link
+// stream (576-672 bytes per site) is shared, each system adds only its
+// 16-byte input and output sites.  With 16 systems a hop moves ~1.1 KB per
+// site instead of 16 x 0.6 KB, and the kernel becomes bound by FP32 issue
+// rather than HBM.
+//
+// One iteration for all systems is four launches:
+//   K1  t_j  = D_oe p_j                 (shared links; sums |t_j|^2)
+//   K2  Ap_j = m_j^2 p_j - D_eo t_j     (shared links; sums |p_j|^2 -> alpha_j)
+//   K3  x_j += alpha_j p_j, r_j -= alpha_j Ap_j   (|r_j|^2 -> beta_j, update test)
+//   K4  p_j = r_j + beta_j p_j
+// A system whose state flag is set (update requested, breakdown, converged)
+// is skipped by every kernel; the host serves reliable updates between
+// chunks of `chunk` iterations and retires converged systems.  The decode
+// and arithmetic of a slot are those of the single-system int16 hop, so a
+// system takes the same iterations alone or in a batch.
+#include "solvers.cuh"
+#include "reduce.cuh"
+#include "dslash.cuh"
+#include "prof.cuh"
+#include "fields.cuh"
+#include "mixed.cuh"
+#include <algorithm>
+#include <vector>
+#include <cmath>
+
+namespace qopb {
+
+constexpr int BG = 4;        // systems per thread (and per block) in the hop
+enum { MIX_DONE = 4 };
+
+// link of one slot decoded to integer units; returns the factor that scales them
+__device__ __forceinline__ float q16_link(const uint4 ua, const uint4 ub, const uint2 uc, float2 U[9]) {
+  U[0] = make_float2(u16_lo(ua.x), u16_hi(ua.x)); U[1] = make_float2(u16_lo(ua.y), u16_hi(ua.y));
+  U[2] = make_float2(u16_lo(ua.z), u16_hi(ua.z)); U[3] = make_float2(u16_lo(ua.w), u16_hi(ua.w));
+  U[4] = make_float2(u16_lo(ub.x), u16_hi(ub.x)); U[5] = make_float2(u16_lo(ub.y), u16_hi(ub.y));
+  U[6] = make_float2(u16_lo(ub.z), u16_hi(ub.z)); U[7] = make_float2(u16_lo(ub.w), u16_hi(ub.w));
+  U[8] = make_float2(u16_lo(uc.x), u16_hi(uc.x));
+  return __uint_as_float(uc.y) * (1.0f / 32767.0f);
+}
+
+// long link stored as two rows (units of |c|/32767) + det phase; row 2 is
+// det * conj(row0 x row1), brought to the same units
+__device__ __forceinline__ float q16_link_recon(const uint4 ua, const uint2 ub, const float phase, const float cl,
+                                                float2 U[9]) {
+  U[0] = make_float2(u16_lo(ua.x), u16_hi(ua.x)); U[1] = make_float2(u16_lo(ua.y), u16_hi(ua.y));
+  U[2] = make_float2(u16_lo(ua.z), u16_hi(ua.z)); U[3] = make_float2(u16_lo(ua.w), u16_hi(ua.w));
+  U[4] = make_float2(u16_lo(ub.x), u16_hi(ub.x)); U[5] = make_float2(u16_lo(ub.y), u16_hi(ub.y));
+  float sn, cs;
+  __sincosf(phase, &sn, &cs);
+  const float2 z = make_float2(cs * (1.0f / 32767.0f), sn * (1.0f / 32767.0f));
+  const float2 c0 = csub<float>(cmul<float>(U[1], U[5]), cmul<float>(U[2], U[4]));
+  const float2 c1 = csub<float>(cmul<float>(U[2], U[3]), cmul<float>(U[0], U[5]));
+  const float2 c2 = csub<float>(cmul<float>(U[0], U[4]), cmul<float>(U[1], U[3]));
+  U[6] = cmul<float>(z, make_float2(c0.x, -c0.y));
+  U[7] = cmul<float>(z, make_float2(c1.x, -c1.y));
+  U[8] = cmul<float>(z, make_float2(c2.x, -c2.y));
+  return cl * (1.0f / 32767.0f);
+}
+
+// Blocks are (site block sb, system group grp) flattened with the group
+// fastest, so the blocks that share a site block's links run together and
+// the links come from HBM once.  Vectors are [system][Vh] int16 sites.
+template <int NL, int KIND, bool RECON>
+__global__ void __launch_bounds__(QB)
+k_bhop(uint4 *__restrict__ out, const uint4 *__restrict__ src, const unsigned char *__restrict__ lk,
+       const uint4 *__restrict__ same, Geom g, NbrGeom ng, int p, MixState *st, int nsys, int ngrp, double *part,
+       unsigned *count, float c_long) {
+  const int grp = blockIdx.x % ngrp, sb = blockIdx.x / ngrp, nsb = gridDim.x / ngrp;
+  const int tid = threadIdx.x;
+  const i64 Vh = g.Vh;
+  const int i = sb * QB + tid;
+  const int j0 = grp * BG;
+  bool act[BG];
+  bool any = false;
+#pragma unroll
+  for (int b = 0; b < BG; b++) {
+    act[b] = (j0 + b < nsys) && st[j0 + b].flag == 0;
+    any = any || act[b];
+  }
+  if (!any) return;   // uniform over the group: no block of it reduces
+  double acc[BG];
+#pragma unroll
+  for (int b = 0; b < BG; b++) acc[b] = 0.0;
+  if (i < Vh) {
+    int x[4];
+    site_coords(g, i, p, x);
+    const int lex = ((x[0] * g.L[1] + x[1]) * g.L[2] + x[2]) * g.L[3] + x[3];
+    float2 a[BG][3];
+#pragma unroll
+    for (int b = 0; b < BG; b++) a[b][0] = a[b][1] = a[b][2] = make_float2(0.f, 0.f);
+    const unsigned char *gl = lk + (size_t)sb * q16_block_bytes(NL, RECON);
+#pragma unroll
+    for (int k = 0; k < NL; k++) {
+      const unsigned char *ls = gl + q16_slot_off(k, RECON);
+      float2 U[9];
+      float sl;
+      if (RECON && (k & 1)) {
+        const uint4 ua = __ldcs(reinterpret_cast<const uint4 *>(ls) + tid);
+        const uint2 ub = __ldcs(reinterpret_cast<const uint2 *>(ls + 16 * QB) + tid);
+        const float ph = __ldcs(reinterpret_cast<const float *>(ls + 24 * QB) + tid);
+        sl = q16_link_recon(ua, ub, ph, c_long, U);
+      } else {
+        const uint4 ua = __ldcs(reinterpret_cast<const uint4 *>(ls) + tid);
+        const uint4 ub = __ldcs(reinterpret_cast<const uint4 *>(ls + 16 * QB) + tid);
+        const uint2 uc = __ldcs(reinterpret_cast<const uint2 *>(ls + 32 * QB) + tid);
+        sl = q16_link(ua, ub, uc, U);
+      }
+      const int nbi = nbr_fast(ng, x, lex, slot_mu<NL>(k), slot_disp<NL>(k));
+      uint4 nb[BG];
+#pragma unroll
+      for (int b = 0; b < BG; b++) nb[b] = act[b] ? src[(i64)(j0 + b) * Vh + nbi] : make_uint4(0, 0, 0, 0);
+#pragma unroll
+      for (int b = 0; b < BG; b++) {
+        if (!act[b]) continue;
+        float2 v[3];
+        const float sc = sl * SpQ16::raw(nb[b], v);
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+          float2 t = make_float2(0.f, 0.f);
+          cfmaf(t, U[3 * r], v[0]);
+          cfmaf(t, U[3 * r + 1], v[1]);
+          cfmaf(t, U[3 * r + 2], v[2]);
+          a[b][r].x = fmaf(sc, t.x, a[b][r].x);
+          a[b][r].y = fmaf(sc, t.y, a[b][r].y);
+        }
+      }
+    }
+#pragma unroll
+    for (int b = 0; b < BG; b++) {
+      if (!act[b]) continue;
+      const i64 o = (i64)(j0 + b) * Vh;
+      if (KIND == 1) {
+        acc[b] = (double)a[b][0].x * a[b][0].x + (double)a[b][0].y * a[b][0].y + (double)a[b][1].x * a[b][1].x +
+                 (double)a[b][1].y * a[b][1].y + (double)a[b][2].x * a[b][2].x + (double)a[b][2].y * a[b][2].y;
+        SpQ16::store(out + o, i, Vh, a[b]);
+      } else {
+        const float m2 = (float)st[j0 + b].m2;
+        float2 sv[3];
+        SpQ16::load(same + o, i, Vh, sv);
+#pragma unroll
+        for (int c = 0; c < 3; c++) a[b][c] = make_float2(m2 * sv[c].x - a[b][c].x, m2 * sv[c].y - a[b][c].y);
+        SpQ16::store(out + o, i, Vh, a[b]);
+        acc[b] = (double)sv[0].x * sv[0].x + (double)sv[0].y * sv[0].y + (double)sv[1].x * sv[1].x +
+                 (double)sv[1].y * sv[1].y + (double)sv[2].x * sv[2].x + (double)sv[2].y * sv[2].y;
+      }
+    }
+  }
+  __shared__ double res[BG];
+  if (group_sum<BG>(acc, part + (size_t)grp * nsb * BG, count + grp, res, sb, nsb)) {
+#pragma unroll
+    for (int b = 0; b < BG; b++) {
+      if (!act[b]) continue;
+      MixState *s = st + j0 + b;
+      if (KIND == 1) {
+        s->dp2 = res[b];
+      } else {
+        const double pAp = s->dp2 + s->m2 * res[b];   // <p, A p> = |D p|^2 + m^2 |p|^2
+        if (!(pAp > 0)) s->flag = MIX_BREAK;
+        else s->alpha = s->rsq / pAp;
+      }
+    }
+  }
+}
+
+// x_j += alpha_j p_j, r_j -= alpha_j Ap_j, |r_j|^2: blockIdx.y = system
+__global__ void __launch_bounds__(256)
+k_bupdate(float2 *__restrict__ xs, uint4 *__restrict__ r, const uint4 *__restrict__ p, const uint4 *__restrict__ Ap,
+          i64 Vh, MixState *st, double *part, unsigned *count) {
+  const int j = blockIdx.y;
+  MixState *s = st + j;
+  if (s->flag) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const i64 o = (i64)j * Vh;
+  float2 *xj = xs + 3 * o;
+  double acc1[1] = {0.0};
+  if (i < Vh) {
+    const float al = (float)s->alpha;
+    float2 pv[3], av[3], rv[3];
+    SpQ16::load(p + o, i, Vh, pv);
+    SpQ16::load(Ap + o, i, Vh, av);
+    SpQ16::load(r + o, i, Vh, rv);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      float2 xv = xj[c * Vh + i];
+      xv.x = fmaf(al, pv[c].x, xv.x);
+      xv.y = fmaf(al, pv[c].y, xv.y);
+      xj[c * Vh + i] = xv;
+      rv[c].x = fmaf(-al, av[c].x, rv[c].x);
+      rv[c].y = fmaf(-al, av[c].y, rv[c].y);
+    }
+    SpQ16::store(r + o, i, Vh, rv);
+    acc1[0] = (double)rv[0].x * rv[0].x + (double)rv[0].y * rv[0].y + (double)rv[1].x * rv[1].x +
+              (double)rv[1].y * rv[1].y + (double)rv[2].x * rv[2].x + (double)rv[2].y * rv[2].y;
+  }
+  if (grid_sum<1>(acc1, part + (size_t)j * gridDim.x, count + j, &s->red)) {
+    const double rn = s->red;
+    s->iter += 1;
+    s->rsq_old = s->rsq;
+    s->rsq = rn;
+    s->beta = rn / s->rsq_old;
+    if (rn > s->maxr2) s->maxr2 = rn;
+    if (rn < s->delta2 * s->maxr2 || rn <= s->stop || s->iter >= s->max_iter) s->flag = MIX_UPDATE;
+  }
+}
+
+// p_j = r_j + beta_j p_j: blockIdx.y = system
+__global__ void __launch_bounds__(256)
+k_bp(uint4 *__restrict__ p, const uint4 *__restrict__ r, i64 Vh, const MixState *st) {
+  const int j = blockIdx.y;
+  if (st[j].flag) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= Vh) return;
+  const i64 o = (i64)j * Vh;
+  const float be = (float)st[j].beta;
+  float2 pv[3], rv[3];
+  SpQ16::load(p + o, i, Vh, pv);
+  SpQ16::load(r + o, i, Vh, rv);
+#pragma unroll
+  for (int c = 0; c < 3; c++) pv[c] = make_float2(fmaf(be, pv[c].x, rv[c].x), fmaf(be, pv[c].y, rv[c].y));
+  SpQ16::store(p + o, i, Vh, pv);
+}
+
+template <int KIND>
+static void launch_bhop(int nl, bool recon, int ngrp, int nsb, uint4 *out, const uint4 *src,
+                        const unsigned char *lk, const uint4 *same, const Geom &g, const NbrGeom &ng, int par,
+                        MixState *st, int nsys, double *part, unsigned *count, float c_long) {
+  Context &c = ctx();
+  const int grid = ngrp * nsb;
+#define BH_ARGS out, src, lk, same, g, ng, par, st, nsys, ngrp, part, count, c_long
+  if (nl != 16) k_bhop<8, KIND, false><<<grid, QB, 0, c.s>>>(BH_ARGS);
+  else if (recon) k_bhop<16, KIND, true><<<grid, QB, 0, c.s>>>(BH_ARGS);
+  else k_bhop<16, KIND, false><<<grid, QB, 0, c.s>>>(BH_ARGS);
+#undef BH_ARGS
+}
+
+void run_batch(FlaT<double> *f, int eo, int n, const double *mass, c2<double> **x, c2<double> *const *b,
+               const double *rsqmin, int max_iter, int *iters, double *final_rsq) {
+  Context &c = ctx();
+  const Geom &g = c.g;
+  const i64 Vh = g.Vh;
+  const int p = eo, q = 1 - eo;
+  const Range is = vrange(g, eo);
+  if (n < 1) return;
+  if (n > BATCH_MAX) fail(QOP_FAIL, "run_batch: %d systems exceed the batch limit %d", n, BATCH_MAX);
+  SloppyLinks *sl = sloppy_get(f, LK_Q16);
+  const LinksSloppy lk_p = links_parity(sl, LK_Q16, p), lk_q = links_parity(sl, LK_Q16, q);
+  const int ngrp = (n + BG - 1) / BG, nsb = (int)((Vh + QB - 1) / QB), gridv = grid_for(Vh, 256);
+  const int nl = sl->nl;
+  const bool recon = sl->recon != 0;
+  const float c_long = (float)sl->c_long;
+  NbrGeom ng;
+  for (int d = 0; d < 4; d++) ng.L[d] = g.L[d];
+  ng.str[3] = 1; ng.str[2] = g.L[3]; ng.str[1] = g.L[2] * g.L[3]; ng.str[0] = g.L[1] * g.L[2] * g.L[3];
+
+  uint4 *rs = dalloc<uint4>(n * Vh), *ps = dalloc<uint4>(n * Vh), *Aps = dalloc<uint4>(n * Vh),
+        *ts = dalloc<uint4>(n * Vh);
+  float2 *xs = dalloc<float2>(3 * n * Vh);
+  dzero(xs, sizeof(float2) * 3 * n * Vh);
+  c2<double> *r = dalloc<c2<double>>(vec_elems(g)), *Ax = dalloc<c2<double>>(vec_elems(g));
+  c2<double> *tmp = dalloc<c2<double>>(vec_elems(g));
+  const size_t npart = std::max<size_t>((size_t)ngrp * nsb * BG, (size_t)n * gridv);
+  double *part = dalloc<double>(npart);
+  const int ncount = std::max(ngrp, n);
+  unsigned *count = dalloc<unsigned>(ncount);
+  dzero(count, sizeof(unsigned) * ncount);
+  MixState *dst = dalloc<MixState>(n);
+  std::vector<MixState> h(n);
+  std::vector<double> b2(n), r2(n);
+  std::vector<int> nru(n, 0), stalls(n, 0), last_iter(n, 0);
+  auto release = [&]() {
+    dfree(rs); dfree(ps); dfree(Aps); dfree(ts); dfree(xs); dfree(r); dfree(Ax); dfree(tmp);
+    dfree(part); dfree(count); dfree(dst);
+  };
+  // FP64 true residual b_j - A_j x_j into r; returns its norm^2
+  auto true_resid = [&](int j) {
+    LinOp<double> L{f, mass[j], eo, tmp};
+    L.d2(Ax, x[j]);
+    Blas<double>::axpby(r, 1.0, b[j], -1.0, Ax, is);
+    return Blas<double>::norm2(r, is);
+  };
+  const double delta2 = c.opt.ru_delta * c.opt.ru_delta;
+  int active = 0;
+  for (int j = 0; j < n; j++) {
+    b2[j] = Blas<double>::norm2(b[j], is);
+    MixState &s = h[j];
+    s = MixState{};
+    s.stop = rsqmin[j] * b2[j];
+    s.delta2 = delta2;
+    s.m2 = mass[j] * mass[j];
+    s.max_iter = max_iter;
+    if (b2[j] == 0.0) Blas<double>::zero(x[j], is);
+    r2[j] = b2[j] == 0.0 ? 0.0 : true_resid(j);
+    if (b2[j] == 0.0 || r2[j] <= s.stop) {
+      s.flag = MIX_DONE;
+      continue;
+    }
+    k_to_sloppy<SpQ16><<<gridv, 256, 0, c.s>>>(rs + j * Vh, r + is.off, Vh);
+    k_copy_elems<uint4><<<grid_for(Vh, 256), 256, 0, c.s>>>(ps + j * Vh, rs + j * Vh, Vh);
+    QLAUNCHN(2);
+    s.rsq = s.rsq_old = s.maxr2 = r2[j];
+    s.flag = MIX_RUN;
+    active++;
+  }
+  QCHECK(cudaMemcpyAsync(dst, h.data(), sizeof(MixState) * n, cudaMemcpyHostToDevice, c.s));
+  const int chunk = c.opt.chunk;
+  char hname[32];
+  snprintf(hname, sizeof hname, "bhop_q16_x%d", n);
+  const double link_site = recon ? (nl / 2) * (40.0 + 28.0) : nl * 40.0;
+  while (active > 0) {
+    // compulsory bytes of one hop for the systems running in this chunk
+    const double hop_bytes = (double)Vh * (link_site + 2.0 * 16 * active);
+    std::vector<int> recs;
+    for (int k = 0; k < chunk; k++) {
+      {
+        ProfScope s1(hname, hop_bytes);
+        launch_bhop<1>(nl, recon, ngrp, nsb, ts, ps, (const unsigned char *)lk_q.a, nullptr, g, ng, q, dst, n, part,
+                       count, c_long);
+        recs.push_back(s1.idx);
+      }
+      {
+        ProfScope s2(hname, hop_bytes + (double)Vh * 16 * active);
+        launch_bhop<2>(nl, recon, ngrp, nsb, Aps, ts, (const unsigned char *)lk_p.a, ps, g, ng, p, dst, n, part,
+                       count, c_long);
+        recs.push_back(s2.idx);
+      }
+      k_bupdate<<<dim3(gridv, n), 256, 0, c.s>>>(xs, rs, ps, Aps, Vh, dst, part, count);
+      k_bp<<<dim3(gridv, n), 256, 0, c.s>>>(ps, rs, Vh, dst);
+      QLAUNCHN(4);
+    }
+    QCHECK(cudaMemcpyAsync(h.data(), dst, sizeof(MixState) * n, cudaMemcpyDeviceToHost, c.s));
+    sync();
+    // drop timing records of hops that found every system idle
+    int most = 0;
+    for (int j = 0; j < n; j++) most = std::max(most, h[j].iter - last_iter[j] + (h[j].flag == MIX_BREAK ? 1 : 0));
+    for (size_t k = 2 * (size_t)most; k < recs.size(); k++) prof_discard(recs[k]);
+    std::vector<int> pupd;
+    for (int j = 0; j < n; j++) {
+      MixState &s = h[j];
+      const int ran = s.iter - last_iter[j];
+      last_iter[j] = s.iter;
+      if (s.flag != MIX_UPDATE && s.flag != MIX_BREAK) continue;
+      stalls[j] = ran == 0 ? stalls[j] + 1 : 0;   // repeated breakdown without progress
+      // reliable update: fold the sloppy solution into FP64, true residual
+      k_fold_x<<<grid_for(3 * Vh, 256), 256, 0, c.s>>>(x[j] + is.off, xs + 3 * j * Vh, 3 * Vh);
+      QLAUNCH();
+      r2[j] = true_resid(j);
+      nru[j]++;
+      log0(QOP_VERB_MED, "BATCHCG[%d/%d]: iter %d sloppy rsq %g true rsq %g (stop %g)\n", j, n, s.iter, s.rsq, r2[j],
+           s.stop);
+      if (r2[j] <= s.stop || s.iter + nru[j] >= s.max_iter || stalls[j] > 2) {
+        s.flag = MIX_DONE;
+        active--;
+        continue;
+      }
+      const bool broke = s.flag == MIX_BREAK || !(s.rsq_old > 0);
+      const double rsq_prev = s.rsq_old;
+      k_to_sloppy<SpQ16><<<gridv, 256, 0, c.s>>>(rs + j * Vh, r + is.off, Vh);
+      QLAUNCH();
+      s.rsq = r2[j];
+      s.maxr2 = r2[j];
+      s.flag = MIX_RUN;
+      if (broke) {   // restart the recursion from the true residual
+        k_copy_elems<uint4><<<grid_for(Vh, 256), 256, 0, c.s>>>(ps + j * Vh, rs + j * Vh, Vh);
+        QLAUNCH();
+      } else {
+        s.beta = r2[j] / rsq_prev;
+        pupd.push_back(j);
+      }
+    }
+    QCHECK(cudaMemcpyAsync(dst, h.data(), sizeof(MixState) * n, cudaMemcpyHostToDevice, c.s));
+    for (int j : pupd) {
+      k_bp<<<dim3(gridv, 1), 256, 0, c.s>>>(ps + j * Vh, rs + j * Vh, Vh, dst + j);
+      QLAUNCH();
+    }
+  }
+  for (int j = 0; j < n; j++) {
+    iters[j] = h[j].iter + nru[j];
+    final_rsq[j] = b2[j] > 0 ? r2[j] / b2[j] : 0.0;
+  }
+  release();
+  sync();
+}
+
+}  // namespace qopb

@@ -188,7 +188,8 @@ int QOP_sites_on_node_raw_V(QOP_evenodd_t eo) { (void)eo; return (int)ctx().g.V;
 int QOP_sites_on_node_raw_G(QOP_evenodd_t eo) { (void)eo; return (int)ctx().g.V; }
 
 // tags: st, ns, nm, cg, eigcg_nev, eigcg_m, eigcg_l (reference) and
-// prec_sloppy (64|32|16), ru_delta, chunk (B200 additions)
+// prec_sloppy (64|32|16), half_format, hop_kernel, recon_long, multi_shift,
+// ru_delta, chunk (B200 additions)
 QOP_status_t QOP_asqtad_invert_set_opts(QOP_opt_t opts[], int nopts) {
   Options &o = ctx().opt;
   int st = o.style, ns = o.nsvec, nm = o.nvec;
@@ -213,6 +214,8 @@ QOP_status_t QOP_asqtad_invert_set_opts(QOP_opt_t opts[], int nopts) {
       int p = (int)v;
       if (p != 16 && p != 32 && p != 64) return QOP_FAIL;
       n.sloppy_prec = p;
+    } else if (!strcmp(t, "multi_shift")) {
+      n.multi_shift = v != 0;
     } else if (!strcmp(t, "recon_long")) {
       n.recon_long = v != 0;
     } else if (!strcmp(t, "hop_kernel")) {

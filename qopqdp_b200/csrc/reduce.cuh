@@ -42,17 +42,20 @@ __device__ inline void block_sum(double (&v)[N]) {
 
 // called by every thread of every block with its private accumulators;
 // the last block writes the grid total to res[0..N-1] and returns true in
-// thread 0 so that a caller may run a scalar epilogue there
+// thread 0 so that a caller may run a scalar epilogue there.  `bid` / `nb`
+// name the block within the set of blocks that reduce together (several
+// independent reductions may share one launch, each with its own partials
+// and ticket).
 template <int N>
-__device__ inline bool grid_sum(double (&v)[N], double *part, unsigned *count, double *res) {
+__device__ inline bool group_sum(double (&v)[N], double *part, unsigned *count, double *res, int bid, int nb) {
   block_sum<N>(v);
   __shared__ bool am_last;
   if (threadIdx.x == 0) {
 #pragma unroll
-    for (int k = 0; k < N; k++) part[blockIdx.x * N + k] = v[k];
+    for (int k = 0; k < N; k++) part[bid * N + k] = v[k];
     __threadfence();
     unsigned t = atomicAdd(count, 1u);
-    am_last = (t == gridDim.x - 1);
+    am_last = (t == (unsigned)nb - 1);
   }
   __syncthreads();
   if (!am_last) return false;
@@ -60,7 +63,7 @@ __device__ inline bool grid_sum(double (&v)[N], double *part, unsigned *count, d
   double s[N];
 #pragma unroll
   for (int k = 0; k < N; k++) s[k] = 0.0;
-  for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x)
+  for (int b = threadIdx.x; b < nb; b += blockDim.x)
 #pragma unroll
     for (int k = 0; k < N; k++) s[k] += __ldcg(part + b * N + k);
   block_sum<N>(s);
@@ -71,6 +74,11 @@ __device__ inline bool grid_sum(double (&v)[N], double *part, unsigned *count, d
     return true;
   }
   return false;
+}
+
+template <int N>
+__device__ inline bool grid_sum(double (&v)[N], double *part, unsigned *count, double *res) {
+  return group_sum<N>(v, part, count, res, blockIdx.x, gridDim.x);
 }
 
 // grid size for reductions: fixed per element count so the order is fixed

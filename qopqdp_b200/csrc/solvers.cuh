@@ -37,6 +37,15 @@ void invert_multi(QOP_info_t *info, FlaT<T> *f, QOP_invert_arg_t *ia, QOP_resid_
 // base system.  Returns false when the path is not applicable.
 bool mixed_cgms(LinOp<double> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t **ra, const double *shifts, int ns,
                 c2<double> **out, const c2<double> *in, int eo, int prec);
+// Independent systems (m_j^2 - D D) x_j = b_j on parity eo, solved
+// together with int16 storage and one link stream per hop (batch.cu).  x_j
+// holds the starting guess on entry and the solution on return; rsqmin_j is
+// the target on |b_j - A_j x_j|^2 / |b_j|^2.  Returns per system its
+// iteration count (hop pairs plus reliable updates) and the final FP64
+// |r|^2 / |b|^2.
+constexpr int BATCH_MAX = 16;
+void run_batch(FlaT<double> *f, int eo, int n, const double *mass, c2<double> **x, c2<double> *const *b,
+               const double *rsqmin, int max_iter, int *iters, double *final_rsq);
 // several masses on one parity with prec_sloppy < 64: reduced-precision
 // multi-shift CG per shared source, then per-solve refinement
 void solve_multi_mixed(QOP_info_t *info, FlaT<double> *f, QOP_invert_arg_t *ia, QOP_resid_arg_t **ra,

@@ -145,12 +145,13 @@ def test_mixed_multi_mass(prec):
     q.destroy_L(fla)
 
 
-def test_mixed_multi_mass_iterations():
-    """One multi-mass solve costs fewer iterations than the separate
-    single-mass solves it replaces; a non-zero starting guess skips the
-    multi-shift phase and still converges."""
+@pytest.mark.parametrize("multi_shift", [0, 1])
+def test_mixed_multi_mass_iterations(multi_shift):
+    """int16 multi-mass solves: batched (every system keeps the iteration
+    count of its own single-mass solve) or multi-shift first (fewer
+    iterations than the separate solves together); a non-zero starting
+    guess converges too."""
     L = (8, 8, 8, 8)
-    V = int(np.prod(L))
     q = gpu_lattice(L, "D")
     fat, lng, _, _ = hisq_links(L, 0.5, 9)
     fo = O.Fla(O.Lattice(L), fat, lng)
@@ -158,18 +159,66 @@ def test_mixed_multi_mass_iterations():
     rsq = 1e-20
     ms = [0.01, 0.03, 0.1, 0.3]
     src = LT.gaussian_vector(L, 320)
-    assert q.set_opts(prec_sloppy=16) == 0
+    assert q.set_opts(prec_sloppy=16, multi_shift=multi_shift) == 0
     _, ras, _ = _run_multi(q, fla, [ms], [src], rsq)
-    multi = ras[0][0].final_iter
-    sep = 0
+    its = [r.final_iter for r in ras[0]]
+    sep = []
     for m in ms:
         _, r1, _ = _run_multi(q, fla, [[m]], [src], rsq)
-        sep += r1[0][0].final_iter
+        sep.append(r1[0][0].final_iter)
     guess = LT.gaussian_vector(L, 321) * 1e-3
     _, rg, og = _run_multi(q, fla, [ms], [src], rsq, guess=guess)
-    assert q.set_opts(prec_sloppy=64) == 0
-    print("multi-mass iterations", multi, "separate", sep, "with guess", rg[0][0].final_iter)
-    assert multi < 0.9 * sep, (multi, sep)
+    assert q.set_opts(prec_sloppy=64, multi_shift=0) == 0
+    print("multi-mass iterations", its, "separate", sep, "with guess", [r.final_iter for r in rg[0]])
+    if multi_shift:
+        assert max(its) < 0.9 * sum(sep), (its, sep)
+    else:
+        for a, b in zip(its, sep):
+            assert abs(a - b) <= 0.05 * b + 5, (its, sep)
     for j, m in enumerate(ms):
         assert eo_residual(fo, m, og[0][j], src, L, 0) <= rsq * 1.05
+    q.destroy_L(fla)
+
+
+@pytest.mark.parametrize("L,kind", [((8, 8, 8, 8), "asqtad"), ((4, 4, 4, 8), "hisq")])
+def test_mixed_multi_source(L, kind):
+    """Many sources, one mass each (some masses repeated, one zero source),
+    odd parity: the batched int16 solver meets every FP64 tolerance, returns
+    m A^{-1} b like the oracle, and a zero source gives a zero solution."""
+    V = int(np.prod(L))
+    q = gpu_lattice(L, "D")
+    if kind == "asqtad":
+        fat, lng = asqtad_links(L, 0.4, 11)
+    else:
+        fat, lng, _, _ = hisq_links(L, 0.5, 9)
+    fo = O.Fla(O.Lattice(L), fat, lng)
+    fla = q.create_L_from_raw(fat, lng)
+    rsq = 1e-18
+    nsrc = 6
+    srcs = [LT.gaussian_vector(L, 400 + s) for s in range(nsrc - 1)]
+    srcs.append(np.zeros_like(srcs[0]))
+    masses = [[0.03], [0.03], [0.05], [0.08], [0.2], [0.05]]
+    assert q.set_opts(prec_sloppy=16) == 0
+    ras = [[QOP_resid_arg_t(rsq, 0, 0, 0, 0, 0)] for _ in range(nsrc)]
+    hins = [q.create_V(s) for s in srcs]
+    houts = [[q.create_V(np.zeros_like(srcs[0]))] for _ in range(nsrc)]
+    ia = QOP_invert_arg_t(1e9, 20000, 20000, 20, 1)
+    info = q.invert_multi(fla, masses, houts, hins, ia, ras)
+    assert q.set_opts(prec_sloppy=64) == 0
+    assert info.status == 0
+    for s in range(nsrc):
+        got = q.extract_V(houts[s][0], V)
+        m = masses[s][0]
+        if s == nsrc - 1:
+            assert np.all(half(got, L, 1) == 0) and ras[s][0].final_rsq == 0
+            continue
+        true = eo_residual(fo, m, got, srcs[s], L, 1)
+        assert true <= rsq * 1.05, (s, true)
+        assert abs(ras[s][0].final_rsq - true) <= 0.05 * true + 1e-26
+        ref, _ = fo.invert(m, srcs[s], O.InvertArg(1e9, 20000, 20000, 5, 1), O.ResidArg(rsq, 0, 0, 0, 0, 0))
+        assert rel_norm_err(half(got, L, 1), half(ref, L, 1)) <= max(1e-6, 30 * np.sqrt(rsq) / m ** 2)
+    for h in hins:
+        q.destroy_V(h)
+    for row in houts:
+        q.destroy_V(row[0])
     q.destroy_L(fla)
