@@ -25,7 +25,7 @@ typedef struct {
   char name[32];            /* kernel class, e.g. "hop_f16_r13"           */
   int launches;             /* launches recorded                          */
   double total_ms;          /* summed device time of those launches       */
-  double bytes_per_launch;  /* algorithmic (compulsory) bytes per launch  */
+  double bytes_per_launch;  /* mean algorithmic (compulsory) bytes per launch */
 } QOPB_kstat_t;
 int QOPB_prof_begin(void);
 int QOPB_prof_end(QOPB_kstat_t *out, int max);

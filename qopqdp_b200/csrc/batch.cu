@@ -34,7 +34,6 @@
 
 namespace qopb {
 
-constexpr int BG = 4;        // systems per thread (and per block) in the hop
 enum { MIX_DONE = 4 };
 
 // link of one slot decoded to integer units; returns the factor that scales them
@@ -69,8 +68,9 @@ __device__ __forceinline__ float q16_link_recon(const uint4 ua, const uint2 ub, 
 // Blocks are (site block sb, system group grp) flattened with the group
 // fastest, so the blocks that share a site block's links run together and
 // the links come from HBM once.  Vectors are [system][Vh] int16 sites.
-template <int NL, int KIND, bool RECON>
-__global__ void __launch_bounds__(QB)
+// BG systems per thread (and per block); MINB resident blocks per SM
+template <int NL, int KIND, bool RECON, int BG, int MINB>
+__global__ void __launch_bounds__(QB, MINB)
 k_bhop(uint4 *__restrict__ out, const uint4 *__restrict__ src, const unsigned char *__restrict__ lk,
        const uint4 *__restrict__ same, Geom g, NbrGeom ng, int p, MixState *st, int nsys, int ngrp, double *part,
        unsigned *count, float c_long) {
@@ -118,19 +118,30 @@ k_bhop(uint4 *__restrict__ out, const uint4 *__restrict__ src, const unsigned ch
       uint4 nb[BG];
 #pragma unroll
       for (int b = 0; b < BG; b++) nb[b] = act[b] ? src[(i64)(j0 + b) * Vh + nbi] : make_uint4(0, 0, 0, 0);
+      // packed FP32x2 FMAs (sm_100): t += (Re u, Re u)(v.x, v.y) + (-Im u, Im u)(v.y, v.x)
+      // rounds every lane exactly as the scalar complex FMA sequence does
+      float2 ur[9], ui[9];
+#pragma unroll
+      for (int e = 0; e < 9; e++) {
+        ur[e] = make_float2(U[e].x, U[e].x);
+        ui[e] = make_float2(-U[e].y, U[e].y);
+      }
 #pragma unroll
       for (int b = 0; b < BG; b++) {
         if (!act[b]) continue;
         float2 v[3];
         const float sc = sl * SpQ16::raw(nb[b], v);
+        const float2 sc2 = make_float2(sc, sc);
+        const float2 w[3] = {make_float2(v[0].y, v[0].x), make_float2(v[1].y, v[1].x), make_float2(v[2].y, v[2].x)};
 #pragma unroll
         for (int r = 0; r < 3; r++) {
           float2 t = make_float2(0.f, 0.f);
-          cfmaf(t, U[3 * r], v[0]);
-          cfmaf(t, U[3 * r + 1], v[1]);
-          cfmaf(t, U[3 * r + 2], v[2]);
-          a[b][r].x = fmaf(sc, t.x, a[b][r].x);
-          a[b][r].y = fmaf(sc, t.y, a[b][r].y);
+#pragma unroll
+          for (int c = 0; c < 3; c++) {
+            t = __ffma2_rn(ur[3 * r + c], v[c], t);
+            t = __ffma2_rn(ui[3 * r + c], w[c], t);
+          }
+          a[b][r] = __ffma2_rn(sc2, t, a[b][r]);
         }
       }
     }
@@ -229,17 +240,45 @@ k_bp(uint4 *__restrict__ p, const uint4 *__restrict__ r, i64 Vh, const MixState 
   SpQ16::store(p + o, i, Vh, pv);
 }
 
-template <int KIND>
-static void launch_bhop(int nl, bool recon, int ngrp, int nsb, uint4 *out, const uint4 *src,
-                        const unsigned char *lk, const uint4 *same, const Geom &g, const NbrGeom &ng, int par,
-                        MixState *st, int nsys, double *part, unsigned *count, float c_long) {
+// batched hop variants (option batch_kernel): systems per thread and the
+// register cap (resident blocks per SM).  At 32^4 with 16 systems a hop
+// takes 574 us with variant 1 (default), 605-679 us with 0, 2, 3, 5 and
+// 1074 us with 4 (8 systems per thread: 238 registers).  The kernel issues
+// ~60-90 instructions per system and slot and runs at ~55% issue
+// utilisation with 16-24 warps per SM; HBM traffic equals the compulsory
+// bytes (ncu), so it is instruction- and latency-bound, not HBM-bound.
+struct BhopShape { int bg, minb; };
+static const BhopShape kBhop[] = {{4, 1}, {4, 5}, {2, 8}, {2, 1}, {8, 1}, {4, 6}};
+constexpr int N_BHOP = (int)(sizeof(kBhop) / sizeof(kBhop[0]));
+
+template <int KIND, int BG, int MINB>
+static void launch_bhop_t(int nl, bool recon, int ngrp, int nsb, uint4 *out, const uint4 *src,
+                          const unsigned char *lk, const uint4 *same, const Geom &g, const NbrGeom &ng, int par,
+                          MixState *st, int nsys, double *part, unsigned *count, float c_long) {
   Context &c = ctx();
   const int grid = ngrp * nsb;
 #define BH_ARGS out, src, lk, same, g, ng, par, st, nsys, ngrp, part, count, c_long
-  if (nl != 16) k_bhop<8, KIND, false><<<grid, QB, 0, c.s>>>(BH_ARGS);
-  else if (recon) k_bhop<16, KIND, true><<<grid, QB, 0, c.s>>>(BH_ARGS);
-  else k_bhop<16, KIND, false><<<grid, QB, 0, c.s>>>(BH_ARGS);
+  if (nl != 16) k_bhop<8, KIND, false, BG, MINB><<<grid, QB, 0, c.s>>>(BH_ARGS);
+  else if (recon) k_bhop<16, KIND, true, BG, MINB><<<grid, QB, 0, c.s>>>(BH_ARGS);
+  else k_bhop<16, KIND, false, BG, MINB><<<grid, QB, 0, c.s>>>(BH_ARGS);
 #undef BH_ARGS
+}
+
+template <int KIND>
+static void launch_bhop(int variant, int nl, bool recon, int ngrp, int nsb, uint4 *out, const uint4 *src,
+                        const unsigned char *lk, const uint4 *same, const Geom &g, const NbrGeom &ng, int par,
+                        MixState *st, int nsys, double *part, unsigned *count, float c_long) {
+#define BH_CALL(B, M) launch_bhop_t<KIND, B, M>(nl, recon, ngrp, nsb, out, src, lk, same, g, ng, par, st, nsys, \
+                                                part, count, c_long)
+  switch (variant) {
+    case 1: BH_CALL(4, 5); break;
+    case 2: BH_CALL(2, 8); break;
+    case 3: BH_CALL(2, 1); break;
+    case 4: BH_CALL(8, 1); break;
+    case 5: BH_CALL(4, 6); break;
+    default: BH_CALL(4, 1); break;
+  }
+#undef BH_CALL
 }
 
 void run_batch(FlaT<double> *f, int eo, int n, const double *mass, c2<double> **x, c2<double> *const *b,
@@ -253,6 +292,7 @@ void run_batch(FlaT<double> *f, int eo, int n, const double *mass, c2<double> **
   if (n > BATCH_MAX) fail(QOP_FAIL, "run_batch: %d systems exceed the batch limit %d", n, BATCH_MAX);
   SloppyLinks *sl = sloppy_get(f, LK_Q16);
   const LinksSloppy lk_p = links_parity(sl, LK_Q16, p), lk_q = links_parity(sl, LK_Q16, q);
+  const int variant = std::min(std::max(c.opt.batch_kernel, 0), N_BHOP - 1), BG = kBhop[variant].bg;
   const int ngrp = (n + BG - 1) / BG, nsb = (int)((Vh + QB - 1) / QB), gridv = grid_for(Vh, 256);
   const int nl = sl->nl;
   const bool recon = sl->recon != 0;
@@ -322,13 +362,13 @@ void run_batch(FlaT<double> *f, int eo, int n, const double *mass, c2<double> **
     for (int k = 0; k < chunk; k++) {
       {
         ProfScope s1(hname, hop_bytes);
-        launch_bhop<1>(nl, recon, ngrp, nsb, ts, ps, (const unsigned char *)lk_q.a, nullptr, g, ng, q, dst, n, part,
+        launch_bhop<1>(variant, nl, recon, ngrp, nsb, ts, ps, (const unsigned char *)lk_q.a, nullptr, g, ng, q, dst, n, part,
                        count, c_long);
         recs.push_back(s1.idx);
       }
       {
         ProfScope s2(hname, hop_bytes + (double)Vh * 16 * active);
-        launch_bhop<2>(nl, recon, ngrp, nsb, Aps, ts, (const unsigned char *)lk_p.a, ps, g, ng, p, dst, n, part,
+        launch_bhop<2>(variant, nl, recon, ngrp, nsb, Aps, ts, (const unsigned char *)lk_p.a, ps, g, ng, p, dst, n, part,
                        count, c_long);
         recs.push_back(s2.idx);
       }

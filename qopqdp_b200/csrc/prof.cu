@@ -8,8 +8,8 @@
 namespace qopb {
 
 namespace {
-struct Cls { std::string name; double bytes; int launches = 0; double ms = 0; };
-struct Rec { int cls; cudaEvent_t a, b; };
+struct Cls { std::string name; double bytes = 0; int launches = 0; double ms = 0; };
+struct Rec { int cls; cudaEvent_t a, b; double bytes; };
 struct Prof {
   bool active = false;
   std::vector<Cls> cls;
@@ -38,15 +38,15 @@ int prof_start(const char *name, double bytes) {
   if (!g_prof.active || g_prof.recs.size() >= g_prof.cap) return -1;
   int c = -1;
   for (size_t i = 0; i < g_prof.cls.size(); i++)
-    if (g_prof.cls[i].name == name && g_prof.cls[i].bytes == bytes) { c = (int)i; break; }
+    if (g_prof.cls[i].name == name) { c = (int)i; break; }
   if (c < 0) {
-    g_prof.cls.push_back(Cls{name, bytes});
+    g_prof.cls.push_back(Cls{name});
     c = (int)g_prof.cls.size() - 1;
   }
   cudaEvent_t a = take_event(), b = take_event();
   if (!a || !b) return -1;
   cudaEventRecord(a, ctx().s);
-  g_prof.recs.push_back(Rec{c, a, b});
+  g_prof.recs.push_back(Rec{c, a, b, bytes});
   return (int)g_prof.recs.size() - 1;
 }
 
@@ -97,6 +97,7 @@ extern "C" int QOPB_prof_end(QOPB_kstat_t *out, int max) {
     if (cudaEventElapsedTime(&ms, r.a, r.b) == cudaSuccess) {
       g_prof.cls[r.cls].ms += ms;
       g_prof.cls[r.cls].launches += 1;
+      g_prof.cls[r.cls].bytes += r.bytes;
     } else {
       cudaGetLastError();
     }
@@ -110,7 +111,7 @@ extern "C" int QOPB_prof_end(QOPB_kstat_t *out, int max) {
     strncpy(out[i].name, g_prof.cls[i].name.c_str(), sizeof(out[i].name) - 1);
     out[i].launches = g_prof.cls[i].launches;
     out[i].total_ms = g_prof.cls[i].ms;
-    out[i].bytes_per_launch = g_prof.cls[i].bytes;
+    out[i].bytes_per_launch = g_prof.cls[i].launches ? g_prof.cls[i].bytes / g_prof.cls[i].launches : 0.0;
   }
   return n;
 }
