@@ -16,6 +16,11 @@ buffers, p50/p99 latency, the same solve with plain FP64 CG, Dslash GB/s
 and the roofline of the dominant kernel, and the oracle's CPU time.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Further workloads (one step = one QOP_D3_asqtad_invert_multi call, solved
+by the batched int16 solver, compared with the same call in FP64):
+  --workload multimass   HISQ 24^3x48, one source, 12 masses sqrt(logspace(-4, 0))
+  --workload multisrc    asqtad 32^4 (eps 0.4), 16 sources, mass 0.005
 """
 import argparse
 import json
@@ -41,7 +46,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--lattice", default="32,32,32,64")
+    ap.add_argument("--lattice", default=None, help="default: 32,32,32,64 (single) or the workload's own")
     ap.add_argument("--mass", type=float, default=0.01)
     ap.add_argument("--tol", type=float, default=1e-10, help="|r|/|b| target")
     ap.add_argument("--eps", type=float, default=0.5)
@@ -52,6 +57,8 @@ def parse():
     ap.add_argument("--cpu-iters", type=int, default=12, help="CG iterations timed on the host")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--quick", action="store_true", help="skip FP64 baseline and e2e (development)")
+    ap.add_argument("--workload", default="single", choices=["single", "multimass", "multisrc"],
+                    help="single: the headline solve; multimass / multisrc: batched invert_multi workloads")
     return ap.parse_args()
 
 
@@ -169,7 +176,7 @@ def run_reference(a):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     from qopqdp_b200 import lattice as LT
-    L = tuple(int(x) for x in a.lattice.split(","))
+    L = tuple(int(x) for x in (a.lattice or "32,32,32,64").split(","))
     threads = os.cpu_count() or 1
     O.set_threads(threads)
     U = LT.random_gauge(L, a.eps, a.seed, device="cpu")
@@ -237,7 +244,7 @@ def run_b200(a):
         return {buf[i].name.decode(): (buf[i].launches, buf[i].total_ms, buf[i].bytes_per_launch)
                 for i in range(min(n, 32))}
 
-    L = tuple(int(x) for x in a.lattice.split(","))
+    L = tuple(int(x) for x in (a.lattice or "32,32,32,64").split(","))
     V = int(np.prod(L))
     q = Qop("D")
     assert q.init(L) == 0
@@ -409,10 +416,175 @@ def run_b200(a):
         dist.destroy_process_group()
 
 
+# ---------------------------------------------------------------- batched workloads
+MULTI = {
+    # HISQ 24^3x48, one source, 12 masses m_i = sqrt(sigma_i), sigma log-spaced 1e-4..1
+    "multimass": {"lattice": (24, 24, 24, 48), "eps": 0.5, "kind": "hisq", "nsrc": 1,
+                  "masses": [float(x) for x in np.sqrt(np.logspace(-4, 0, 12))]},
+    # asqtad 32^4 (eps 0.4), 16 sources, mass 0.005
+    "multisrc": {"lattice": (32, 32, 32, 32), "eps": 0.4, "kind": "asqtad", "nsrc": 16, "masses": [0.005]},
+}
+
+
+def run_multi(a):
+    """One step = one QOP_D3_asqtad_invert_multi call on the EVEN parity:
+    `multimass` solves one source at 12 masses, `multisrc` 16 sources at
+    one mass, every solve to |r|/|b| <= tol.  The int16 path runs all solves
+    of the call as one batched reliable-update CG sharing each hop's links.
+    Compared with the same call in FP64 (the reference algorithm: CGMS +
+    refine for multimass; for multisrc one FP64 single-source solve times 16,
+    which bounds the reference's sequential restarts from below)."""
+    rank, local, world = rank_info()
+    import torch
+    import ctypes as C
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    from qopqdp_b200 import lattice as LT
+    from qopqdp_b200.qop import Qop, QOP_invert_arg_t, QOP_resid_arg_t, QOP_EVEN, load_library
+    w = MULTI[a.workload]
+    L = tuple(int(x) for x in a.lattice.split(",")) if a.lattice else w["lattice"]
+    lib = load_library()
+    lib.QOPB_stream.restype = C.c_void_p
+    lib.QOPB_launch_count.restype = C.c_ulonglong
+
+    class KStat(C.Structure):
+        _fields_ = [("name", C.c_char * 32), ("launches", C.c_int), ("total_ms", C.c_double),
+                    ("bytes_per_launch", C.c_double)]
+
+    lib.QOPB_prof_end.argtypes = [C.POINTER(KStat), C.c_int]
+    q = Qop("D")
+    assert q.init(L) == 0
+    U = LT.random_gauge(L, w["eps"], a.seed, device="cuda")
+    G = q.create_G(U)
+    del U
+    q.rephase_G(G, LT.BENCH_R0, LT.BENCH_BC, LT.BENCH_SIGNMASK)
+    H = None
+    if w["kind"] == "hisq":
+        q.set_hisq_opts(want_aux=0)
+        H = q.hisq_create_L_from_G(LT.hisq_bench_coeffs(), G)
+        fla = q.hisq_asqtad_links(H, 0)
+    else:
+        fla = q.create_L_from_G(LT.ASQTAD_BENCH_COEFFS, G)
+    q.destroy_G(G)
+    srcs = [LT.gaussian_vector(L, a.seed + s) for s in range(w["nsrc"])]
+    hins = [q.create_V(s, QOP_EVEN) for s in srcs]
+    masses = [list(w["masses"]) for _ in range(w["nsrc"])]
+    nsolve = sum(len(m) for m in masses)
+    stream = torch.cuda.ExternalStream(lib.QOPB_stream())
+    rsq = a.tol * a.tol
+
+    def step(prec, ms=masses, ins=hins):
+        q.set_opts(prec_sloppy=prec, half_format=0, ru_delta=a.ru_delta)
+        outs = [[q.create_V(np.zeros_like(srcs[0])) for _ in m] for m in ms]
+        ras = [[QOP_resid_arg_t(rsq, 0, 0, 0, 0, 0) for _ in m] for m in ms]
+        ia = QOP_invert_arg_t(1e9, 200000, 200000, 50, QOP_EVEN)
+        q.invert_multi(fla, ms, outs, ins, ia, ras)
+        for row in outs:
+            for h in row:
+                q.destroy_V(h)
+        return [r for row in ras for r in row]
+
+    def ev():
+        e = torch.cuda.Event(enable_timing=True)
+        e.record(stream)
+        return e
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(a.warmup):
+        step(a.prec)
+    lib.QOPB_prof_begin()
+    barrier()
+    n0 = lib.QOPB_launch_count()
+    rsqs, lat = [], []
+    with Clocks(local) as clk:
+        e0 = ev()
+        for _ in range(a.steps):
+            s0 = ev()
+            ras = step(a.prec)
+            s1 = ev()
+            s1.synchronize()
+            lat.append(s0.elapsed_time(s1))
+            rsqs += [r.final_rsq for r in ras]
+        e1 = ev()
+        barrier()
+    n_launch = lib.QOPB_launch_count() - n0
+    buf = (KStat * 32)()
+    nk = lib.QOPB_prof_end(buf, 32)
+    kst = {buf[i].name.decode(): (buf[i].launches, buf[i].total_ms, buf[i].bytes_per_launch) for i in range(nk)}
+    total_ms = reduce_max(e0.elapsed_time(e1), dist, "cuda")
+    value = nsolve * a.steps * world / (total_ms / 1e3)
+    # FP64 reference algorithm for comparison (not timed into value)
+    fp64 = None
+    if not a.quick and a.fp64_steps > 0:
+        torch.cuda.synchronize()
+        s0 = ev()
+        if a.workload == "multisrc":
+            r64 = step(64, [masses[0]], [hins[0]])
+            mult = nsolve
+        else:
+            r64 = step(64)
+            mult = 1
+        s1 = ev()
+        s1.synchronize()
+        ms64 = s0.elapsed_time(s1) * mult
+        fp64 = {"ms_per_step": ms64, "solves_per_s": nsolve / (ms64 / 1e3),
+                "max_final_rsq": max(r.final_rsq for r in r64),
+                "how": "one FP64 single-source solve x %d" % nsolve if mult > 1 else "the same call in FP64"}
+    peak, peak_kind = measured_peak()
+    dom = max(kst.items(), key=lambda kv: kv[1][1]) if kst else None
+    roof = None
+    if dom:
+        name, (n, ms, b) = dom
+        ach = n * b / (ms * 1e-3) / 1e9
+        roof = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                "peak_kind": peak_kind, "kernel": name, "avg_us": 1e3 * ms / max(n, 1), "bytes_per_launch": b,
+                "traffic": None}
+    if rank == 0:
+        line = {"metric": "mixed-prec solves/s @%g (%s)" % (a.tol, a.workload), "value": value, "unit": "solves/s",
+                "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": total_ms / a.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32" if a.prec < 64 else "f64", "data": "synthetic",
+                "config": {"workload": a.workload, "lattice": L, "kind": w["kind"], "eps": w["eps"],
+                           "masses": w["masses"], "sources": w["nsrc"], "tol": a.tol,
+                           "parallelism": "replicas x%d" % world},
+                "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                "final_rsq_max": float(max(rsqs)), "fp64": fp64,
+                "speedup_vs_fp64": (value / world) / fp64["solves_per_s"] if fp64 else None,
+                "roofline": roof, "kernels": {k: {"launches": v[0], "avg_us": 1e3 * v[1] / max(v[0], 1)}
+                                              for k, v in kst.items()},
+                "gpu_launches": int(n_launch), "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    for h in hins:
+        q.destroy_V(h)
+    if H is not None:
+        q.hisq_destroy_L(H)
+    else:
+        q.destroy_L(fla)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     a = parse()
     if a.impl == "reference":
+        if a.workload != "single":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference arm covers the single-solve "
+                              "workload only"}), flush=True)
+            return
         run_reference(a)
+    elif a.workload != "single":
+        run_multi(a)
     else:
         run_b200(a)
 
