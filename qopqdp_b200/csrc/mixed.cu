@@ -557,7 +557,9 @@ k_mix_hop_q16(uint4 *__restrict__ out, const uint4 *__restrict__ src, const unsi
 }
 
 
-template <int NL, int KIND, int BATCH, bool RECON, int MINB = 1>
+// PERSIST: a grid of (SMs x MINB) blocks strides over the site blocks, so
+// no partial last wave of blocks leaves SMs idle
+template <int NL, int KIND, int BATCH, bool RECON, int MINB = 1, bool PERSIST = false>
 __global__ void __launch_bounds__(QB, MINB)
 k_mix_hop_q16r(uint4 *__restrict__ out, const uint4 *__restrict__ src, const unsigned char *__restrict__ lk,
                const uint4 *__restrict__ same, Geom g, NbrGeom ng, int p, MixState *st, double *part,
@@ -565,9 +567,12 @@ k_mix_hop_q16r(uint4 *__restrict__ out, const uint4 *__restrict__ src, const uns
   if (st->flag) return;
   const int tid = threadIdx.x;
   const i64 Vh = g.Vh;
-  const int i = blockIdx.x * QB + tid;
-  const unsigned char *gl = lk + (size_t)blockIdx.x * q16_block_bytes(NL, RECON);
+  const int nsb = PERSIST ? (int)((Vh + QB - 1) / QB) : 0;
   double acc1[1] = {0.0};
+  int sb = blockIdx.x;
+  do {
+  const int i = sb * QB + tid;
+  const unsigned char *gl = lk + (size_t)sb * q16_block_bytes(NL, RECON);
   if (i < Vh) {
     int x[4];
     site_coords(g, i, p, x);
@@ -600,8 +605,9 @@ k_mix_hop_q16r(uint4 *__restrict__ out, const uint4 *__restrict__ src, const uns
           q16_slot(ua[s], ub[s], uc[s], nb[s], a);
       }
     }
-    acc1[0] = q16_epilogue<KIND>(out, same, i, Vh, (float)st->m2, a);
+    acc1[0] += q16_epilogue<KIND>(out, same, i, Vh, (float)st->m2, a);
   }
+  } while (PERSIST && (sb += gridDim.x) < nsb);
   q16_finish<KIND>(acc1, part, count, st);
 }
 
@@ -689,10 +695,14 @@ LinksSloppy links_parity(SloppyLinks *s, int lkfmt, int p) {
 // int16 hop launch: variant 0 = plain loads, 4 slots batched;
 // 1 / 2 = TMA bulk staging with 2- / 4-slot groups; 3 / 4 = plain loads
 // with 2 / 8 slots batched; 5-10 = plain loads with the registers capped
-// for B resident blocks per SM (5: 2 slots, B 10 = 48 registers, the
-// default; 6: 2, 12 (spills); 7: 4, 8; 8: 2, 8; 9: 1, 10; 10: 2, 9).
-// Without a cap the compiler takes ~150 registers and 3 blocks fit per SM;
-// at 32^3x64 variant 5 runs a hop in 131 us against 149 us for variant 3.
+// for B resident blocks per SM (5: 2 slots, B 10 = 48 registers; 6: 2, 12
+// (spills); 7: 4, 8; 8: 2, 8; 9: 1, 10; 10: 2, 9); 11-16 = the same with a
+// persistent grid of (SMs x B) blocks striding over the site blocks
+// (11: 2, 10 (spills); 12: 2, 8; 13: 2, 7; 14: 4, 8; 15: 2, 6 = 80
+// registers, the default; 16: 1, 8).  At 32^3x64 a hop takes 115.7 us with
+// variant 15, 116-117 us with 12-14 and 16, 131 us with 5 and 149 us with 3
+// (no register cap, ~150 registers): the persistent grid removes the
+// partial last wave of blocks, the register cap matters less once it does.
 template <int KIND>
 static void launch_q16(int variant, int nl, bool recon, float c_long, int grid, uint4 *out, const uint4 *src,
                        const unsigned char *lk, const uint4 *same, const Geom &g, const NbrGeom &ng, int par,
@@ -710,6 +720,13 @@ static void launch_q16(int variant, int nl, bool recon, float c_long, int grid, 
     else if (recon) k_mix_hop_q16r<16, KIND, B, true, M><<<grid, QB, 0, c.s>>>(Q16_ARGS, c_long);        \
     else k_mix_hop_q16r<16, KIND, B, false, M><<<grid, QB, 0, c.s>>>(Q16_ARGS, c_long);                  \
   } while (0)
+#define Q16RP(B, M)                                                                                       \
+  do {                                                                                                    \
+    const int gp = std::min(grid, (c.red_blocks / 8) * M);                                                \
+    if (nl != 16) k_mix_hop_q16r<8, KIND, B, false, M, true><<<gp, QB, 0, c.s>>>(Q16_ARGS, c_long);      \
+    else if (recon) k_mix_hop_q16r<16, KIND, B, true, M, true><<<gp, QB, 0, c.s>>>(Q16_ARGS, c_long);    \
+    else k_mix_hop_q16r<16, KIND, B, false, M, true><<<gp, QB, 0, c.s>>>(Q16_ARGS, c_long);              \
+  } while (0)
   switch (variant) {
     case 5: Q16RM(2, 10); break;   // register cap for 10 resident blocks
     case 6: Q16RM(2, 12); break;
@@ -717,6 +734,12 @@ static void launch_q16(int variant, int nl, bool recon, float c_long, int grid, 
     case 8: Q16RM(2, 8); break;
     case 9: Q16RM(1, 10); break;
     case 10: Q16RM(2, 9); break;
+    case 11: Q16RP(2, 10); break;   // persistent grid of SMs x 10 blocks
+    case 12: Q16RP(2, 8); break;
+    case 13: Q16RP(2, 7); break;
+    case 14: Q16RP(4, 8); break;
+    case 15: Q16RP(2, 6); break;
+    case 16: Q16RP(1, 8); break;
     case 1:
       if (nl == 16) k_mix_hop_q16<16, KIND, 2><<<grid, QB, 4 * QSLOT, c.s>>>(Q16_ARGS);
       else k_mix_hop_q16<8, KIND, 2><<<grid, QB, 4 * QSLOT, c.s>>>(Q16_ARGS);
@@ -738,6 +761,7 @@ static void launch_q16(int variant, int nl, bool recon, float c_long, int grid, 
       else k_mix_hop_q16r<8, KIND, 4, false><<<grid, QB, 0, c.s>>>(Q16_ARGS, c_long);
       break;
   }
+#undef Q16RP
 #undef Q16RM
 #undef Q16R
 #undef Q16_ARGS
