@@ -21,6 +21,8 @@ Further workloads (one step = one QOP_D3_asqtad_invert_multi call, solved
 by the batched int16 solver, compared with the same call in FP64):
   --workload multimass   HISQ 24^3x48, one source, 12 masses sqrt(logspace(-4, 0))
   --workload multisrc    asqtad 32^4 (eps 0.4), 16 sources, mass 0.005
+  --workload serve       the solve service (QOPB_serve_*) with HISQ 16^4,
+                         24^3x48 and 32^3x64 resident, Poisson arrivals
 """
 import argparse
 import json
@@ -57,8 +59,11 @@ def parse():
     ap.add_argument("--cpu-iters", type=int, default=12, help="CG iterations timed on the host")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--quick", action="store_true", help="skip FP64 baseline and e2e (development)")
-    ap.add_argument("--workload", default="single", choices=["single", "multimass", "multisrc"],
-                    help="single: the headline solve; multimass / multisrc: batched invert_multi workloads")
+    ap.add_argument("--workload", default="single", choices=["single", "multimass", "multisrc", "serve"],
+                    help="single: the headline solve; multimass / multisrc: batched invert_multi workloads; "
+                         "serve: the solve service under Poisson load")
+    ap.add_argument("--serve-burst", type=int, default=12, help="requests of the peak-throughput burst")
+    ap.add_argument("--serve-seconds", type=float, default=20.0, help="arrival window per load level")
     return ap.parse_args()
 
 
@@ -575,6 +580,127 @@ def run_multi(a):
         dist.destroy_process_group()
 
 
+SERVE_LATTICES = [(16, 16, 16, 16), (24, 24, 24, 48), (32, 32, 32, 64)]
+
+
+def run_serve(a):
+    """Solve service under load: HISQ links resident on 16^4, 24^3x48 and
+    32^3x64 (one process, three lattices); requests pick a lattice uniformly,
+    a mass log-uniform in [0.005, 0.1], |r|/|b| in {1e-8, 1e-10} and 1-8
+    sources (seeded).  Peak throughput is measured on a burst of requests
+    submitted at once; then Poisson arrivals at 50 / 80 / 95 % of that peak
+    for --serve-seconds each give p50 / p99 latency (submit -> result in the
+    caller's buffer) and the throughput achieved."""
+    rank, local, world = rank_info()
+    import torch
+    import threading as th
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900),
+                                device_id=torch.device("cuda", local))
+    from qopqdp_b200 import lattice as LT
+    from qopqdp_b200.qop import Qop, QOP_EVEN
+    q = Qop("D")
+    assert q.init(SERVE_LATTICES[0]) == 0
+    lats, links, pools = [], [], []
+    q.set_hisq_opts(want_aux=0)
+    for k, L in enumerate(SERVE_LATTICES):
+        lat = 0 if k == 0 else q.lattice_create(L)
+        assert q.lattice_use(lat) == 0
+        U = LT.random_gauge(L, a.eps, a.seed + k, device="cuda")
+        G = q.create_G(U)
+        del U
+        q.rephase_G(G, LT.BENCH_R0, LT.BENCH_BC, LT.BENCH_SIGNMASK)
+        H = q.hisq_create_L_from_G(LT.hisq_bench_coeffs(), G)
+        q.destroy_G(G)
+        lats.append(lat)
+        links.append((H, q.hisq_asqtad_links(H, 0)))
+        srcs = [LT.gaussian_vector(L, a.seed + 100 * k + s) for s in range(8)]
+        pools.append((srcs, [np.zeros_like(s) for s in srcs]))
+    rng = np.random.default_rng(a.seed + 7 * rank)
+
+    def request():
+        k = int(rng.integers(0, len(SERVE_LATTICES)))
+        mass = float(np.exp(rng.uniform(np.log(0.005), np.log(0.1))))
+        tol = 1e-8 if rng.random() < 0.5 else 1e-10
+        return k, mass, tol * tol, int(rng.integers(1, 9))
+
+    def submit(k, mass, rsq, nrhs):
+        srcs, dsts = pools[k]
+        return q.serve_submit(links[k][1], lats[k], QOP_EVEN, mass, rsq, srcs[:nrhs], dsts[:nrhs])
+
+    def collect(tickets):
+        out = []
+        for t, nrhs, rsq in tickets:
+            rc, res = q.serve_wait(t, 3600.0)
+            out.append((rc, res.status, res.total_ms, res.final_rsq_max / rsq, nrhs, res.batch_systems))
+        return out
+
+    assert q.serve_start() == 0
+    # warm-up: one request per lattice (builds the int16 link copies)
+    collect([(submit(k, 0.05, 1e-16, 1), 1, 1e-16) for k in range(len(SERVE_LATTICES))])
+    # peak: a burst submitted at once
+    burst = [request() for _ in range(a.serve_burst)]
+    t0 = time.perf_counter()
+    done = collect([(submit(*r), r[3], r[2]) for r in burst])
+    t_peak = time.perf_counter() - t0
+    peak = sum(d[4] for d in done) / t_peak
+    loads = []
+    for frac in (0.5, 0.8, 0.95):
+        rate = frac * peak / 4.5                       # requests/s (mean 4.5 sources per request)
+        reqs = []
+        t_arr = 0.0
+        while t_arr < a.serve_seconds:
+            t_arr += rng.exponential(1.0 / rate)
+            reqs.append((t_arr, request()))
+        tickets = []
+
+        def feeder():
+            s0 = time.perf_counter()
+            for t_at, r in reqs:
+                dt = t_at - (time.perf_counter() - s0)
+                if dt > 0:
+                    time.sleep(dt)
+                tickets.append((submit(*r), r[3], r[2]))
+
+        s0 = time.perf_counter()
+        f = th.Thread(target=feeder)
+        f.start()
+        f.join()
+        res = collect(tickets)
+        wall = time.perf_counter() - s0
+        lat = np.array([r[2] for r in res])
+        ok = all(r[0] == 0 and r[1] == 0 for r in res)
+        loads.append({"load": frac, "requests": len(res), "solves": int(sum(r[4] for r in res)),
+                      "offered_solves_per_s": frac * peak, "solves_per_s": sum(r[4] for r in res) / wall,
+                      "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                      "mean_batch": float(np.mean([r[5] for r in res])),
+                      "max_final_rsq_over_target": max(r[3] for r in res) if res else None, "all_ok": ok})
+    q.serve_stop()
+    p99 = reduce_max(max(l["p99_ms"] for l in loads), dist, "cuda")
+    if rank == 0:
+        line = {"metric": "solve service p99 latency and solves/s (3 resident HISQ lattices)",
+                "value": peak * world, "unit": "solves/s", "n_gpus": world, "steps": a.serve_burst,
+                "warmup": len(SERVE_LATTICES), "ms_per_step": 1e3 * t_peak / a.serve_burst,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic",
+                "config": {"workload": "serve", "lattices": SERVE_LATTICES, "mass": "log-uniform [0.005, 0.1]",
+                           "tol": [1e-8, 1e-10], "sources_per_request": "1-8", "burst": a.serve_burst,
+                           "seconds_per_load": a.serve_seconds, "parallelism": "replicas x%d" % world},
+                "peak_solves_per_s": peak, "loads": loads, "p99_ms_max_over_ranks": p99}
+        print(json.dumps(line), flush=True)
+    for lat, (H, _) in zip(lats, links):
+        q.lattice_use(lat)
+        q.hisq_destroy_L(H)
+    q.lattice_use(0)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     a = parse()
     if a.impl == "reference":
@@ -583,6 +709,8 @@ def main():
                               "workload only"}), flush=True)
             return
         run_reference(a)
+    elif a.workload == "serve":
+        run_serve(a)
     elif a.workload != "single":
         run_multi(a)
     else:

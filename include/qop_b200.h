@@ -50,6 +50,53 @@ unsigned long long QOPB_launch_count(void);
 double QOPB_D3_asqtad_ddagd_norm2_noalloc(QOP_info_t *info, QOP_D3_FermionLinksAsqtad *asqtad, double mass,
                                           QOP_D3_ColorVector *out, QOP_D3_ColorVector *in, QOP_evenodd_t eo);
 
+/* Several lattices in one process (no counterpart in the reference, whose
+   QOP_init fixes one geometry per process).  QOP_init defines lattice 0;
+   QOPB_lattice_create adds a geometry (extents even and >= 4) and returns
+   its id (-1 on error); QOPB_lattice_use makes it current (0, or -1 for an
+   unknown id).  Every handle belongs to the lattice that was current when it
+   was created; entry points given a handle of another lattice report
+   QOP_FAIL. */
+int QOPB_lattice_create(const int latsize[4]);
+int QOPB_lattice_use(int id);
+int QOPB_lattice_current(void);
+
+/* Solve service (no counterpart in the reference).  A worker thread
+   takes queued requests, groups the systems of requests on the same link
+   handle (up to 16) into one batched mixed-precision solve (int16 storage,
+   FP64 reliable updates: every solution meets its FP64 target) and copies
+   the results to the caller's buffers.  A request solves, for each of its
+   nrhs sources, A x = b with A = m^2 - D D on parity `evenodd` (QOP_EVEN or
+   QOP_ODD) and writes m A^-1 b on that parity (the QOP_asqtad_invert
+   convention) into dst[k]; src[k] / dst[k] are raw full-volume arrays
+   (QOP raw site order, 6 doubles per site) that the caller keeps valid until
+   QOPB_serve_wait has returned for the ticket.  While the service runs, the
+   worker is the only thread that may call into the library: callers use
+   only QOPB_serve_submit / QOPB_serve_wait / QOPB_serve_stop. */
+typedef struct {
+  QOP_D3_FermionLinksAsqtad *links; /* handle (of lattice `lattice`)        */
+  int lattice;                      /* lattice id of the handle             */
+  QOP_evenodd_t evenodd;            /* QOP_EVEN or QOP_ODD                  */
+  double mass;
+  double rsqmin;                    /* target |r|^2 / |b|^2                 */
+  int max_iter;                     /* per system; <= 0: 100000             */
+  int nrhs;                         /* 1 .. 16                              */
+  const double *const *src;         /* nrhs raw sources                     */
+  double *const *dst;               /* nrhs raw outputs                     */
+} QOPB_request_t;
+typedef struct {
+  int status;                       /* QOP_SUCCESS or QOP_FAIL              */
+  int iters_max;                    /* largest iteration count of the request */
+  double final_rsq_max;             /* largest final |r|^2 / |b|^2          */
+  double queue_ms, solve_ms, total_ms; /* waiting, batch solve, submit->done */
+  int batch_systems;                /* systems in the batch that solved it  */
+} QOPB_result_t;
+int QOPB_serve_start(void);                                 /* 0 or -1 */
+long long QOPB_serve_submit(const QOPB_request_t *req);     /* ticket >= 0, or -1 */
+/* 0: done (result filled, ticket released); 1: timed out; -1: bad ticket */
+int QOPB_serve_wait(long long ticket, double timeout_s, QOPB_result_t *res);
+int QOPB_serve_stop(void);   /* finishes queued requests, joins the worker */
+
 #ifdef __cplusplus
 }
 #endif

@@ -36,9 +36,7 @@ void report(QOP_info_t *info, const Fail &e, const char *fn) {
 #define CATCH(info, ret) } catch (Fail &e) { report(info, e, __func__); return ret; }
 #define CATCHV(info) } catch (Fail &e) { report(info, e, __func__); return; }
 
-template <typename T> void need_handle(const void *h, const char *what) {
-  if (!h) fail(QOP_FAIL, "NULL %s handle", what);
-}
+template <typename T> void need_handle(const void *h, const char *what) { handle_check(h, what); }
 
 // ---------------------------------------------------------------- fields
 template <typename T, typename R> VecT<T> *create_V(const R *src, int eo) {

@@ -4,6 +4,8 @@
 #include "qopb.h"
 #include <cstdarg>
 #include <sys/time.h>
+#include <mutex>
+#include <unordered_map>
 
 namespace qopb {
 
@@ -88,6 +90,61 @@ void dfree(void *p) {
 void dzero(void *p, size_t bytes) { QCHECK(cudaMemsetAsync(p, 0, bytes, g_ctx.s)); }
 void sync() { QCHECK(cudaStreamSynchronize(g_ctx.s)); }
 
+static std::mutex g_hmu;
+static std::unordered_map<const void *, int> g_handles;
+void handle_register(const void *h) {
+  std::lock_guard<std::mutex> lk(g_hmu);
+  g_handles[h] = g_ctx.lat;
+}
+void handle_forget(const void *h) {
+  std::lock_guard<std::mutex> lk(g_hmu);
+  g_handles.erase(h);
+}
+void handle_check(const void *h, const char *what) {
+  if (!h) fail(QOP_FAIL, "NULL %s handle", what);
+  int lat = -1;
+  {
+    std::lock_guard<std::mutex> lk(g_hmu);
+    auto it = g_handles.find(h);
+    if (it != g_handles.end()) lat = it->second;
+  }
+  if (lat < 0) fail(QOP_FAIL, "%s handle is not a live handle of this library", what);
+  if (lat != g_ctx.lat)
+    fail(QOP_FAIL, "%s handle belongs to lattice %d, the current lattice is %d", what, lat, g_ctx.lat);
+}
+
+// extents even and >= 4 (eo preconditioning and the 3-hop Naik term), V < 2^31
+static bool make_geom(const int *ls, Geom &g) {
+  g = Geom{};
+  g.V = 1;
+  for (int i = 0; i < 4; i++) {
+    if (ls[i] < 4 || (ls[i] & 1)) {
+      fprintf(stderr, "QOP: extent %d in direction %d must be even and >= 4\n", ls[i], i);
+      return false;
+    }
+    g.L[i] = ls[i];
+    g.V *= ls[i];
+  }
+  g.Vh = g.V / 2;
+  if (g.V >= (1LL << 31)) {
+    fprintf(stderr, "QOP: volume too large for one device\n");
+    return false;
+  }
+  return true;
+}
+
+// fused reductions run one block per 64+ sites with up to 4 sums each
+static void ensure_partials(const Geom &g) {
+  Context &c = g_ctx;
+  size_t need = (size_t)4 * (g.Vh / 64 + 64);
+  if (need > c.part_cap) {
+    QCHECK(cudaStreamSynchronize(c.s));
+    QCHECK(cudaFree(c.d_part));
+    QCHECK(cudaMalloc(&c.d_part, sizeof(double) * need));
+    c.part_cap = need;
+  }
+}
+
 int grid_for(i64 n, int block) {
   i64 b = (n + block - 1) / block;
   if (b < 1) b = 1;
@@ -112,38 +169,41 @@ QOP_status_t QOP_init(QOP_layout_t *layout) {
     return QOP_FAIL;
   }
   Geom g{};
-  g.V = 1;
-  for (int i = 0; i < 4; i++) {
-    int L = layout->latsize[i];
-    if (L < 4 || (L & 1)) {
-      fprintf(stderr, "QOP_init: extent %d in direction %d must be even and >= 4\n", L, i);
-      return QOP_FAIL;
-    }
-    g.L[i] = L;
-    g.V *= L;
-  }
-  g.Vh = g.V / 2;
-  if (g.V >= (1LL << 31)) {
-    fprintf(stderr, "QOP_init: volume too large for one device\n");
-    return QOP_FAIL;
-  }
+  if (!make_geom(layout->latsize, g)) return QOP_FAIL;
   OPT_TRY
   ensure_ready();
-  // fused reductions run one block per 64+ sites with up to 4 sums each
-  size_t need = (size_t)4 * (g.Vh / 64 + 64);
-  if (need > c.part_cap) {
-    QCHECK(cudaStreamSynchronize(c.s));
-    QCHECK(cudaFree(c.d_part));
-    QCHECK(cudaMalloc(&c.d_part, sizeof(double) * need));
-    c.part_cap = need;
-  }
+  ensure_partials(g);
   OPT_CATCH(QOP_FAIL)
   c.g = g;
+  c.lats.assign(1, g);
+  c.lat = 0;
   c.verbosity = 0;
   c.proflevel = 0;
   c.inited = 1;
   return QOP_SUCCESS;
 }
+
+int QOPB_lattice_create(const int latsize[4]) {
+  Context &c = ctx();
+  if (!c.inited || !latsize) return -1;
+  Geom g{};
+  if (!make_geom(latsize, g)) return -1;
+  OPT_TRY
+  ensure_partials(g);
+  OPT_CATCH(-1)
+  c.lats.push_back(g);
+  return (int)c.lats.size() - 1;
+}
+
+int QOPB_lattice_use(int id) {
+  Context &c = ctx();
+  if (!c.inited || id < 0 || id >= (int)c.lats.size()) return -1;
+  c.lat = id;
+  c.g = c.lats[id];
+  return 0;
+}
+
+int QOPB_lattice_current(void) { return ctx().inited ? ctx().lat : -1; }
 
 QOP_status_t QOP_finalize(void) {
   Context &c = ctx();

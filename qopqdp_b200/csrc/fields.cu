@@ -119,6 +119,7 @@ GaugeT<T> *gauge_new() {
   GaugeT<T> *G = new GaugeT<T>();
   G->d = dalloc<c2<T>>(4 * 18 * g.Vh);
   dzero(G->d, sizeof(c2<T>) * 4 * 18 * g.Vh);
+  handle_register(G);
   return G;
 }
 template <typename T>
@@ -126,6 +127,7 @@ void gauge_destroy(GaugeT<T> *G) {
   if (!G) return;
   dfree(G->d);
   delete[] G->r0; delete[] G->bc; delete[] G->signmask;
+  handle_forget(G);
   delete G;
 }
 template GaugeT<float> *gauge_new<float>();
@@ -139,12 +141,14 @@ VecT<T> *vec_new() {
   VecT<T> *v = new VecT<T>();
   v->d = dalloc<c2<T>>(vec_elems(g));
   dzero(v->d, sizeof(c2<T>) * vec_elems(g));
+  handle_register(v);
   return v;
 }
 template <typename T>
 void vec_destroy(VecT<T> *v) {
   if (!v) return;
   dfree(v->d);
+  handle_forget(v);
   delete v;
 }
 template VecT<float> *vec_new<float>();

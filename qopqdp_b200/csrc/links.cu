@@ -432,6 +432,7 @@ FlaT<T> *fla_alloc(int nlinks) {
   FlaT<T> *f = new FlaT<T>();
   f->nlinks = nlinks;
   f->d = dalloc<c2<T>>(2LL * nlinks * 9 * g.Vh);
+  handle_register(f);
   return f;
 }
 
@@ -479,6 +480,7 @@ void fla_destroy(FlaT<T> *f) {
   if (!f) return;
   sloppy_invalidate((void *)f);
   dfree(f->d);
+  handle_forget(f);
   delete f;
 }
 
@@ -601,6 +603,7 @@ HisqT<T> *hisq_from_G(QOP_info_t *info, const QOP_hisq_coeffs_t *c, GaugeT<T> *g
   a2.lepage = c->asqtad_lepage; a2.naik = c->asqtad_naik;
   a3.one_link = c->difference_one_link; a3.naik = c->difference_naik;
   HisqT<T> *h = new HisqT<T>();
+  handle_register(h);
   h->n_naiks = c->n_naiks;
   bool own;
   double2 *U = gauge_fp64(gauge, own);
@@ -663,6 +666,7 @@ void hisq_destroy(HisqT<T> *h) {
   for (int k = 0; k < h->n_naiks; k++) fla_destroy(h->fn[k]);
   fla_destroy(h->fn_deps);
   gauge_destroy(h->U); gauge_destroy(h->V); gauge_destroy(h->W);
+  handle_forget(h);
   delete h;
 }
 

@@ -23,6 +23,7 @@
 #include <string>
 #include <type_traits>
 #include <stdexcept>
+#include <vector>
 #include "qop.h"
 #include "qop_b200.h"
 
@@ -123,6 +124,10 @@ struct Context {
   double *h_res = nullptr;   // pinned
   int red_blocks = 0;
   size_t part_cap = 0;       // doubles in d_part
+  // lattices: QOP_init defines lattice 0, QOPB_lattice_create adds more;
+  // `g` is the geometry of the current one (QOPB_lattice_use)
+  std::vector<Geom> lats;
+  int lat = 0;
 };
 Context &ctx();
 void require_init(const char *fn);
@@ -136,6 +141,12 @@ void dzero(void *p, size_t bytes);
 void sync();
 
 int grid_for(i64 n, int block);
+
+// every handle remembers the lattice it was created on; entry points refuse
+// handles of another lattice (their device arrays have another size)
+void handle_register(const void *h);
+void handle_forget(const void *h);
+void handle_check(const void *h, const char *what);
 
 // ---------------------------------------------------------------- handles
 template <typename T> struct VecT {       // QOP_*_ColorVector

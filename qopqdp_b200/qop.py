@@ -47,6 +47,19 @@ class QOP_opt_t(C.Structure):
     _fields_ = [("tag", C.c_char_p), ("value", C.c_double), ("extra", C.c_void_p)]
 
 
+class QOPB_request_t(C.Structure):
+    """One request of the solve service (include/qop_b200.h)."""
+    _fields_ = [("links", C.c_void_p), ("lattice", C.c_int), ("evenodd", C.c_int), ("mass", C.c_double),
+                ("rsqmin", C.c_double), ("max_iter", C.c_int), ("nrhs", C.c_int),
+                ("src", C.POINTER(C.POINTER(C.c_double))), ("dst", C.POINTER(C.POINTER(C.c_double)))]
+
+
+class QOPB_result_t(C.Structure):
+    _fields_ = [("status", C.c_int), ("iters_max", C.c_int), ("final_rsq_max", C.c_double),
+                ("queue_ms", C.c_double), ("solve_ms", C.c_double), ("total_ms", C.c_double),
+                ("batch_systems", C.c_int)]
+
+
 class QOP_info_t(C.Structure):
     _fields_ = [("final_sec", C.c_double), ("final_flop", C.c_double), ("status", C.c_int),
                 ("count1", C.c_int), ("count2", C.c_int)]
@@ -110,6 +123,17 @@ def load_library(path=None):
     lib.QOP_node_index_raw_V.restype = ip
     lib.QOP_sites_on_node_raw_V.argtypes = [ip]
     lib.QOP_sites_on_node_raw_V.restype = ip
+    lib.QOPB_lattice_create.argtypes = [C.POINTER(C.c_int)]
+    lib.QOPB_lattice_create.restype = ip
+    lib.QOPB_lattice_use.argtypes = [ip]
+    lib.QOPB_lattice_use.restype = ip
+    lib.QOPB_lattice_current.restype = ip
+    lib.QOPB_serve_start.restype = ip
+    lib.QOPB_serve_stop.restype = ip
+    lib.QOPB_serve_submit.argtypes = [C.POINTER(QOPB_request_t)]
+    lib.QOPB_serve_submit.restype = C.c_longlong
+    lib.QOPB_serve_wait.argtypes = [C.c_longlong, C.c_double, C.POINTER(QOPB_result_t)]
+    lib.QOPB_serve_wait.restype = ip
     for f in ("QOP_asqtad_invert_set_opts", "QOP_hisq_links_set_opts", "QOP_hisq_invert_set_opts"):
         getattr(lib, f).argtypes = [C.POINTER(QOP_opt_t), ip]
         getattr(lib, f).restype = ip
@@ -378,3 +402,38 @@ class Qop:
         ip_ = (C.c_void_p * nsrc)(*ins)
         self.f("asqtad_invert_multi")(C.byref(info), fla, C.byref(inv_arg), ra, mp, nm, op, ip_, nsrc)
         return info
+
+    # ------------------------------------------------------------ lattices and the solve service
+    def lattice_create(self, L):
+        return self.lib.QOPB_lattice_create((C.c_int * 4)(*L))
+
+    def lattice_use(self, lat):
+        return self.lib.QOPB_lattice_use(lat)
+
+    def serve_start(self):
+        self._pending = {}
+        return self.lib.QOPB_serve_start()
+
+    def serve_stop(self):
+        return self.lib.QOPB_serve_stop()
+
+    def serve_submit(self, fla, lattice, eo, mass, rsqmin, srcs, dsts, max_iter=0):
+        """srcs: raw float64 arrays (kept alive here); dsts: preallocated raw
+        float64 arrays written by the service.  Returns the ticket (< 0 on error)."""
+        n = len(srcs)
+        src = [np.ascontiguousarray(a, dtype=np.float64) for a in srcs]
+        pp = C.POINTER(C.c_double)
+        sp = (pp * n)(*[a.ctypes.data_as(pp) for a in src])
+        dp = (pp * n)(*[a.ctypes.data_as(pp) for a in dsts])
+        rq = QOPB_request_t(fla, lattice, eo, mass, rsqmin, max_iter, n, sp, dp)
+        t = self.lib.QOPB_serve_submit(C.byref(rq))
+        if t >= 0:
+            self._pending[t] = (src, dsts, sp, dp)
+        return t
+
+    def serve_wait(self, ticket, timeout=0.0):
+        res = QOPB_result_t()
+        rc = self.lib.QOPB_serve_wait(ticket, timeout, C.byref(res))
+        if rc == 0:
+            self._pending.pop(ticket, None)
+        return rc, res
