@@ -557,6 +557,118 @@ k_mix_hop_q16(uint4 *__restrict__ out, const uint4 *__restrict__ src, const unsi
 }
 
 
+// ---------------------------------------------------------------- cp.async-pipelined hop
+// Variants 17-19: persistent grid; every thread streams the raw words of its
+// next R slots (the link and the neighbour site) into its own ring in shared
+// memory with cp.async, so R x 56 bytes per thread are in flight without
+// holding registers.  Slots are consumed in order across site blocks (the
+// first slots of the next site block are fetched while the current block's
+// last ones are computed).  The ring has R + 1 stages and a stage is refilled
+// one slot after it was read.  Only the thread that wrote a stage reads it,
+// so cp.async.wait_group alone orders the data: no barrier.  Sites beyond Vh
+// in the last block fetch their (zero) padding links and site 0's
+// neighbours, and are not stored.
+__device__ __forceinline__ void cpa16(void *sm, const void *gm) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(sm)), "l"(gm) : "memory");
+}
+__device__ __forceinline__ void cpa8(void *sm, const void *gm) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(sm)), "l"(gm) : "memory");
+}
+__device__ __forceinline__ void cpa4(void *sm, const void *gm) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(sm)), "l"(gm) : "memory");
+}
+__device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cpa_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// neighbour index with the direction chosen at run time (no indexed arrays)
+__device__ __forceinline__ int nbr_sel(const NbrGeom &n, int x0, int x1, int x2, int x3, int lex, int mu, int d) {
+  const int xm = mu == 0 ? x0 : mu == 1 ? x1 : mu == 2 ? x2 : x3;
+  const int Lm = mu == 0 ? n.L[0] : mu == 1 ? n.L[1] : mu == 2 ? n.L[2] : n.L[3];
+  const int sm = mu == 0 ? n.str[0] : mu == 1 ? n.str[1] : mu == 2 ? n.str[2] : n.str[3];
+  const int t = xm + d;
+  int off = d * sm;
+  if (t >= Lm) off -= Lm * sm;
+  else if (t < 0) off += Lm * sm;
+  return (lex + off) >> 1;
+}
+
+template <int NL, int KIND, bool RECON, int R, int MINB>
+__global__ void __launch_bounds__(QB, MINB)
+k_mix_hop_q16a(uint4 *__restrict__ out, const uint4 *__restrict__ src, const unsigned char *__restrict__ lk,
+               const uint4 *__restrict__ same, Geom g, NbrGeom ng, int p, MixState *st, double *part,
+               unsigned *count, float c_long) {
+  if (st->flag) return;
+  constexpr int S = R + 1;
+  __shared__ __align__(16) uint4 sa[S][QB];
+  __shared__ __align__(16) uint4 sb[S][QB];
+  __shared__ __align__(16) uint4 sn[S][QB];
+  __shared__ __align__(16) uint2 sc[S][QB];
+  const int tid = threadIdx.x;
+  const i64 Vh = g.Vh;
+  const int nsb = (int)((Vh + QB - 1) / QB);
+  // issue cursor: site block, slot, this thread's site coordinates there
+  int isb = blockIdx.x, ik = 0, ilex = 0, is = 0;
+  int y0 = 0, y1 = 0, y2 = 0, y3 = 0;
+  auto site_of = [&](int blk) {
+    const i64 i = (i64)blk * QB + tid;
+    int x[4];
+    site_coords(g, i < Vh ? (int)i : 0, p, x);
+    y0 = x[0]; y1 = x[1]; y2 = x[2]; y3 = x[3];
+    ilex = ((y0 * g.L[1] + y1) * g.L[2] + y2) * g.L[3] + y3;
+  };
+  auto issue = [&]() {
+    if (isb < nsb) {
+      const unsigned char *ls = lk + (size_t)isb * q16_block_bytes(NL, RECON) + q16_slot_off(ik, RECON);
+      if (RECON && (ik & 1)) {
+        cpa16(&sa[is][tid], ls + 16 * tid);
+        cpa8(&sb[is][tid], ls + 16 * QB + 8 * tid);
+        cpa4(&sc[is][tid], ls + 24 * QB + 4 * tid);
+      } else {
+        cpa16(&sa[is][tid], ls + 16 * tid);
+        cpa16(&sb[is][tid], ls + 16 * QB + 16 * tid);
+        cpa8(&sc[is][tid], ls + 32 * QB + 8 * tid);
+      }
+      const int j = nbr_sel(ng, y0, y1, y2, y3, ilex, slot_mu<NL>(ik), slot_disp<NL>(ik));
+      cpa16(&sn[is][tid], src + j);
+      if (++ik == NL) {
+        ik = 0;
+        isb += gridDim.x;
+        if (isb < nsb) site_of(isb);
+      }
+    }
+    cpa_commit();
+    is = (is + 1 == S) ? 0 : is + 1;
+  };
+  if (isb < nsb) site_of(isb);
+#pragma unroll
+  for (int r = 0; r < R; r++) issue();
+  int cs = 0;   // stage being consumed
+  double acc1[1] = {0.0};
+  for (int cb = blockIdx.x; cb < nsb; cb += gridDim.x) {
+    const int i = cb * QB + tid;
+    float2 a[3] = {make_float2(0, 0), make_float2(0, 0), make_float2(0, 0)};
+#pragma unroll
+    for (int k = 0; k < NL; k++) {
+      cpa_wait<R - 1>();
+      const uint4 ua = sa[cs][tid], nb = sn[cs][tid];
+      if (RECON && (k & 1)) {
+        const uint4 w = sb[cs][tid];
+        const uint2 c = sc[cs][tid];
+        q16_slot_recon(ua, make_uint2(w.x, w.y), __uint_as_float(c.x), nb, c_long, a);
+      } else {
+        q16_slot(ua, sb[cs][tid], sc[cs][tid], nb, a);
+      }
+      cs = (cs + 1 == S) ? 0 : cs + 1;
+      issue();   // refills the stage read one slot ago
+    }
+    if (i < Vh) acc1[0] += q16_epilogue<KIND>(out, same, i, Vh, (float)st->m2, a);
+  }
+  cpa_wait<0>();
+  q16_finish<KIND>(acc1, part, count, st);
+}
+
 // PERSIST: a grid of (SMs x MINB) blocks strides over the site blocks, so
 // no partial last wave of blocks leaves SMs idle
 template <int NL, int KIND, int BATCH, bool RECON, int MINB = 1, bool PERSIST = false>
@@ -703,6 +815,9 @@ LinksSloppy links_parity(SloppyLinks *s, int lkfmt, int p) {
 // variant 15, 116-117 us with 12-14 and 16, 131 us with 5 and 149 us with 3
 // (no register cap, ~150 registers): the persistent grid removes the
 // partial last wave of blocks, the register cap matters less once it does.
+// 17-19 = persistent with a per-thread cp.async ring 3 / 2 / 4 slots ahead
+// (6 / 8 / 5 blocks per SM): 157-170 us, the 4-5 small asynchronous copies
+// per slot and thread cost more issue slots than the latency they hide.
 template <int KIND>
 static void launch_q16(int variant, int nl, bool recon, float c_long, int grid, uint4 *out, const uint4 *src,
                        const unsigned char *lk, const uint4 *same, const Geom &g, const NbrGeom &ng, int par,
@@ -727,6 +842,13 @@ static void launch_q16(int variant, int nl, bool recon, float c_long, int grid, 
     else if (recon) k_mix_hop_q16r<16, KIND, B, true, M, true><<<gp, QB, 0, c.s>>>(Q16_ARGS, c_long);    \
     else k_mix_hop_q16r<16, KIND, B, false, M, true><<<gp, QB, 0, c.s>>>(Q16_ARGS, c_long);              \
   } while (0)
+#define Q16A(RR, M)                                                                                       \
+  do {                                                                                                    \
+    const int gp = std::min(grid, (c.red_blocks / 8) * M);                                                \
+    if (nl != 16) k_mix_hop_q16a<8, KIND, false, RR, M><<<gp, QB, 0, c.s>>>(Q16_ARGS, c_long);            \
+    else if (recon) k_mix_hop_q16a<16, KIND, true, RR, M><<<gp, QB, 0, c.s>>>(Q16_ARGS, c_long);          \
+    else k_mix_hop_q16a<16, KIND, false, RR, M><<<gp, QB, 0, c.s>>>(Q16_ARGS, c_long);                    \
+  } while (0)
   switch (variant) {
     case 5: Q16RM(2, 10); break;   // register cap for 10 resident blocks
     case 6: Q16RM(2, 12); break;
@@ -740,6 +862,9 @@ static void launch_q16(int variant, int nl, bool recon, float c_long, int grid, 
     case 14: Q16RP(4, 8); break;
     case 15: Q16RP(2, 6); break;
     case 16: Q16RP(1, 8); break;
+    case 17: Q16A(3, 6); break;    // cp.async ring of 3 slots ahead
+    case 18: Q16A(2, 8); break;
+    case 19: Q16A(4, 5); break;
     case 1:
       if (nl == 16) k_mix_hop_q16<16, KIND, 2><<<grid, QB, 4 * QSLOT, c.s>>>(Q16_ARGS);
       else k_mix_hop_q16<8, KIND, 2><<<grid, QB, 4 * QSLOT, c.s>>>(Q16_ARGS);
@@ -761,6 +886,7 @@ static void launch_q16(int variant, int nl, bool recon, float c_long, int grid, 
       else k_mix_hop_q16r<8, KIND, 4, false><<<grid, QB, 0, c.s>>>(Q16_ARGS, c_long);
       break;
   }
+#undef Q16A
 #undef Q16RP
 #undef Q16RM
 #undef Q16R
