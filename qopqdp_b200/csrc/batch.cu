@@ -68,8 +68,10 @@ __device__ __forceinline__ float q16_link_recon(const uint4 ua, const uint2 ub, 
 // Blocks are (site block sb, system group grp) flattened with the group
 // fastest, so the blocks that share a site block's links run together and
 // the links come from HBM once.  Vectors are [system][Vh] int16 sites.
-// BG systems per thread (and per block); MINB resident blocks per SM
-template <int NL, int KIND, bool RECON, int BG, int MINB>
+// BG systems per thread (and per block); MINB resident blocks per SM; UNR
+// slots unrolled (NL: straight-line code; 1: a loop over the slots, less
+// code and fewer registers)
+template <int NL, int KIND, bool RECON, int BG, int MINB, int UNR = NL>
 __global__ void __launch_bounds__(QB, MINB)
 k_bhop(uint4 *__restrict__ out, const uint4 *__restrict__ src, const unsigned char *__restrict__ lk,
        const uint4 *__restrict__ same, Geom g, NbrGeom ng, int p, MixState *st, int nsys, int ngrp, double *part,
@@ -93,12 +95,13 @@ k_bhop(uint4 *__restrict__ out, const uint4 *__restrict__ src, const unsigned ch
   if (i < Vh) {
     int x[4];
     site_coords(g, i, p, x);
-    const int lex = ((x[0] * g.L[1] + x[1]) * g.L[2] + x[2]) * g.L[3] + x[3];
+    const int x0 = x[0], x1 = x[1], x2 = x[2], x3 = x[3];
+    const int lex = ((x0 * g.L[1] + x1) * g.L[2] + x2) * g.L[3] + x3;
     float2 a[BG][3];
 #pragma unroll
     for (int b = 0; b < BG; b++) a[b][0] = a[b][1] = a[b][2] = make_float2(0.f, 0.f);
     const unsigned char *gl = lk + (size_t)sb * q16_block_bytes(NL, RECON);
-#pragma unroll
+#pragma unroll UNR
     for (int k = 0; k < NL; k++) {
       const unsigned char *ls = gl + q16_slot_off(k, RECON);
       float2 U[9];
@@ -114,7 +117,9 @@ k_bhop(uint4 *__restrict__ out, const uint4 *__restrict__ src, const unsigned ch
         const uint2 uc = __ldcs(reinterpret_cast<const uint2 *>(ls + 32 * QB) + tid);
         sl = q16_link(ua, ub, uc, U);
       }
-      const int nbi = nbr_fast(ng, x, lex, slot_mu<NL>(k), slot_disp<NL>(k));
+      int nbi;
+      if constexpr (UNR == NL) nbi = nbr_fast(ng, x, lex, slot_mu<NL>(k), slot_disp<NL>(k));
+      else nbi = nbr_sel(ng, x0, x1, x2, x3, lex, slot_mu<NL>(k), slot_disp<NL>(k));
       uint4 nb[BG];
 #pragma unroll
       for (int b = 0; b < BG; b++) nb[b] = act[b] ? src[(i64)(j0 + b) * Vh + nbi] : make_uint4(0, 0, 0, 0);
@@ -240,27 +245,31 @@ k_bp(uint4 *__restrict__ p, const uint4 *__restrict__ r, i64 Vh, const MixState 
   SpQ16::store(p + o, i, Vh, pv);
 }
 
-// batched hop variants (option batch_kernel): systems per thread and the
-// register cap (resident blocks per SM).  At 32^4 with 16 systems a hop
-// takes 574 us with variant 1 (default), 605-679 us with 0, 2, 3, 5 and
-// 1074 us with 4 (8 systems per thread: 238 registers).  The kernel issues
-// ~60-90 instructions per system and slot and runs at ~55% issue
-// utilisation with 16-24 warps per SM; HBM traffic equals the compulsory
-// bytes (ncu), so it is instruction- and latency-bound, not HBM-bound.
+// batched hop variants (option batch_kernel): systems per thread, the
+// register cap (resident blocks per SM) and the slot unrolling.  At 32^4
+// with 16 systems a hop takes 531 us with variant 7 (8 systems per thread,
+// 3 blocks per SM, slot loop unrolled by 2; the default), 557-580 us with
+// 1, 6, 9, 10, 605-679 us with 0, 2, 3, 5, 622 us with 8 and 705-1074 us
+// with 11 and 4 (16 / 8 systems, fully unrolled: ~240 registers).  The
+// kernel issues ~60-90 instructions per system and slot at ~55% issue
+// utilisation; HBM traffic equals the compulsory bytes (ncu), so it is
+// instruction- and latency-bound, not HBM-bound.
 struct BhopShape { int bg, minb; };
-static const BhopShape kBhop[] = {{4, 1}, {4, 5}, {2, 8}, {2, 1}, {8, 1}, {4, 6}};
+static const BhopShape kBhop[] = {{4, 1}, {4, 5}, {2, 8}, {2, 1}, {8, 1}, {4, 6}, {4, 5}, {8, 3}, {8, 2},
+                                  {8, 3}, {8, 4}, {16, 2}};
 constexpr int N_BHOP = (int)(sizeof(kBhop) / sizeof(kBhop[0]));
 
-template <int KIND, int BG, int MINB>
+template <int KIND, int BG, int MINB, int UNR = 16>
 static void launch_bhop_t(int nl, bool recon, int ngrp, int nsb, uint4 *out, const uint4 *src,
                           const unsigned char *lk, const uint4 *same, const Geom &g, const NbrGeom &ng, int par,
                           MixState *st, int nsys, double *part, unsigned *count, float c_long) {
   Context &c = ctx();
   const int grid = ngrp * nsb;
 #define BH_ARGS out, src, lk, same, g, ng, par, st, nsys, ngrp, part, count, c_long
-  if (nl != 16) k_bhop<8, KIND, false, BG, MINB><<<grid, QB, 0, c.s>>>(BH_ARGS);
-  else if (recon) k_bhop<16, KIND, true, BG, MINB><<<grid, QB, 0, c.s>>>(BH_ARGS);
-  else k_bhop<16, KIND, false, BG, MINB><<<grid, QB, 0, c.s>>>(BH_ARGS);
+  constexpr int U8 = UNR < 8 ? UNR : 8;
+  if (nl != 16) k_bhop<8, KIND, false, BG, MINB, U8><<<grid, QB, 0, c.s>>>(BH_ARGS);
+  else if (recon) k_bhop<16, KIND, true, BG, MINB, UNR><<<grid, QB, 0, c.s>>>(BH_ARGS);
+  else k_bhop<16, KIND, false, BG, MINB, UNR><<<grid, QB, 0, c.s>>>(BH_ARGS);
 #undef BH_ARGS
 }
 
@@ -268,7 +277,7 @@ template <int KIND>
 static void launch_bhop(int variant, int nl, bool recon, int ngrp, int nsb, uint4 *out, const uint4 *src,
                         const unsigned char *lk, const uint4 *same, const Geom &g, const NbrGeom &ng, int par,
                         MixState *st, int nsys, double *part, unsigned *count, float c_long) {
-#define BH_CALL(B, M) launch_bhop_t<KIND, B, M>(nl, recon, ngrp, nsb, out, src, lk, same, g, ng, par, st, nsys, \
+#define BH_CALL(B, M, ...) launch_bhop_t<KIND, B, M, ##__VA_ARGS__>(nl, recon, ngrp, nsb, out, src, lk, same, g, ng, par, st, nsys, \
                                                 part, count, c_long)
   switch (variant) {
     case 1: BH_CALL(4, 5); break;
@@ -276,6 +285,12 @@ static void launch_bhop(int variant, int nl, bool recon, int ngrp, int nsb, uint
     case 3: BH_CALL(2, 1); break;
     case 4: BH_CALL(8, 1); break;
     case 5: BH_CALL(4, 6); break;
+    case 6: BH_CALL(4, 5, 2); break;   // slot loop unrolled by 2
+    case 7: BH_CALL(8, 3, 2); break;
+    case 8: BH_CALL(8, 2, 1); break;
+    case 9: BH_CALL(8, 3, 4); break;
+    case 10: BH_CALL(8, 4, 1); break;
+    case 11: BH_CALL(16, 2, 1); break;
     default: BH_CALL(4, 1); break;
   }
 #undef BH_CALL

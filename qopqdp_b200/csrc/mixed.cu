@@ -582,18 +582,6 @@ template <int N> __device__ __forceinline__ void cpa_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-// neighbour index with the direction chosen at run time (no indexed arrays)
-__device__ __forceinline__ int nbr_sel(const NbrGeom &n, int x0, int x1, int x2, int x3, int lex, int mu, int d) {
-  const int xm = mu == 0 ? x0 : mu == 1 ? x1 : mu == 2 ? x2 : x3;
-  const int Lm = mu == 0 ? n.L[0] : mu == 1 ? n.L[1] : mu == 2 ? n.L[2] : n.L[3];
-  const int sm = mu == 0 ? n.str[0] : mu == 1 ? n.str[1] : mu == 2 ? n.str[2] : n.str[3];
-  const int t = xm + d;
-  int off = d * sm;
-  if (t >= Lm) off -= Lm * sm;
-  else if (t < 0) off += Lm * sm;
-  return (lex + off) >> 1;
-}
-
 template <int NL, int KIND, bool RECON, int R, int MINB>
 __global__ void __launch_bounds__(QB, MINB)
 k_mix_hop_q16a(uint4 *__restrict__ out, const uint4 *__restrict__ src, const unsigned char *__restrict__ lk,

@@ -215,6 +215,18 @@ __device__ __forceinline__ int nbr_fast(const NbrGeom &n, const int x[4], int le
   return (lex + off) >> 1;
 }
 
+// neighbour index with the direction chosen at run time (no indexed arrays)
+__device__ __forceinline__ int nbr_sel(const NbrGeom &n, int x0, int x1, int x2, int x3, int lex, int mu, int d) {
+  const int xm = mu == 0 ? x0 : mu == 1 ? x1 : mu == 2 ? x2 : x3;
+  const int Lm = mu == 0 ? n.L[0] : mu == 1 ? n.L[1] : mu == 2 ? n.L[2] : n.L[3];
+  const int sm = mu == 0 ? n.str[0] : mu == 1 ? n.str[1] : mu == 2 ? n.str[2] : n.str[3];
+  const int t = xm + d;
+  int off = d * sm;
+  if (t >= Lm) off -= Lm * sm;
+  else if (t < 0) off += Lm * sm;
+  return (lex + off) >> 1;
+}
+
 // a += (link scale x site scale) x (integer link) (integer site): one slot
 __device__ __forceinline__ void q16_slot(const uint4 ua, const uint4 ub, const uint2 uc, const uint4 nb, float2 a[3]) {
   float2 v[3];

@@ -101,7 +101,7 @@ struct Options {
   int chunk = 16;                // iterations launched per host check
   int hop_kernel = 15;           // int16 hop variant (mixed.cu launch_q16); 15 measured fastest
   int recon_long = 1;            // int16 long links as two rows + det phase when exact
-  int batch_kernel = 1;          // batched int16 hop variant (batch.cu kBhop); 1 measured fastest
+  int batch_kernel = 7;          // batched int16 hop variant (batch.cu kBhop); 7 measured fastest
   int multi_shift = 0;           // int16 multi-mass: 1 = sloppy multi-shift CG before the batched refinement
   // QOP_hisq_links_set_opts (lib/hisq_links.c:4-78)
   int want_deps = 0, want_aux = 1, reunit_allow_svd = 1, reunit_svd_only = 0;
