@@ -21,6 +21,8 @@ Further workloads (one step = one QOP_D3_asqtad_invert_multi call, solved
 by the batched int16 solver, compared with the same call in FP64):
   --workload multimass   HISQ 24^3x48, one source, 12 masses sqrt(logspace(-4, 0))
   --workload multisrc    asqtad 32^4 (eps 0.4), 16 sources, mass 0.005
+  --workload small       F3 asqtad 8^4: the nine Dslash cases and the eo CG,
+                         GPU and oracle times, Dslash parity
   --workload serve       the solve service (QOPB_serve_*) with HISQ 16^4,
                          24^3x48 and 32^3x64 resident, Poisson arrivals
 """
@@ -59,7 +61,7 @@ def parse():
     ap.add_argument("--cpu-iters", type=int, default=12, help="CG iterations timed on the host")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--quick", action="store_true", help="skip FP64 baseline and e2e (development)")
-    ap.add_argument("--workload", default="single", choices=["single", "multimass", "multisrc", "serve"],
+    ap.add_argument("--workload", default="single", choices=["single", "multimass", "multisrc", "serve", "small"],
                     help="single: the headline solve; multimass / multisrc: batched invert_multi workloads; "
                          "serve: the solve service under Poisson load")
     ap.add_argument("--serve-burst", type=int, default=12, help="requests of the peak-throughput burst")
@@ -580,6 +582,97 @@ def run_multi(a):
         dist.destroy_process_group()
 
 
+def run_small(a):
+    """Plain asqtad in single precision (QOP_F3_*) on 8^4 (eps 0.3), m = 0.1:
+    the nine (eo_out, eo_in) Dslash cases and the eo-preconditioned CG to
+    |r|/|b| <= 1e-5 (rsqmin 1e-10), timed on the GPU (CUDA events, mean over
+    --steps repetitions after --warmup) and with the oracle on the host;
+    each Dslash checked against the oracle (F3 tolerance 2e-6 per site).
+    The whole problem is cache-resident: not an HBM measurement."""
+    import torch
+    torch.cuda.set_device(0)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from qopqdp_b200 import lattice as LT
+    from qopqdp_b200.qop import Qop, QOP_invert_arg_t, QOP_resid_arg_t, QOP_EVEN, load_library
+    L = (8, 8, 8, 8)
+    V = int(np.prod(L))
+    lat = O.Lattice(L)
+    U = lat.rephase_G(LT.random_gauge(L, 0.3, a.seed, device="cpu"), LT.BENCH_R0, LT.BENCH_BC, LT.BENCH_SIGNMASK)
+    fat, lng = lat.make_imp_links(LT.ASQTAD_BENCH_COEFFS, list(U), naik=True)
+    fat = [np.asarray(x, np.float32) for x in fat]
+    lng = [np.asarray(x, np.float32) for x in lng]
+    fo = O.Fla(lat, [x.astype(np.float64) for x in fat], [x.astype(np.float64) for x in lng])
+    q = Qop("F")
+    assert q.init(L) == 0
+    lib = load_library()
+    lib.QOPB_stream.restype = __import__("ctypes").c_void_p
+    stream = torch.cuda.ExternalStream(lib.QOPB_stream())
+    fla = q.create_L_from_raw(fat, lng)
+    src = LT.gaussian_vector(L, a.seed).astype(np.float32)
+    hin, hout = q.create_V(src), q.create_V(np.zeros_like(src))
+    mass = 0.1
+    m32 = float(np.float32(mass))
+
+    def ev():
+        e = torch.cuda.Event(enable_timing=True)
+        e.record(stream)
+        return e
+
+    cases, worst = {}, 0.0
+    for eo_out in (0, 1, 2):
+        for eo_in in (0, 1, 2):
+            for _ in range(a.warmup):
+                q.dslash(fla, mass, hout, hin, eo_out, eo_in)
+            e0 = ev()
+            for _ in range(a.steps):
+                q.dslash(fla, mass, hout, hin, eo_out, eo_in)
+            e1 = ev()
+            e1.synchronize()
+            got = q.extract_V(hout, V).astype(np.float64)
+            ref = fo.dslash(m32, src.astype(np.float64), eo_out, eo_in)
+            num = np.sqrt(((got - ref) ** 2).reshape(V, -1).sum(1))
+            den = np.sqrt((ref ** 2).reshape(V, -1).sum(1))
+            err = float(np.max(num[den > 0] / den[den > 0])) if (den > 0).any() else 0.0
+            worst = max(worst, err)
+            cases["%d,%d" % (eo_out, eo_in)] = {"us": 1e3 * e0.elapsed_time(e1) / a.steps, "max_site_rel_err": err}
+    # eo CG (reference algorithm, F3)
+    q.set_opts(prec_sloppy=64)
+    cg_ms, iters = [], 0
+    for k in range(a.warmup + a.steps):
+        q.dslash(fla, 0.0, hout, hout, QOP_EVEN, QOP_EVEN)
+        ia = QOP_invert_arg_t(1e9, 2000, 2000, 5, QOP_EVEN)
+        ra = QOP_resid_arg_t(1e-10, 0, 0, 0, 0, 0)
+        e0 = ev()
+        q.invert(fla, mass, hout, hin, ia, ra)
+        e1 = ev()
+        e1.synchronize()
+        if k >= a.warmup:
+            cg_ms.append(e0.elapsed_time(e1))
+            iters = ra.final_iter
+    # the oracle on the host: one Dslash (EVENODD) and the same CG
+    t0 = time.perf_counter()
+    for _ in range(20):
+        fo.dslash(m32, src.astype(np.float64), 2, 2)
+    cpu_dslash_us = (time.perf_counter() - t0) / 20 * 1e6
+    t0 = time.perf_counter()
+    ora = O.ResidArg(1e-10, 0, 0, 0, 0, 0)
+    fo.invert(m32, src.astype(np.float64), O.InvertArg(1e9, 2000, 2000, 5, 0), ora)
+    cpu_cg_ms = (time.perf_counter() - t0) * 1e3
+    line = {"metric": "F3 asqtad 8^4: Dslash us and eo CG ms", "value": float(np.mean(cg_ms)), "unit": "ms per CG solve",
+            "n_gpus": 1, "steps": a.steps, "warmup": a.warmup, "ms_per_step": float(np.mean(cg_ms)),
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "small", "lattice": L, "mass": mass, "rsqmin": 1e-10, "eps": 0.3,
+                       "note": "cache-resident, not an HBM measurement"},
+            "dslash": cases, "dslash_max_site_rel_err": worst, "cg_iters": iters, "oracle_cg_iters": ora.final_iter,
+            "cpu_baseline": {"dslash_us": cpu_dslash_us, "cg_ms": cpu_cg_ms, "kind": "port",
+                             "cores": O.get_threads()}}
+    print(json.dumps(line), flush=True)
+    q.destroy_V(hin)
+    q.destroy_V(hout)
+    q.destroy_L(fla)
+
+
 SERVE_LATTICES = [(16, 16, 16, 16), (24, 24, 24, 48), (32, 32, 32, 64)]
 
 
@@ -711,6 +804,8 @@ def main():
         run_reference(a)
     elif a.workload == "serve":
         run_serve(a)
+    elif a.workload == "small":
+        run_small(a)
     elif a.workload != "single":
         run_multi(a)
     else:

@@ -222,3 +222,65 @@ def test_mixed_multi_source(L, kind):
     for row in houts:
         q.destroy_V(row[0])
     q.destroy_L(fla)
+
+
+def _single_iters(q, fla, src, m, L):
+    ia = QOP_invert_arg_t(1e9, 20000, 20000, 5, 0)
+    ra = QOP_resid_arg_t(1e-20, 0, 0, 0, 0, 0)
+    hin, hout = q.create_V(src), q.create_V(np.zeros_like(src))
+    info = q.invert(fla, m, hout, hin, ia, ra)
+    got = q.extract_V(hout, int(np.prod(L)))
+    q.destroy_V(hin)
+    q.destroy_V(hout)
+    return info.status, ra.final_iter, got
+
+
+def test_every_hop_kernel_variant():
+    """Each selectable int16 hop kernel (option hop_kernel 0-19: plain,
+    TMA-staged, register-capped, persistent and cp.async-ring forms) solves
+    to the FP64 target; all share the decode and arithmetic order, so their
+    iteration counts agree within the reduction-order noise."""
+    L = (8, 8, 8, 8)
+    q = gpu_lattice(L, "D")
+    fat, lng, _, _ = hisq_links(L, 0.5, 9)
+    fo = O.Fla(O.Lattice(L), fat, lng)
+    fla = q.create_L_from_raw(fat, lng)
+    src = LT.gaussian_vector(L, 330)
+    its = {}
+    for v in range(20):
+        assert q.set_opts(prec_sloppy=16, hop_kernel=v) == 0
+        st, it, got = _single_iters(q, fla, src, 0.03, L)
+        assert st == 0
+        assert eo_residual(fo, 0.03, got, src, L, 0) <= 1.05e-20, v
+        its[v] = it
+    assert q.set_opts(hop_kernel=20) != 0                  # out of range
+    assert q.set_opts(prec_sloppy=64, hop_kernel=15) == 0
+    ref = its[15]
+    assert all(abs(i - ref) <= 0.03 * ref + 3 for i in its.values()), its
+    q.destroy_L(fla)
+
+
+def test_every_batch_kernel_variant():
+    """Each selectable batched hop (option batch_kernel 0-11) solves a
+    four-source batch to the FP64 target with the iteration counts of the
+    default variant."""
+    L = (8, 8, 8, 8)
+    q = gpu_lattice(L, "D")
+    fat, lng = asqtad_links(L, 0.4, 11)
+    fo = O.Fla(O.Lattice(L), fat, lng)
+    fla = q.create_L_from_raw(fat, lng)
+    srcs = [LT.gaussian_vector(L, 340 + s) for s in range(4)]
+    ms = [[0.03], [0.05], [0.03], [0.1]]
+    its = {}
+    for v in range(12):
+        assert q.set_opts(prec_sloppy=16, batch_kernel=v) == 0
+        info, ras, outs = _run_multi(q, fla, ms, srcs, 1e-20)
+        assert info.status == 0
+        for s in range(4):
+            assert eo_residual(fo, ms[s][0], outs[s][0], srcs[s], L, 0) <= 1.05e-20, (v, s)
+        its[v] = [r[0].final_iter for r in ras]
+    assert q.set_opts(batch_kernel=12) != 0
+    assert q.set_opts(prec_sloppy=64, batch_kernel=7) == 0
+    for v, it in its.items():
+        assert all(abs(a - b) <= 0.03 * b + 3 for a, b in zip(it, its[7])), its
+    q.destroy_L(fla)
