@@ -58,6 +58,8 @@ def lib():
         l.or_hisq_links.argtypes = [vp, DP, C.POINTER(DP), C.POINTER(DP), C.POINTER(DP), C.POINTER(DP)]
         l.or_hisq_links.restype = C.c_int
         l.or_fla_create.argtypes = [vp, C.POINTER(DP), C.POINTER(DP)]
+        l.or_asqtad_deriv.argtypes = [vp, DP, C.POINTER(DP), C.POINTER(DP), C.POINTER(DP), C.POINTER(DP)]
+        l.or_asqtad_force.argtypes = [vp, DP, C.POINTER(DP), C.POINTER(DP), DP, C.POINTER(DP), C.c_int]
         l.or_fla_create.restype = vp
         l.or_fla_destroy.argtypes = [vp]
         l.or_dslash.argtypes = [vp, C.c_double, DP, DP, C.c_int, C.c_int]
@@ -118,6 +120,27 @@ class Lattice:
         c = np.array(coeffs, dtype=np.float64)
         lib().or_make_imp_links(self.h, _p(c), _p4(gauge), _p4(gauge), _p4(fat), _p4(lng) if naik else None)
         return fat, lng
+
+    def asqtad_deriv(self, coeffs, gauge, midF, midN=None):
+        """deriv_mu = dE/dU_mu for E = Re sum tr[midF^+ fat + midN^+ long]."""
+        gauge = [f64(a) for a in gauge]
+        midF = [f64(a) for a in midF]
+        midN = [f64(a) for a in midN] if midN is not None else None
+        der = [np.zeros_like(gauge[0]) for _ in range(4)]
+        c = np.array(coeffs, dtype=np.float64)
+        lib().or_asqtad_deriv(self.h, _p(c), _p4(gauge), _p4(midF), _p4(midN) if midN is not None else None, _p4(der))
+        return der
+
+    def asqtad_force(self, coeffs, gauge, eps, xs, force=None):
+        """force_mu += -2 TA(U_mu deriv_mu^+) for the outer products of xs."""
+        gauge = [f64(a) for a in gauge]
+        force = [np.zeros_like(gauge[0]) for _ in range(4)] if force is None else [f64(a).copy() for a in force]
+        xs = [f64(x) for x in xs]
+        xp = (DP * len(xs))(*[_p(x) for x in xs])
+        e = np.array(eps, dtype=np.float64)
+        c = np.array(coeffs, dtype=np.float64)
+        lib().or_asqtad_force(self.h, _p(c), _p4(gauge), _p4(force), _p(e), xp, len(xs))
+        return force
 
     def hisq_links(self, hcoef, gauge, want_W=False):
         gauge = [f64(a) for a in gauge]

@@ -1172,3 +1172,154 @@ void or_invert_multi(or_fla *f, or_invert_arg *ia, or_resid_arg **ra[], double *
   if (final_flop) *final_flop = flop;
   free(cgp);
 }
+
+/* ------------------------------------------------------------------ */
+/* asqtad fermion force: lib/asqtad_force_p.c:16-64 (entry points),     */
+/* lib/asqtad_force_fnmat_p.c:4-43 (outer products, scale -1), :491-513 */
+/* (sign flip on odd sites), :516-546 (force += -2 antiherm(U deriv^+)). */
+/* The derivative of the smeared links is formed here by reverse-mode    */
+/* differentiation of make_imp_links' staple sums (the adjoint of every  */
+/* staple application, in reverse order); the reference forms the same   */
+/* derivative with its staple / side-force recursion (:85-359).          */
+/* ------------------------------------------------------------------ */
+static inline void m_acc(dc *r, const dc *a, double c) { for (int e = 0; e < 9; e++) r[e] += c * a[e]; }
+
+/* adjoint of fl += coef*staple(in; mu, nu) with respect to `in`:
+   Gin(z) += coef [U_nu(z-nu)^+ G(z-nu) U_nu(z-nu+mu) + U_nu(z) G(z+nu) U_nu(z+mu)^+] */
+static void adj_staple_in(const or_lat *g, dc *Gin, const dc *G, int mu, int nu, double coef, dc **U) {
+#pragma omp parallel for
+  for (long z = 0; z < g->V; z++) {
+    dc t[9], r[9];
+    long zmn = nbr(g, z, nu, -1), zmnpm = nbr(g, zmn, mu, 1);
+    long zpn = nbr(g, z, nu, 1), zpm = nbr(g, z, mu, 1);
+    m_mul_an(t, U[nu] + 9 * zmn, G + 9 * zmn);
+    m_mul(r, t, U[nu] + 9 * zmnpm);
+    m_acc(Gin + 9 * z, r, coef);
+    m_mul(t, U[nu] + 9 * z, G + 9 * zpn);
+    m_mul_na(r, t, U[nu] + 9 * zpm);
+    m_acc(Gin + 9 * z, r, coef);
+  }
+}
+
+/* adjoint of fl += coef*staple(in; mu, nu) with respect to U_nu:
+   GU(z) += coef [G(z) U(z+mu) in(z+nu)^+ + G(z-mu)^+ U(z-mu) in(z-mu+nu)
+                  + in(z-mu)^+ U(z-mu) G(z-mu+nu) + in(z) U(z+mu) G(z+nu)^+],  U = U_nu */
+static void adj_staple_link(const or_lat *g, dc *GU, const dc *G, const dc *in, int mu, int nu, double coef,
+                            dc **U) {
+#pragma omp parallel for
+  for (long z = 0; z < g->V; z++) {
+    dc t[9], r[9];
+    long zpm = nbr(g, z, mu, 1), zpn = nbr(g, z, nu, 1);
+    long zmm = nbr(g, z, mu, -1), zmmpn = nbr(g, zmm, nu, 1);
+    const dc *Un = U[nu];
+    m_mul(t, G + 9 * z, Un + 9 * zpm);      m_mul_na(r, t, in + 9 * zpn);   m_acc(GU + 9 * z, r, coef);
+    m_mul_an(t, G + 9 * zmm, Un + 9 * zmm); m_mul(r, t, in + 9 * zmmpn);    m_acc(GU + 9 * z, r, coef);
+    m_mul_an(t, in + 9 * zmm, Un + 9 * zmm); m_mul(r, t, G + 9 * zmmpn);    m_acc(GU + 9 * z, r, coef);
+    m_mul(t, in + 9 * z, Un + 9 * zpm);     m_mul_na(r, t, G + 9 * zpn);    m_acc(GU + 9 * z, r, coef);
+  }
+}
+
+void or_asqtad_deriv(const or_lat *g, const double coef[6], double *Ur[4], double *midFr[4], double *midNr[4],
+                     double *derivr[4]) {
+  dc *U[4], *M[4], *D[4];
+  for (int i = 0; i < 4; i++) { U[i] = (dc *)Ur[i]; M[i] = (dc *)midFr[i]; D[i] = (dc *)derivr[i]; }
+  const double c1 = coef[0] - 6 * coef[4], c3 = coef[1], c5 = coef[2], c7 = coef[3], cL = coef[4];
+  const int have5 = c5 != 0 || c7 != 0 || cL != 0, have3 = c3 != 0 || have5;
+  const size_t fsz = sizeof(dc) * 9 * g->V;
+  dc *S3 = calloc(9 * g->V, sizeof(dc)), *S5 = calloc(9 * g->V, sizeof(dc));
+  dc *G3 = malloc(fsz), *G5 = malloc(fsz), *junk = calloc(9 * g->V, sizeof(dc));
+  for (int mu = 0; mu < 4; mu++) {
+
+    for (long s = 0; s < 9 * g->V; s++) D[mu][s] += c1 * M[mu][s];
+    if (!have3) continue;
+    for (int nu = 0; nu < 4; nu++) {
+      if (nu == mu) continue;
+      memset(junk, 0, fsz);
+      gen_staple(g, S3, mu, nu, U[mu], 0.0, U, junk);              /* S3 = staple(U_mu; mu, nu) */
+      for (long s = 0; s < 9 * g->V; s++) G3[s] = c3 * M[mu][s];
+      if (cL != 0) {                                                /* fl += cL staple(S3; mu, nu) */
+        adj_staple_in(g, G3, M[mu], mu, nu, cL, U);
+        adj_staple_link(g, D[nu], M[mu], S3, mu, nu, cL, U);
+      }
+      if (c5 != 0 || c7 != 0) {
+        for (int rho = 0; rho < 4; rho++) {
+          if (rho == mu || rho == nu) continue;
+          memset(junk, 0, fsz);
+          gen_staple(g, S5, mu, rho, S3, 0.0, U, junk);           /* S5 = staple(S3; mu, rho) */
+          for (long s = 0; s < 9 * g->V; s++) G5[s] = c5 * M[mu][s];
+          if (c7 != 0)
+            for (int sig = 0; sig < 4; sig++) {
+              if (sig == mu || sig == nu || sig == rho) continue;   /* fl += c7 staple(S5; mu, sig) */
+              adj_staple_in(g, G5, M[mu], mu, sig, c7, U);
+              adj_staple_link(g, D[sig], M[mu], S5, mu, sig, c7, U);
+            }
+          adj_staple_in(g, G3, G5, mu, rho, 1.0, U);
+          adj_staple_link(g, D[rho], G5, S3, mu, rho, 1.0, U);
+        }
+      }
+      adj_staple_in(g, D[mu], G3, mu, nu, 1.0, U);
+      adj_staple_link(g, D[nu], G3, U[mu], mu, nu, 1.0, U);
+    }
+  }
+  if (midNr && coef[5] != 0) {                                      /* long = naik U U U */
+    const double cn = coef[5];
+    for (int mu = 0; mu < 4; mu++) {
+      const dc *N = (const dc *)midNr[mu], *Um = U[mu];
+#pragma omp parallel for
+      for (long z = 0; z < g->V; z++) {
+        dc t[9], r[9];
+        long p1 = nbr(g, z, mu, 1), p2 = nbr(g, p1, mu, 1);
+        long m1 = nbr(g, z, mu, -1), m2 = nbr(g, m1, mu, -1);
+        m_mul(t, Um + 9 * p1, Um + 9 * p2);   m_mul_na(r, N + 9 * z, t);       m_acc(D[mu] + 9 * z, r, cn);
+        m_mul_an(t, Um + 9 * m1, N + 9 * m1); m_mul_na(r, t, Um + 9 * p1);     m_acc(D[mu] + 9 * z, r, cn);
+        m_mul(t, Um + 9 * m2, Um + 9 * m1);   m_mul_an(r, t, N + 9 * m2);      m_acc(D[mu] + 9 * z, r, cn);
+      }
+    }
+  }
+  free(S3); free(S5); free(G3); free(G5); free(junk);
+}
+
+void or_asqtad_force(const or_lat *g, const double coef[6], double *Ur[4], double *forcer[4], const double *eps,
+                     double *xr[], int nsrc) {
+  const size_t n = 9 * (size_t)g->V;
+  double *mid[8], *der[4];
+  for (int i = 0; i < 8; i++) mid[i] = calloc(2 * n, sizeof(double));
+  for (int i = 0; i < 4; i++) der[i] = calloc(2 * n, sizeof(double));
+  for (int mu = 0; mu < 4; mu++) {
+    dc *MF = (dc *)mid[mu], *MN = (dc *)mid[4 + mu];
+#pragma omp parallel for
+    for (long z = 0; z < g->V; z++) {
+      const int *xc = g->x + 4 * z;
+      const double sgn = ((xc[0] + xc[1] + xc[2] + xc[3]) & 1) ? 1.0 : -1.0;   /* -1 times (-1 on odd) */
+      long z1 = nbr(g, z, mu, 1), z3 = nbr(g, z, mu, 3);
+      for (int i = 0; i < nsrc; i++) {
+        const dc *x = (const dc *)xr[i];
+        for (int a = 0; a < 3; a++)
+          for (int b = 0; b < 3; b++) {
+            MF[9 * z + 3 * a + b] += sgn * eps[i] * x[3 * z + a] * conj(x[3 * z1 + b]);
+            MN[9 * z + 3 * a + b] += sgn * eps[i] * x[3 * z + a] * conj(x[3 * z3 + b]);
+          }
+      }
+    }
+  }
+  or_asqtad_deriv(g, coef, Ur, mid, coef[5] != 0 ? mid + 4 : NULL, der);
+  for (int mu = 0; mu < 4; mu++) {
+    const dc *Um = (const dc *)Ur[mu], *Dm = (const dc *)der[mu];
+    dc *F = (dc *)forcer[mu];
+#pragma omp parallel for
+    for (long z = 0; z < g->V; z++) {
+      dc a[9];
+      m_mul_na(a, Um + 9 * z, Dm + 9 * z);                 /* U deriv^+ */
+      dc tr = 0;
+      for (int k = 0; k < 3; k++) tr += a[4 * k] - conj(a[4 * k]);
+      for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) {
+          dc ta = 0.5 * (a[3 * i + j] - conj(a[3 * j + i]));
+          if (i == j) ta -= tr / 6.0;
+          F[9 * z + 3 * i + j] += -2.0 * ta;
+        }
+    }
+  }
+  for (int i = 0; i < 8; i++) free(mid[i]);
+  for (int i = 0; i < 4; i++) free(der[i]);
+}

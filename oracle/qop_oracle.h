@@ -82,6 +82,19 @@ void or_solve_multi(or_fla *f, or_invert_arg *ia, or_resid_arg *ra[],
                     double masses[], double *out[], double *in[], int nsolve,
                     double *final_flop);
 
+/* asqtad fermion force (lib/asqtad_force_p.c:16-64, asqtad_force_fnmat_p.c).
+   deriv: the derivative of
+     E(U) = Re sum_{x,mu} tr[ midF_mu(x)^+ fat_mu(x) + midN_mu(x)^+ long_mu(x) ]
+   with (fat, long) = make_imp_links(coef, U, U), in the convention
+   dE = Re sum tr[ deriv^+ dU ]; midN may be NULL (no Naik term).
+   force: the outer products midF_mu(x) = -s(x) sum_i eps_i x_i(x) x_i(x+mu)^+
+   (midN with x+3mu; s = +1 even, -1 odd sites), deriv, and
+   force_mu += -2 TA(U_mu deriv_mu^+), TA the traceless anti-Hermitian part. */
+void or_asqtad_deriv(const or_lat *g, const double coef[6], double *U[4],
+                     double *midF[4], double *midN[4], double *deriv[4]);
+void or_asqtad_force(const or_lat *g, const double coef[6], double *U[4],
+                     double *force[4], const double *eps, double *x[], int nsrc);
+
 /* threads used by OpenMP regions (0 = leave default) */
 void or_set_threads(int n);
 int or_get_threads(void);

@@ -155,3 +155,85 @@ def test_evenodd_solve_and_multimass():
     outs, _ = fo.invert_multi([ms], [src], O.InvertArg(1e9, 8000, 1000, 20, 0), ras)
     for j, m in enumerate(ms):
         assert eo_residual(fo, m, outs[0][j], src, L, 0) <= 1e-18 * 1.05
+
+
+# ---------------------------------------------------------------- fermion force
+def _shift(L, mu, d):
+    X = LT.raw_coords(L)
+    Y = X.copy()
+    Y[:, mu] = (Y[:, mu] + d) % L[mu]
+    return LT.raw_index(L, Y)
+
+
+def _cgauss(rng, shape):
+    return rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+
+
+def _E(lat, coef, U, midF, midN):
+    fat, lng = lat.make_imp_links(coef, U, naik=True)
+    e = 0.0
+    for mu in range(4):
+        e += np.sum(np.conj(LT.to_complex(midF[mu])) * LT.to_complex(fat[mu])).real
+        e += np.sum(np.conj(LT.to_complex(midN[mu])) * LT.to_complex(lng[mu])).real
+    return e
+
+
+@pytest.mark.parametrize("coef", [(1.0, 0.1, 0.1, 0.1, 0.1, 0.1), (0.7, -0.23, 0.31, -0.17, 0.29, -0.13)])
+def test_asqtad_deriv_is_the_derivative_of_the_smeared_links(coef):
+    """deriv = dE/dU for E = Re sum tr[midF^+ fat + midN^+ long], fat/long from
+    make_imp_links (one-link, 3-, 5-, 7-staple, Lepage and Naik terms):
+    central finite differences along random directions agree to 1e-7."""
+    L = (4, 4, 4, 6)
+    V = int(np.prod(L))
+    lat = O.Lattice(L)
+    rng = np.random.default_rng(3)
+    U = [np.asarray(u) for u in gauge(L, 0.3, 5)]
+    midF = [LT.from_complex(_cgauss(rng, (V, 3, 3))) for _ in range(4)]
+    midN = [LT.from_complex(_cgauss(rng, (V, 3, 3))) for _ in range(4)]
+    der = lat.asqtad_deriv(coef, U, midF, midN)
+    for trial in range(2):
+        dU = [_cgauss(rng, (V, 3, 3)) for _ in range(4)]
+        h = 1e-5
+        Up = [LT.from_complex(LT.to_complex(U[m]) + h * dU[m]) for m in range(4)]
+        Um = [LT.from_complex(LT.to_complex(U[m]) - h * dU[m]) for m in range(4)]
+        fd = (_E(lat, coef, Up, midF, midN) - _E(lat, coef, Um, midF, midN)) / (2 * h)
+        an = sum(np.sum(np.conj(LT.to_complex(der[m])) * dU[m]).real for m in range(4))
+        assert abs(fd - an) <= 1e-7 * abs(an), (fd, an)
+
+
+def test_asqtad_force_outer_products_and_projection():
+    """force_mu = -2 TA(U_mu deriv_mu^+) with deriv from the outer products
+    midF_mu(x) = -s(x) sum_i eps_i x_i(x) x_i(x+mu)^+ (x+3mu for Naik),
+    s = -1 on odd sites (lib/asqtad_force_fnmat_p.c:4-43, :491-546); the result
+    is traceless anti-Hermitian and accumulates into the force field."""
+    L = (4, 4, 4, 6)
+    V = int(np.prod(L))
+    lat = O.Lattice(L)
+    coef = (1.0, 0.1, 0.1, 0.1, 0.1, 0.1)
+    U = [np.asarray(u) for u in gauge(L, 0.3, 5)]
+    xs = [LT.gaussian_vector(L, 70 + i) for i in range(2)]
+    eps = [0.7, -0.4]
+    f0 = [LT.from_complex(_cgauss(np.random.default_rng(1), (V, 3, 3))) for _ in range(4)]
+    F = lat.asqtad_force(coef, U, eps, xs, force=f0)
+    sgn = np.where(LT.parity_mask(L), -1.0, 1.0)
+    midF, midN = [], []
+    for mu in range(4):
+        mf = np.zeros((V, 3, 3), complex)
+        mn = np.zeros((V, 3, 3), complex)
+        for e, x in zip(eps, xs):
+            xc = LT.to_complex(x)
+            mf += e * np.einsum("va,vb->vab", xc, np.conj(xc[_shift(L, mu, 1)]))
+            mn += e * np.einsum("va,vb->vab", xc, np.conj(xc[_shift(L, mu, 3)]))
+        midF.append(LT.from_complex(sgn[:, None, None] * mf))
+        midN.append(LT.from_complex(sgn[:, None, None] * mn))
+    der = lat.asqtad_deriv(coef, U, midF, midN)
+    for mu in range(4):
+        A = LT.to_complex(U[mu]) @ np.conj(np.transpose(LT.to_complex(der[mu]), (0, 2, 1)))
+        T = 0.5 * (A - np.conj(np.transpose(A, (0, 2, 1))))
+        T -= np.trace(T, axis1=1, axis2=2)[:, None, None] / 3 * np.eye(3)
+        expect = LT.to_complex(f0[mu]) - 2 * T
+        got = LT.to_complex(F[mu])
+        assert np.max(np.abs(got - expect)) <= 1e-12 * np.max(np.abs(expect))
+        G = got - LT.to_complex(f0[mu])
+        assert np.max(np.abs(G + np.conj(np.transpose(G, (0, 2, 1))))) <= 1e-12 * np.max(np.abs(G))
+        assert np.max(np.abs(np.trace(G, axis1=1, axis2=2))) <= 1e-12 * np.max(np.abs(G))
