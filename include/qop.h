@@ -186,6 +186,8 @@ int QOP_node_index_raw_G(int coords[], QOP_evenodd_t evenodd);
 int QOP_sites_on_node_raw_V(QOP_evenodd_t evenodd);
 int QOP_sites_on_node_raw_G(QOP_evenodd_t evenodd);
 QOP_status_t QOP_asqtad_invert_set_opts(QOP_opt_t opts[], int nopts);
+/* fermion-force options fnmat_src_min, veclength (lib/asqtad_force.c:3-41) */
+QOP_status_t QOP_asqtad_force_set_opts(QOP_opt_t opts[], int nopts);
 QOP_status_t QOP_hisq_invert_set_opts(QOP_opt_t opts[], int nopts);
 QOP_status_t QOP_hisq_links_set_opts(QOP_opt_t opts[], int nopts);
 
@@ -195,6 +197,7 @@ typedef struct QOP_##PC##_ColorVector_struct        QOP_##PC##_ColorVector;    \
 typedef struct QOP_##PC##_GaugeField_struct         QOP_##PC##_GaugeField;     \
 typedef struct QOP_##PC##_FermionLinksAsqtad_struct QOP_##PC##_FermionLinksAsqtad; \
 typedef struct QOP_##PC##_FermionLinksHisq_struct   QOP_##PC##_FermionLinksHisq; \
+typedef struct QOP_##PC##_Force_struct              QOP_##PC##_Force;          \
 /* fields (qop_f3.h:52-66, 115) */                                             \
 QOP_##PC##_ColorVector *QOP_##PC##_create_V_from_raw(REAL *src, QOP_evenodd_t evenodd); \
 void QOP_##PC##_extract_V_to_raw(REAL *dest, QOP_##PC##_ColorVector *src, QOP_evenodd_t evenodd); \
@@ -243,6 +246,16 @@ void QOP_##PC##_asqtad_invert_multi(QOP_info_t *info,                          \
     QOP_##PC##_FermionLinksAsqtad *asqtad, QOP_invert_arg_t *inv_arg,          \
     QOP_resid_arg_t **res_arg[], REAL *masses[], int nmass[],                  \
     QOP_##PC##_ColorVector **out_pt[], QOP_##PC##_ColorVector *in_pt[], int nsrc); \
+/* force fields and the asqtad fermion force (qop_pc.h:53-67, 435-448) */     \
+QOP_##PC##_Force *QOP_##PC##_create_F_from_raw(REAL *force[], QOP_evenodd_t evenodd); \
+void QOP_##PC##_extract_F_to_raw(REAL *dest[], QOP_##PC##_Force *src, QOP_evenodd_t evenodd); \
+void QOP_##PC##_destroy_F(QOP_##PC##_Force *field);                            \
+void QOP_##PC##_asqtad_force(QOP_info_t *info, QOP_##PC##_GaugeField *gauge,   \
+    QOP_##PC##_Force *force, QOP_asqtad_coeffs_t *coeffs, REAL eps,            \
+    QOP_##PC##_ColorVector *in_pt);                                            \
+void QOP_##PC##_asqtad_force_multi(QOP_info_t *info, QOP_##PC##_GaugeField *gauge, \
+    QOP_##PC##_Force *force, QOP_asqtad_coeffs_t *coef, REAL eps[],            \
+    QOP_##PC##_ColorVector *in_pt[], int nsrc);                                \
 /* HISQ links (qop_f3.h:473-483) */                                            \
 QOP_##PC##_FermionLinksHisq *QOP_##PC##_hisq_create_L_from_G(QOP_info_t *info, \
     QOP_hisq_coeffs_t *coeffs, QOP_##PC##_GaugeField *gauge);                  \
@@ -274,6 +287,12 @@ typedef QOP_D_Real QOP_Real;
 #define QOP_extract_V_to_raw            QOPB_GEN(extract_V_to_raw)
 #define QOP_destroy_V                   QOPB_GEN(destroy_V)
 #define QOP_create_G_from_raw           QOPB_GEN(create_G_from_raw)
+#define QOP_Force                       QOPB_GEN(Force)
+#define QOP_create_F_from_raw           QOPB_GEN(create_F_from_raw)
+#define QOP_extract_F_to_raw            QOPB_GEN(extract_F_to_raw)
+#define QOP_destroy_F                   QOPB_GEN(destroy_F)
+#define QOP_asqtad_force                QOPB_GEN(asqtad_force)
+#define QOP_asqtad_force_multi          QOPB_GEN(asqtad_force_multi)
 #define QOP_extract_G_to_raw            QOPB_GEN(extract_G_to_raw)
 #define QOP_destroy_G                   QOPB_GEN(destroy_G)
 #define QOP_rephase_G                   QOPB_GEN(rephase_G)

@@ -330,3 +330,63 @@ extern "C" QOP_F3_FermionLinksAsqtad *QOP_FD3_asqtad_create_L_from_L(QOP_D3_Ferm
   return reinterpret_cast<QOP_F3_FermionLinksAsqtad *>(f);
   CATCH(nullptr, nullptr)
 }
+
+// ---------------------------------------------------------------- fermion force
+// Force fields share the gauge-field layout ([4 mu][2][9][Vh]); the force
+// accumulates into the handle as in the reference (asqtad_force_fnmat_p.c:536-538).
+namespace {
+template <typename T, typename R>
+void force_multi(QOP_info_t *info, GaugeT<T> *G, GaugeT<T> *F, QOP_asqtad_coeffs_t *coef, const R *eps,
+                 VecT<T> *const *in, int nsrc) {
+  require_init("asqtad_force");
+  need_handle<T>(G, "GaugeField");
+  need_handle<T>(F, "Force");
+  if (!coef || !eps || !in || nsrc < 1) fail(QOP_FAIL, "asqtad_force: NULL coefficients / eps / sources or nsrc < 1");
+  std::vector<double> e(nsrc);
+  for (int i = 0; i < nsrc; i++) {
+    need_handle<T>(in[i], "ColorVector");
+    e[i] = (double)eps[i];
+  }
+  asqtad_force<T>(info, G, F, coef, e.data(), in, nsrc);
+}
+}  // namespace
+
+#define QOPB_DEFINE_FORCE(PC, T, REAL)                                                                            \
+  extern "C" QOP_##PC##_Force *QOP_##PC##_create_F_from_raw(REAL *force[], QOP_evenodd_t eo) {                     \
+    TRY return reinterpret_cast<QOP_##PC##_Force *>(create_G<T, REAL>(force, eo)); CATCH(nullptr, nullptr)          \
+  }                                                                                                                 \
+  extern "C" void QOP_##PC##_extract_F_to_raw(REAL *dest[], QOP_##PC##_Force *src, QOP_evenodd_t eo) {            \
+    TRY extract_G<T, REAL>(dest, reinterpret_cast<GaugeT<T> *>(src), eo); CATCHV(nullptr)                          \
+  }                                                                                                                 \
+  extern "C" void QOP_##PC##_destroy_F(QOP_##PC##_Force *F) {                                                     \
+    TRY gauge_destroy<T>(reinterpret_cast<GaugeT<T> *>(F)); CATCHV(nullptr)                                         \
+  }                                                                                                                 \
+  extern "C" void QOP_##PC##_asqtad_force_multi(QOP_info_t *info, QOP_##PC##_GaugeField *gauge,                   \
+                                                QOP_##PC##_Force *force, QOP_asqtad_coeffs_t *coef, REAL eps[],   \
+                                                QOP_##PC##_ColorVector *in_pt[], int nsrc) {                      \
+    TRY force_multi<T, REAL>(info, ig<T>(gauge), reinterpret_cast<GaugeT<T> *>(force), coef, eps,                  \
+                             reinterpret_cast<VecT<T> *const *>(in_pt), nsrc);                                     \
+    CATCHV(info)                                                                                                    \
+  }                                                                                                                 \
+  extern "C" void QOP_##PC##_asqtad_force(QOP_info_t *info, QOP_##PC##_GaugeField *gauge, QOP_##PC##_Force *force, \
+                                          QOP_asqtad_coeffs_t *coef, REAL eps, QOP_##PC##_ColorVector *in_pt) {   \
+    QOP_##PC##_asqtad_force_multi(info, gauge, force, coef, &eps, &in_pt, 1);                                      \
+  }
+
+QOPB_DEFINE_FORCE(F3, float, float)
+QOPB_DEFINE_FORCE(D3, double, double)
+
+// lib/asqtad_force.c:19-41: validated and kept; the device force has one
+// algorithm for every number of sources, so they select nothing here
+extern "C" QOP_status_t QOP_asqtad_force_set_opts(QOP_opt_t opts[], int nopts) {
+  int fsm = ctx().opt.force_fnmat_src_min, vl = ctx().opt.force_veclength;
+  for (int i = 0; i < nopts; i++) {
+    if (!opts[i].tag) continue;
+    if (!strcmp(opts[i].tag, "fnmat_src_min")) fsm = (int)opts[i].value;
+    else if (!strcmp(opts[i].tag, "veclength")) vl = (int)opts[i].value;
+  }
+  if (fsm < 0 || vl <= 0) return QOP_FAIL;
+  ctx().opt.force_fnmat_src_min = fsm;
+  ctx().opt.force_veclength = vl;
+  return QOP_SUCCESS;
+}

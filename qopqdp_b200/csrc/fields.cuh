@@ -28,4 +28,9 @@ template <typename T> FlaT<T> *fla_scaled_copy(FlaT<T> *src, double s);
 template <typename T> void fla_peq(FlaT<T> *f, FlaT<T> *g);
 void sloppy_invalidate(void *fla_any);   // drop reduced-precision copies (mixed.cu)
 
+// force.cu: F_mu += -2 TA(U_mu deriv_mu^+) for the sources x (eps weights)
+template <typename T>
+void asqtad_force(QOP_info_t *info, GaugeT<T> *G, GaugeT<T> *F, const QOP_asqtad_coeffs_t *cf, const double *eps,
+                  VecT<T> *const *x, int nsrc);
+
 }  // namespace qopb

@@ -1,0 +1,295 @@
+// force.cu -- asqtad fermion force on the device.
+// Reference: lib/asqtad_force_p.c:16-64 (QOP_asqtad_force / _multi),
+// lib/asqtad_force_fnmat_p.c:4-43 (outer products of the sources, scale -1),
+// :491-513 (sign flip on odd sites), :516-546 (force += -2 antiherm(U deriv^+)).
+//
+// deriv_mu is the derivative of
+//   E(U) = Re sum_{x,mu} tr[ midF_mu(x)^+ fat_mu(x) + midN_mu(x)^+ long_mu(x) ]
+// with (fat, long) = make_imp_links(U), in the convention
+// dE = Re sum tr[deriv^+ dU].  It is formed by reverse-mode differentiation
+// of the staple sums of make_imp_links (links.cu): for every staple
+// application out += c staple(in; mu, nu) the adjoint kernels add the
+// contributions to the adjoint of `in` and of U_nu, in the reverse order of
+// the forward sums (7-staples, 5-staples, Lepage, 3-staples, one-link), and
+// the Naik products add theirs.  Every adjoint kernel is written in gather
+// form (each thread owns one output site and reads its neighbours), so no
+// atomics are needed and results are deterministic.  Everything runs in
+// FP64; the result is rounded once into the force handle's precision.
+#include "fields.cuh"
+#include "mat3.cuh"
+#include <vector>
+
+namespace qopb {
+namespace {
+
+__device__ __forceinline__ void site_of(const Geom &g, i64 s, int &p, int &i, int x[4]) {
+  p = (int)(s / g.Vh);
+  i = (int)(s % g.Vh);
+  site_coords(g, i, p, x);
+}
+__device__ __forceinline__ void nbr_pi(const Geom &g, const int x[4], int mu, int d, int &p, int &i) {
+  int y[4];
+  shifted(g, x, mu, d, y);
+  par_idx(g, y, p, i);
+}
+__device__ __forceinline__ M3 ldf(const double2 *f, const Geom &g, int p, int i) { return ld3(fptr(f, g, p, i), g.Vh); }
+__device__ __forceinline__ void accf(double2 *f, const Geom &g, int p, int i, const M3 &m, double c) {
+  double2 *b = f + (i64)p * 9 * g.Vh + i;
+#pragma unroll
+  for (int e = 0; e < 9; e++) {
+    double2 v = b[e * g.Vh];
+    b[e * g.Vh] = make_double2(v.x + c * m.e[e].x, v.y + c * m.e[e].y);
+  }
+}
+
+// out = staple(in; mu, nu) = U_nu(x) in(x+nu) U_nu(x+mu)^+ + U_nu(y)^+ in(y) U_nu(y+mu), y = x-nu
+__global__ void k_fstaple(double2 *out, const double2 *in, const double2 *Unu, int mu, int nu, Geom g) {
+  const i64 s = blockIdx.x * (i64)blockDim.x + threadIdx.x;
+  if (s >= 2 * g.Vh) return;
+  int p, i, x[4], pn, in_, pm, im, py, iy, pym, iym, yy[4];
+  site_of(g, s, p, i, x);
+  nbr_pi(g, x, nu, 1, pn, in_);
+  nbr_pi(g, x, mu, 1, pm, im);
+  shifted(g, x, nu, -1, yy);
+  par_idx(g, yy, py, iy);
+  nbr_pi(g, yy, mu, 1, pym, iym);
+  M3 up = mul(ldf(Unu, g, p, i), mul_na(ldf(in, g, pn, in_), ldf(Unu, g, pm, im)));
+  M3 lo = mul(mul_an(ldf(Unu, g, py, iy), ldf(in, g, py, iy)), ldf(Unu, g, pym, iym));
+#pragma unroll
+  for (int e = 0; e < 9; e++) up.e[e] = make_double2(up.e[e].x + lo.e[e].x, up.e[e].y + lo.e[e].y);
+  st3(out + (i64)p * 9 * g.Vh + i, g.Vh, up);
+}
+
+// adjoint of `in` for out += c staple(in; mu, nu):
+// Gin(z) += c [U_nu(z-nu)^+ G(z-nu) U_nu(z-nu+mu) + U_nu(z) G(z+nu) U_nu(z+mu)^+]
+__global__ void k_adj_in(double2 *Gin, const double2 *G, const double2 *Unu, int mu, int nu, double c, Geom g) {
+  const i64 s = blockIdx.x * (i64)blockDim.x + threadIdx.x;
+  if (s >= 2 * g.Vh) return;
+  int p, i, z[4], a, ai, b, bi, pn, in_, pm, im, y[4];
+  site_of(g, s, p, i, z);
+  shifted(g, z, nu, -1, y);
+  par_idx(g, y, a, ai);                 // z - nu
+  nbr_pi(g, y, mu, 1, b, bi);           // z - nu + mu
+  nbr_pi(g, z, nu, 1, pn, in_);         // z + nu
+  nbr_pi(g, z, mu, 1, pm, im);          // z + mu
+  M3 r = mul(mul_an(ldf(Unu, g, a, ai), ldf(G, g, a, ai)), ldf(Unu, g, b, bi));
+  accf(Gin, g, p, i, r, c);
+  r = mul_na(mul(ldf(Unu, g, p, i), ldf(G, g, pn, in_)), ldf(Unu, g, pm, im));
+  accf(Gin, g, p, i, r, c);
+}
+
+// adjoint of U_nu for out += c staple(in; mu, nu):
+// GU(z) += c [G(z) U(z+mu) in(z+nu)^+ + G(z-mu)^+ U(z-mu) in(z-mu+nu)
+//             + in(z-mu)^+ U(z-mu) G(z-mu+nu) + in(z) U(z+mu) G(z+nu)^+],  U = U_nu
+__global__ void k_adj_link(double2 *GU, const double2 *G, const double2 *in, const double2 *Unu, int mu, int nu,
+                           double c, Geom g) {
+  const i64 s = blockIdx.x * (i64)blockDim.x + threadIdx.x;
+  if (s >= 2 * g.Vh) return;
+  int p, i, z[4], pm, im, pn, in_, qm, iqm, qmn, iqmn, y[4];
+  site_of(g, s, p, i, z);
+  nbr_pi(g, z, mu, 1, pm, im);          // z + mu
+  nbr_pi(g, z, nu, 1, pn, in_);         // z + nu
+  shifted(g, z, mu, -1, y);
+  par_idx(g, y, qm, iqm);               // z - mu
+  nbr_pi(g, y, nu, 1, qmn, iqmn);       // z - mu + nu
+  const M3 Upm = ldf(Unu, g, pm, im), Uqm = ldf(Unu, g, qm, iqm);
+  M3 r = mul_na(mul(ldf(G, g, p, i), Upm), ldf(in, g, pn, in_));
+  accf(GU, g, p, i, r, c);
+  r = mul(mul_an(ldf(G, g, qm, iqm), Uqm), ldf(in, g, qmn, iqmn));
+  accf(GU, g, p, i, r, c);
+  r = mul(mul_an(ldf(in, g, qm, iqm), Uqm), ldf(G, g, qmn, iqmn));
+  accf(GU, g, p, i, r, c);
+  r = mul_na(mul(ldf(in, g, p, i), Upm), ldf(G, g, pn, in_));
+  accf(GU, g, p, i, r, c);
+}
+
+// adjoint of long(x) = c U(x) U(x+mu) U(x+2mu):
+// D(z) += c [N(z) (U(z+mu) U(z+2mu))^+ + U(z-mu)^+ N(z-mu) U(z+mu)^+ + (U(z-2mu) U(z-mu))^+ N(z-2mu)]
+__global__ void k_adj_naik(double2 *D, const double2 *N, const double2 *U, int mu, double c, Geom g) {
+  const i64 s = blockIdx.x * (i64)blockDim.x + threadIdx.x;
+  if (s >= 2 * g.Vh) return;
+  int p, i, z[4], p1, i1, p2, i2, m1, j1, m2, j2;
+  site_of(g, s, p, i, z);
+  nbr_pi(g, z, mu, 1, p1, i1);
+  nbr_pi(g, z, mu, 2, p2, i2);
+  nbr_pi(g, z, mu, -1, m1, j1);
+  nbr_pi(g, z, mu, -2, m2, j2);
+  const M3 Up1 = ldf(U, g, p1, i1), Um1 = ldf(U, g, m1, j1);
+  M3 r = mul_na(ldf(N, g, p, i), mul(Up1, ldf(U, g, p2, i2)));
+  accf(D, g, p, i, r, c);
+  r = mul_na(mul_an(Um1, ldf(N, g, m1, j1)), Up1);
+  accf(D, g, p, i, r, c);
+  r = mul_an(mul(ldf(U, g, m2, j2), Um1), ldf(N, g, m2, j2));
+  accf(D, g, p, i, r, c);
+}
+
+__global__ void k_field_axpby(double2 *d, double a, const double2 *s, double b, i64 n) {   // d = a d + b s
+  const i64 k = blockIdx.x * (i64)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const double2 x = d[k], y = s[k];
+  d[k] = make_double2(a * x.x + b * y.x, a * x.y + b * y.y);
+}
+
+// midF_mu(x) = -s(x) sum_i eps_i x_i(x) x_i(x+mu)^+ (midN: x+3mu), s = -1 on odd sites;
+// vectors are [parity][colour][site]
+template <typename T>
+__global__ void k_force_mid(double2 *midF, double2 *midN, const c2<T> *const *xs, const double *eps, int nsrc,
+                            Geom g) {
+  const i64 s = blockIdx.x * (i64)blockDim.x + threadIdx.x;
+  if (s >= 2 * g.Vh) return;
+  int p, i, x[4];
+  site_of(g, s, p, i, x);
+  const double sgn = p ? 1.0 : -1.0;
+  const i64 Vh = g.Vh;
+  for (int mu = 0; mu < 4; mu++) {
+    for (int k = 0; k < 2; k++) {
+      double2 *out = k == 0 ? midF : midN;
+      if (!out) continue;
+      int q, j;
+      nbr_pi(g, x, mu, k == 0 ? 1 : 3, q, j);
+      M3 m;
+#pragma unroll
+      for (int e = 0; e < 9; e++) m.e[e] = make_double2(0, 0);
+      for (int n = 0; n < nsrc; n++) {
+        const c2<T> *v = xs[n];
+        const double w = sgn * eps[n];
+        double2 a[3], b[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+          const c2<T> va = v[((i64)p * 3 + c) * Vh + i], vb = v[((i64)q * 3 + c) * Vh + j];
+          a[c] = make_double2((double)va.x, (double)va.y);
+          b[c] = make_double2((double)vb.x, (double)vb.y);
+        }
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+#pragma unroll
+          for (int c = 0; c < 3; c++) {   // a_r conj(b_c)
+            m.e[3 * r + c].x += w * (a[r].x * b[c].x + a[r].y * b[c].y);
+            m.e[3 * r + c].y += w * (a[r].y * b[c].x - a[r].x * b[c].y);
+          }
+      }
+      st3(out + (i64)mu * 18 * Vh + (i64)p * 9 * Vh + i, Vh, m);
+    }
+  }
+}
+
+// F_mu(x) += -2 TA(U_mu(x) D_mu(x)^+), TA = traceless anti-Hermitian part
+template <typename T>
+__global__ void k_force_ta(c2<T> *F, const double2 *U, const double2 *D, Geom g) {
+  const i64 s = blockIdx.x * (i64)blockDim.x + threadIdx.x;
+  if (s >= 8 * g.Vh) return;           // [4 mu][2 parities][Vh]
+  const i64 Vh = g.Vh;
+  const i64 pm = s / Vh, i = s % Vh;   // pm = mu * 2 + parity
+  const i64 off = pm * 9 * Vh + i;
+  const M3 a = mul_na(ld3(U + off, Vh), ld3(D + off, Vh));
+  double tri = 0;   // Im tr(a - a^+) / 2 = Im tr a
+#pragma unroll
+  for (int k = 0; k < 3; k++) tri += a.e[4 * k].y;
+#pragma unroll
+  for (int r = 0; r < 3; r++)
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const double2 x = a.e[3 * r + c], y = a.e[3 * c + r];
+      double re = 0.5 * (x.x - y.x), im = 0.5 * (x.y + y.y);
+      if (r == c) im -= tri / 3.0;
+      c2<T> &f = F[off + (i64)(3 * r + c) * Vh];
+      f.x = (T)((double)f.x - 2.0 * re);
+      f.y = (T)((double)f.y - 2.0 * im);
+    }
+}
+
+}  // namespace
+
+template <typename T>
+void asqtad_force(QOP_info_t *info, GaugeT<T> *G, GaugeT<T> *F, const QOP_asqtad_coeffs_t *cf, const double *eps,
+                  VecT<T> *const *x, int nsrc) {
+  Context &c = ctx();
+  const Geom &g = c.g;
+  const double t0 = wtime();
+  const i64 Vh = g.Vh, F1 = 18 * Vh, F4 = 72 * Vh;
+  const int grid2 = grid_for(2 * Vh, 128);
+  bool own = false;
+  double2 *U = gauge_fp64(G, own);
+  const bool naik = cf->naik != 0;
+  double2 *mid = dalloc<double2>(naik ? 2 * F4 : F4), *D = dalloc<double2>(F4);
+  dzero(D, sizeof(double2) * F4);
+  double2 *S3 = dalloc<double2>(F1), *S5 = dalloc<double2>(F1), *G3 = dalloc<double2>(F1), *G5 = dalloc<double2>(F1);
+  // outer products
+  std::vector<const c2<T> *> hx(nsrc);
+  for (int n = 0; n < nsrc; n++) hx[n] = x[n]->d;
+  const c2<T> **dx = dalloc<const c2<T> *>(nsrc);
+  double *deps = dalloc<double>(nsrc);
+  QCHECK(cudaMemcpyAsync(dx, hx.data(), sizeof(void *) * nsrc, cudaMemcpyHostToDevice, c.s));
+  QCHECK(cudaMemcpyAsync(deps, eps, sizeof(double) * nsrc, cudaMemcpyHostToDevice, c.s));
+  k_force_mid<T><<<grid2, 128, 0, c.s>>>(mid, naik ? mid + F4 : nullptr, dx, deps, nsrc, g);
+  QLAUNCH();
+  // reverse sweep over the staple sums of make_imp_links
+  const double c1 = cf->one_link - 6 * cf->lepage, c3 = cf->three_staple, c5 = cf->five_staple,
+               c7 = cf->seven_staple, cL = cf->lepage;
+  const bool have5 = c5 != 0 || c7 != 0 || cL != 0, have3 = c3 != 0 || have5;
+  const int gridF = grid_for(F1, 256);
+  auto Uf = [&](int d) { return U + d * F1; };
+  auto Df = [&](int d) { return D + d * F1; };
+  int nk = 0;
+  for (int mu = 0; mu < 4; mu++) {
+    const double2 *M = mid + mu * F1;
+    k_field_axpby<<<gridF, 256, 0, c.s>>>(Df(mu), 1.0, M, c1, F1);
+    nk++;
+    if (!have3) continue;
+    for (int nu = 0; nu < 4; nu++) {
+      if (nu == mu) continue;
+      k_fstaple<<<grid2, 128, 0, c.s>>>(S3, Uf(mu), Uf(nu), mu, nu, g);
+      k_field_axpby<<<gridF, 256, 0, c.s>>>(G3, 0.0, M, c3, F1);
+      nk += 2;
+      if (cL != 0) {
+        k_adj_in<<<grid2, 128, 0, c.s>>>(G3, M, Uf(nu), mu, nu, cL, g);
+        k_adj_link<<<grid2, 128, 0, c.s>>>(Df(nu), M, S3, Uf(nu), mu, nu, cL, g);
+        nk += 2;
+      }
+      if (c5 != 0 || c7 != 0) {
+        for (int rho = 0; rho < 4; rho++) {
+          if (rho == mu || rho == nu) continue;
+          k_fstaple<<<grid2, 128, 0, c.s>>>(S5, S3, Uf(rho), mu, rho, g);
+          k_field_axpby<<<gridF, 256, 0, c.s>>>(G5, 0.0, M, c5, F1);
+          nk += 2;
+          if (c7 != 0)
+            for (int sig = 0; sig < 4; sig++) {
+              if (sig == mu || sig == nu || sig == rho) continue;
+              k_adj_in<<<grid2, 128, 0, c.s>>>(G5, M, Uf(sig), mu, sig, c7, g);
+              k_adj_link<<<grid2, 128, 0, c.s>>>(Df(sig), M, S5, Uf(sig), mu, sig, c7, g);
+              nk += 2;
+            }
+          k_adj_in<<<grid2, 128, 0, c.s>>>(G3, G5, Uf(rho), mu, rho, 1.0, g);
+          k_adj_link<<<grid2, 128, 0, c.s>>>(Df(rho), G5, S3, Uf(rho), mu, rho, 1.0, g);
+          nk += 2;
+        }
+      }
+      k_adj_in<<<grid2, 128, 0, c.s>>>(Df(mu), G3, Uf(nu), mu, nu, 1.0, g);
+      k_adj_link<<<grid2, 128, 0, c.s>>>(Df(nu), G3, Uf(mu), Uf(nu), mu, nu, 1.0, g);
+      nk += 2;
+    }
+  }
+  if (naik)
+    for (int mu = 0; mu < 4; mu++) {
+      k_adj_naik<<<grid2, 128, 0, c.s>>>(Df(mu), mid + F4 + mu * F1, Uf(mu), mu, cf->naik, g);
+      nk++;
+    }
+  k_force_ta<T><<<grid_for(8 * Vh, 128), 128, 0, c.s>>>(F->d, U, D, g);
+  QLAUNCHN(nk + 1);
+  sync();
+  dfree(dx); dfree(deps); dfree(mid); dfree(D); dfree(S3); dfree(S5); dfree(G3); dfree(G5);
+  if (own) dfree(U);
+  if (info) {
+    info->final_sec = wtime() - t0;
+    // outer products, adjoint staples and projection (per site, all directions)
+    info->final_flop = (double)g.V * (4.0 * (naik ? 2 : 1) * 72 * nsrc + (double)nk / 4.0 * 4 * 216 + 4 * 264);
+    info->status = QOP_SUCCESS;
+  }
+}
+
+template void asqtad_force<float>(QOP_info_t *, GaugeT<float> *, GaugeT<float> *, const QOP_asqtad_coeffs_t *,
+                                  const double *, VecT<float> *const *, int);
+template void asqtad_force<double>(QOP_info_t *, GaugeT<double> *, GaugeT<double> *, const QOP_asqtad_coeffs_t *,
+                                   const double *, VecT<double> *const *, int);
+
+}  // namespace qopb

@@ -103,6 +103,8 @@ struct Options {
   int recon_long = 1;            // int16 long links as two rows + det phase when exact
   int batch_kernel = 7;          // batched int16 hop variant (batch.cu kBhop); 7 measured fastest
   int multi_shift = 0;           // int16 multi-mass: 1 = sloppy multi-shift CG before the batched refinement
+  // QOP_asqtad_force_set_opts (lib/asqtad_force.c:3-41)
+  int force_fnmat_src_min = 2, force_veclength = 4;
   // QOP_hisq_links_set_opts (lib/hisq_links.c:4-78)
   int want_deps = 0, want_aux = 1, reunit_allow_svd = 1, reunit_svd_only = 0;
   double reunit_svd_rel_error = 1e-8, reunit_svd_abs_error = 1e-8;

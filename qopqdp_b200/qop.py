@@ -134,7 +134,8 @@ def load_library(path=None):
     lib.QOPB_serve_submit.restype = C.c_longlong
     lib.QOPB_serve_wait.argtypes = [C.c_longlong, C.c_double, C.POINTER(QOPB_result_t)]
     lib.QOPB_serve_wait.restype = ip
-    for f in ("QOP_asqtad_invert_set_opts", "QOP_hisq_links_set_opts", "QOP_hisq_invert_set_opts"):
+    for f in ("QOP_asqtad_invert_set_opts", "QOP_hisq_links_set_opts", "QOP_hisq_invert_set_opts",
+              "QOP_asqtad_force_set_opts"):
         getattr(lib, f).argtypes = [C.POINTER(QOP_opt_t), ip]
         getattr(lib, f).restype = ip
     for pc, real in (("F3", C.c_float), ("D3", C.c_double)):
@@ -151,6 +152,10 @@ def load_library(path=None):
         sig("extract_V_to_raw", [rp, vp, ip])
         sig("destroy_V", [vp])
         sig("create_G_from_raw", [rpp, ip], vp)
+        sig("create_F_from_raw", [rpp, ip], vp)
+        sig("extract_F_to_raw", [rpp, vp, ip])
+        sig("destroy_F", [vp])
+        sig("asqtad_force_multi", [info, vp, vp, C.POINTER(QOP_asqtad_coeffs_t), rp, C.POINTER(vp), ip])
         sig("extract_G_to_raw", [rpp, vp, ip])
         sig("destroy_G", [vp])
         sig("rephase_G", [vp, C.POINTER(C.c_int), C.POINTER(QOP_bc_t), C.POINTER(QOP_staggered_sign_t)])
@@ -287,6 +292,31 @@ class Qop:
         ptrs = (C.POINTER(self.real) * 4)(*[o.ctypes.data_as(C.POINTER(self.real)) for o in outs])
         self.f("extract_G_to_raw")(ptrs, h, eo)
         return outs
+
+    def create_F(self, fields, eo=QOP_EVENODD):
+        keep, ptrs = self._arr4(fields)
+        h = self.f("create_F_from_raw")(ptrs, eo)
+        if not h:
+            raise RuntimeError("create_F_from_raw failed")
+        return h
+
+    def extract_F(self, h, V, eo=QOP_EVENODD):
+        outs = [np.zeros((V, 3, 3, 2), dtype=self.dtype) for _ in range(4)]
+        ptrs = (C.POINTER(self.real) * 4)(*[o.ctypes.data_as(C.POINTER(self.real)) for o in outs])
+        self.f("extract_F_to_raw")(ptrs, h, eo)
+        return outs
+
+    def destroy_F(self, h):
+        self.f("destroy_F")(h)
+
+    def asqtad_force(self, gauge, force, coeffs, eps, vecs, info=None):
+        """QOP_*_asqtad_force_multi: force += -2 TA(U deriv^+) for the sources vecs."""
+        info = info or QOP_info_t()
+        c = QOP_asqtad_coeffs_t(*coeffs)
+        e = (self.real * len(eps))(*eps)
+        v = (C.c_void_p * len(vecs))(*vecs)
+        self.f("asqtad_force_multi")(C.byref(info), gauge, force, C.byref(c), e, v, len(vecs))
+        return info
 
     def destroy_G(self, h):
         self.f("destroy_G")(h)

@@ -1,0 +1,78 @@
+"""Asqtad fermion force through the C ABI (QOP_*_asqtad_force_multi,
+lib/asqtad_force_p.c:16-64) against the oracle on identical inputs: the
+outer products of the sources, the derivative through the smeared links
+(one-link, 3-, 5-, 7-staple, Lepage and Naik terms) and the traceless
+anti-Hermitian projection, accumulated into an existing force field."""
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import gpu_lattice
+from helpers import gauge
+from qopqdp_b200 import lattice as LT
+from qopqdp_b200.qop import QOP_info_t
+
+pytestmark = pytest.mark.gpu
+
+L = (4, 4, 4, 8)
+V = int(np.prod(L))
+
+
+def _run(prec, coef, nsrc):
+    q = gpu_lattice(L, prec)
+    U = [np.asarray(u) for u in gauge(L, 0.3, 5)]
+    xs = [LT.gaussian_vector(L, 80 + i) for i in range(nsrc)]
+    eps = [0.7, -0.4, 0.25][:nsrc]
+    rng = np.random.default_rng(2)
+    f0 = [rng.standard_normal((V, 3, 3, 2)) * 0.1 for _ in range(4)]
+    ref = O.Lattice(L).asqtad_force(coef, U, eps, xs, force=f0)
+    dt = q.dtype
+    G = q.create_G([u.astype(dt) for u in U])
+    F = q.create_F([f.astype(dt) for f in f0])
+    hv = [q.create_V(x.astype(dt)) for x in xs]
+    info = q.asqtad_force(G, F, coef, eps, hv)
+    got = q.extract_F(F, V)
+    for h in hv:
+        q.destroy_V(h)
+    q.destroy_F(F)
+    q.destroy_G(G)
+    return info, got, ref, f0
+
+
+@pytest.mark.parametrize("coef", [(1.0, 0.1, 0.1, 0.1, 0.1, 0.1), (0.7, -0.23, 0.31, -0.17, 0.29, -0.13),
+                                  (1.0, 0.2, 0.0, 0.0, 0.0, 0.0)])
+@pytest.mark.parametrize("nsrc", [1, 3])
+def test_force_matches_oracle_d3(coef, nsrc):
+    info, got, ref, f0 = _run("D", coef, nsrc)
+    assert info.status == 0
+    scale = max(np.max(np.abs(r - f)) for r, f in zip(ref, f0))
+    for g_, r in zip(got, ref):
+        assert np.max(np.abs(g_ - r)) <= 1e-12 * scale
+
+
+def test_force_matches_oracle_f3():
+    info, got, ref, f0 = _run("F", (1.0, 0.1, 0.1, 0.1, 0.1, 0.1), 2)
+    assert info.status == 0
+    scale = max(np.max(np.abs(r - f)) for r, f in zip(ref, f0))
+    for g_, r in zip(got, ref):
+        assert np.max(np.abs(g_.astype(np.float64) - r)) <= 2e-5 * scale
+
+
+def test_force_errors_and_options():
+    q = gpu_lattice(L, "D")
+    U = [np.asarray(u) for u in gauge(L, 0.3, 5)]
+    G = q.create_G(U)
+    F = q.create_F([np.zeros((V, 3, 3, 2)) for _ in range(4)])
+    hv = q.create_V(LT.gaussian_vector(L, 90))
+    info = q.asqtad_force(G, None, (1, 0.1, 0.1, 0.1, 0.1, 0.1), [0.5], [hv])
+    assert info.status != 0                                   # NULL force handle
+    info = q.asqtad_force(G, F, (1, 0.1, 0.1, 0.1, 0.1, 0.1), [0.5], [None])
+    assert info.status != 0                                   # NULL source
+    from qopqdp_b200.qop import _c_opts
+    arr, _k = _c_opts({"fnmat_src_min": 1, "veclength": 8})
+    assert q.lib.QOP_asqtad_force_set_opts(arr, 2) == 0
+    arr, _k = _c_opts({"veclength": 0})
+    assert q.lib.QOP_asqtad_force_set_opts(arr, 1) != 0
+    q.destroy_V(hv)
+    q.destroy_F(F)
+    q.destroy_G(G)

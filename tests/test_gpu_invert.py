@@ -60,7 +60,9 @@ def test_invert_eo_source(prec, rsq, eo):
     ref, _ = fo.invert(float(q.real(m).value), src.astype(np.float64), oia, ora)
     assert rel_norm_err(half(got, L, eo), half(ref, L, eo)) <= (1e-8 if prec == "D" else 1e-4)
     if prec == "D":
-        assert abs(ra.final_iter - ora.final_iter) <= 2
+        # FP64 rounding differs between the device reductions and the oracle's
+        # OpenMP reductions (whose order depends on the host's thread count)
+        assert abs(ra.final_iter - ora.final_iter) <= 0.02 * ora.final_iter + 3
     q.destroy_V(hin)
     q.destroy_V(hout)
     q.destroy_L(fla)
@@ -135,7 +137,7 @@ def test_invert_multi_eo_several_sources_matches_oracle():
             true = eo_residual(fo, m, outs[s][j], srcs[s], L, 0)
             assert abs(true - g) <= 0.05 * g + 1e-24                 # reported = true residual
             assert (g <= rsq * 1.1 and o <= rsq * 1.1) or 0.2 <= g / o <= 5, (s, m, g, o)
-            assert abs(ras[s][j].final_iter - oras[s][j].final_iter) <= 0.02 * oras[s][j].final_iter + 2
+            assert abs(ras[s][j].final_iter - oras[s][j].final_iter) <= 0.02 * oras[s][j].final_iter + 3
     q.destroy_L(fla)
 
 
@@ -155,7 +157,7 @@ def test_invert_multi_evenodd_paths(masses):
     refs, _ = fo.invert_multi(masses, srcs, O.InvertArg(1e9, 2000, 1000, 5, 2), oras)
     for s, ms in enumerate(masses):
         for j, m in enumerate(ms):
-            assert abs(ras[s][j].final_iter - oras[s][j].final_iter) <= 2
+            assert abs(ras[s][j].final_iter - oras[s][j].final_iter) <= 0.02 * oras[s][j].final_iter + 3
             g, o = ras[s][j].final_rsq, oras[s][j].final_rsq
             assert abs(g - o) <= 0.1 * o + 1e-20, (s, m, g, o)
             assert rel_norm_err(half(outs[s][j], L, 0), half(refs[s][j], L, 0)) <= 1e-3
@@ -188,7 +190,7 @@ def test_relmin_and_edge_cases():
     q.invert(fla, 0.1, hout, hin, ia, ra)
     oia, ora = O.InvertArg(1e9, 2000, 1000, 5, 2), O.ResidArg(0.0, 0, 1e-14, 0, 0, 0)
     ref, _ = fo.invert(0.1, src, oia, ora)
-    assert ra.final_rel <= 1e-14 * 1.01 and abs(ra.final_iter - ora.final_iter) <= 2
+    assert ra.final_rel <= 1e-14 * 1.01 and abs(ra.final_iter - ora.final_iter) <= 0.02 * ora.final_iter + 3
     # zero source: zero solution, zero residual
     z = np.zeros_like(src)
     hz, hzo = q.create_V(z), q.create_V(src)
