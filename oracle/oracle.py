@@ -60,6 +60,9 @@ def lib():
         l.or_fla_create.argtypes = [vp, C.POINTER(DP), C.POINTER(DP)]
         l.or_asqtad_deriv.argtypes = [vp, DP, C.POINTER(DP), C.POINTER(DP), C.POINTER(DP), C.POINTER(DP)]
         l.or_asqtad_force.argtypes = [vp, DP, C.POINTER(DP), C.POINTER(DP), DP, C.POINTER(DP), C.c_int]
+        l.or_hisq_deriv.argtypes = [vp, DP, C.POINTER(DP), C.c_int, DP, C.POINTER(DP), C.POINTER(DP), C.POINTER(DP)]
+        l.or_hisq_force.argtypes = [vp, DP, C.POINTER(DP), C.c_int, DP, C.POINTER(DP), DP, C.POINTER(DP),
+                                    C.POINTER(C.c_int)]
         l.or_fla_create.restype = vp
         l.or_fla_destroy.argtypes = [vp]
         l.or_dslash.argtypes = [vp, C.c_double, DP, DP, C.c_int, C.c_int]
@@ -140,6 +143,26 @@ class Lattice:
         e = np.array(eps, dtype=np.float64)
         c = np.array(coeffs, dtype=np.float64)
         lib().or_asqtad_force(self.h, _p(c), _p4(gauge), _p4(force), _p(e), xp, len(xs))
+        return force
+
+    def hisq_deriv(self, hcoef, gauge, eps_naik, midF, midN):
+        """deriv = dE/dU for E = sum_k c_k Re sum tr[midF_k^+ fat_k(W) + midN_k^+ long_k(W)];
+        midF / midN: lists of n_naiks lists of 4 fields."""
+        gauge = [f64(a) for a in gauge]
+        nk = len(midF)
+        mf = [f64(a) for grp in midF for a in grp]
+        mn = [f64(a) for grp in midN for a in grp]
+        der = [np.zeros_like(gauge[0]) for _ in range(4)]
+        lib().or_hisq_deriv(self.h, _p(f64(hcoef)), _p4(gauge), nk, _p(f64(eps_naik)),
+                            (DP * len(mf))(*[_p(a) for a in mf]), (DP * len(mn))(*[_p(a) for a in mn]), _p4(der))
+        return der
+
+    def hisq_force(self, hcoef, gauge, eps_naik, res, xs, n_orders, force=None):
+        gauge = [f64(a) for a in gauge]
+        force = [np.zeros_like(gauge[0]) for _ in range(4)] if force is None else [f64(a).copy() for a in force]
+        xs = [f64(x) for x in xs]
+        lib().or_hisq_force(self.h, _p(f64(hcoef)), _p4(gauge), len(n_orders), _p(f64(eps_naik)), _p4(force),
+                            _p(f64(res)), (DP * len(xs))(*[_p(x) for x in xs]), (C.c_int * len(n_orders))(*n_orders))
         return force
 
     def hisq_links(self, hcoef, gauge, want_W=False):

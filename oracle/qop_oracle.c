@@ -1323,3 +1323,122 @@ void or_asqtad_force(const or_lat *g, const double coef[6], double *Ur[4], doubl
   for (int i = 0; i < 8; i++) free(mid[i]);
   for (int i = 0; i < 4; i++) free(der[i]);
 }
+
+/* ------------------------------------------------------------------ */
+/* HISQ fermion force: lib/hisq_force_p.c:50-80 (n_orders_naik groups),  */
+/* lib/hisq_force_fnmat2_p.c:7-162 (mid with scale +1, sign flip on odd  */
+/* sites, asqtad level on W with the difference terms weighted by        */
+/* eps_naik, reunitarisation, fat7 level on U, factor 2), :164-231       */
+/* (force += antiherm(U deriv^+)).  The reunitarisation adjoint is the   */
+/* derivative of the polar factor W = V f(Q), Q = V^+V, f(q) = q^-1/2:   */
+/*   GV = GW f + V (B + B^+),  B = Z [(Z^+ V^+ GW Z) o Gamma] Z^+,        */
+/*   Gamma_ij = (f(w_i) - f(w_j)) / (w_i - w_j)                           */
+/*            = -1 / (s_i s_j (s_i + s_j)),  s = sqrt(w)  (i = j: f'(w)).  */
+/* ------------------------------------------------------------------ */
+static void reunit_adj(const dc *V, const dc *GW, dc *GV) {
+  dc Q[9], Z[9], f[9], A[9], t[9], At[9], B[9], u[9];
+  double w[3], s[3];
+  m_mul_an(Q, V, V);
+  herm_eig3(Q, w, Z);
+  for (int i = 0; i < 3; i++) s[i] = sqrt(w[i]);
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) {
+      dc acc = 0;
+      for (int k = 0; k < 3; k++) acc += Z[3 * i + k] * (1.0 / s[k]) * conj(Z[3 * j + k]);
+      f[3 * i + j] = acc;
+    }
+  m_mul_an(A, V, GW);
+  m_mul_an(t, Z, A);
+  m_mul(At, t, Z);
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) At[3 * i + j] *= -1.0 / (s[i] * s[j] * (s[i] + s[j]));
+  m_mul(t, Z, At);
+  m_mul_na(B, t, Z);
+  m_mul(GV, GW, f);
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) t[3 * i + j] = B[3 * i + j] + conj(B[3 * j + i]);
+  m_mul(u, V, t);
+  for (int e = 0; e < 9; e++) GV[e] += u[e];
+}
+
+void or_hisq_deriv(const or_lat *g, const double h[17], double *U[4], int n_naiks, const double *eps_naik,
+                   double **midF, double **midN, double *deriv[4]) {
+  const size_t n = 18 * (size_t)g->V;
+  double *Vl[4], *Wl[4], *GW[4], *tmp[4], *GV[4];
+  for (int i = 0; i < 4; i++) {
+    Vl[i] = calloc(n, sizeof(double)); Wl[i] = calloc(n, sizeof(double));
+    GW[i] = calloc(n, sizeof(double)); tmp[i] = calloc(n, sizeof(double)); GV[i] = calloc(n, sizeof(double));
+  }
+  const double c7[6] = {h[0], h[1], h[2], h[3], h[13] != 0 ? h[4] : 0.0, 0.0};
+  or_make_imp_links(g, c7, U, U, Vl, NULL);
+  for (int i = 0; i < 4; i++)
+#pragma omp parallel for
+    for (long s = 0; s < g->V; s++) or_u3_un_analytic(Vl[i] + 18 * s, Wl[i] + 18 * s, h[14] != 0, h[15], h[16]);
+  const double ca[6] = {h[5], h[6], h[7], h[8], h[9], h[10]}, cd[6] = {h[11], 0, 0, 0, 0, h[12]};
+  for (int k = 0; k < n_naiks; k++) {
+    for (int i = 0; i < 4; i++) memset(tmp[i], 0, n * sizeof(double));
+    or_asqtad_deriv(g, k == 0 ? ca : cd, Wl, midF + 4 * k, midN + 4 * k, tmp);
+    const double c = k == 0 ? 1.0 : eps_naik[k];
+    for (int i = 0; i < 4; i++)
+      for (size_t e = 0; e < n; e++) GW[i][e] += c * tmp[i][e];
+  }
+  for (int i = 0; i < 4; i++)
+#pragma omp parallel for
+    for (long s = 0; s < g->V; s++)
+      reunit_adj((const dc *)Vl[i] + 9 * s, (const dc *)GW[i] + 9 * s, (dc *)GV[i] + 9 * s);
+  or_asqtad_deriv(g, c7, U, GV, NULL, deriv);
+  for (int i = 0; i < 4; i++) { free(Vl[i]); free(Wl[i]); free(GW[i]); free(tmp[i]); free(GV[i]); }
+}
+
+void or_hisq_force(const or_lat *g, const double h[17], double *Ur[4], int n_naiks, const double *eps_naik,
+                   double *forcer[4], const double *res, double *xr[], const int *n_orders_naik) {
+  const size_t n = 18 * (size_t)g->V;
+  double **mid = malloc(sizeof(double *) * 8 * n_naiks), *der[4];
+  for (int i = 0; i < 8 * n_naiks; i++) mid[i] = calloc(n, sizeof(double));
+  for (int i = 0; i < 4; i++) der[i] = calloc(n, sizeof(double));
+  int nterms = 0;
+  for (int k = 0; k < n_naiks; k++) nterms += n_orders_naik[k];
+  int shift = 0;
+  for (int k = 0; k < n_naiks; k++) {
+    const int first = k == 0 ? 0 : shift, count = k == 0 ? nterms : n_orders_naik[k];
+    for (int mu = 0; mu < 4; mu++) {
+      dc *MF = (dc *)mid[4 * k + mu], *MN = (dc *)mid[4 * n_naiks + 4 * k + mu];
+#pragma omp parallel for
+      for (long z = 0; z < g->V; z++) {
+        const int *xc = g->x + 4 * z;
+        const double sgn = ((xc[0] + xc[1] + xc[2] + xc[3]) & 1) ? -1.0 : 1.0;
+        long z1 = nbr(g, z, mu, 1), z3 = nbr(g, z, mu, 3);
+        for (int i = first; i < first + count; i++) {
+          const dc *x = (const dc *)xr[i];
+          for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++) {
+              MF[9 * z + 3 * a + b] += sgn * res[i] * x[3 * z + a] * conj(x[3 * z1 + b]);
+              MN[9 * z + 3 * a + b] += sgn * res[i] * x[3 * z + a] * conj(x[3 * z3 + b]);
+            }
+        }
+      }
+    }
+    shift += n_orders_naik[k];
+  }
+  or_hisq_deriv(g, h, Ur, n_naiks, eps_naik, mid, mid + 4 * n_naiks, der);
+  for (int mu = 0; mu < 4; mu++) {
+    const dc *Um = (const dc *)Ur[mu], *Dm = (const dc *)der[mu];
+    dc *F = (dc *)forcer[mu];
+#pragma omp parallel for
+    for (long z = 0; z < g->V; z++) {
+      dc a[9];
+      m_mul_na(a, Um + 9 * z, Dm + 9 * z);
+      dc tr = 0;
+      for (int k = 0; k < 3; k++) tr += a[4 * k] - conj(a[4 * k]);
+      for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) {
+          dc ta = 0.5 * (a[3 * i + j] - conj(a[3 * j + i]));
+          if (i == j) ta -= tr / 6.0;
+          F[9 * z + 3 * i + j] += 2.0 * ta;
+        }
+    }
+  }
+  for (int i = 0; i < 8 * n_naiks; i++) free(mid[i]);
+  free(mid);
+  for (int i = 0; i < 4; i++) free(der[i]);
+}

@@ -95,6 +95,18 @@ void or_asqtad_deriv(const or_lat *g, const double coef[6], double *U[4],
 void or_asqtad_force(const or_lat *g, const double coef[6], double *U[4],
                      double *force[4], const double *eps, double *x[], int nsrc);
 
+/* HISQ fermion force (lib/hisq_force_p.c:50-80, hisq_force_fnmat2_p.c:7-231).
+   W = reunit(V), V = fat7(U) (or_hisq_links).  deriv is the derivative of
+     E(U) = sum_k c_k Re sum tr[ MF_k^+ fat_k(W) + MN_k^+ long_k(W) ]
+   (k = 0: asqtad coefficients, c_0 = 1; k >= 1: difference coefficients,
+   c_k = eps_naik[k]); mids are n_naiks x 4 fields.  The force builds
+   MF_k = s(x) sum_i res_i x_i(x) x_i(x+mu)^+ over group k's sources (group 0:
+   all sources; s = +1 even, -1 odd) and adds TA(U_mu (2 deriv_mu)^+). */
+void or_hisq_deriv(const or_lat *g, const double hcoef[17], double *U[4], int n_naiks, const double *eps_naik,
+                   double **midF, double **midN, double *deriv[4]);
+void or_hisq_force(const or_lat *g, const double hcoef[17], double *U[4], int n_naiks, const double *eps_naik,
+                   double *force[4], const double *res, double *x[], const int *n_orders_naik);
+
 /* threads used by OpenMP regions (0 = leave default) */
 void or_set_threads(int n);
 int or_get_threads(void);

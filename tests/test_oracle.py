@@ -237,3 +237,82 @@ def test_asqtad_force_outer_products_and_projection():
         G = got - LT.to_complex(f0[mu])
         assert np.max(np.abs(G + np.conj(np.transpose(G, (0, 2, 1))))) <= 1e-12 * np.max(np.abs(G))
         assert np.max(np.abs(np.trace(G, axis1=1, axis2=2))) <= 1e-12 * np.max(np.abs(G))
+
+
+def _hisq_E(lat, hc, U, eps_naik, midF, midN):
+    _, _, W, _ = lat.hisq_links(hc, U, want_W=True)
+    ca = hc[5:11]
+    cd = (hc[11], 0, 0, 0, 0, hc[12])
+    e = 0.0
+    for k in range(len(midF)):
+        fat, lng = lat.make_imp_links(ca if k == 0 else cd, W, naik=True)
+        c = 1.0 if k == 0 else eps_naik[k]
+        for mu in range(4):
+            e += c * np.sum(np.conj(LT.to_complex(midF[k][mu])) * LT.to_complex(fat[mu])).real
+            e += c * np.sum(np.conj(LT.to_complex(midN[k][mu])) * LT.to_complex(lng[mu])).real
+    return e
+
+
+@pytest.mark.parametrize("fat7_lepage", [0, 1])
+def test_hisq_deriv_is_the_derivative_of_the_hisq_chain(fat7_lepage):
+    """HISQ deriv = dE/dU through asqtad(W) + eps_naik-weighted difference
+    terms, the U(3) projection W = V (V^+V)^-1/2 and fat7(U): central finite
+    differences of the oracle's own link chain agree to 1e-6."""
+    L = (4, 4, 4, 6)
+    V = int(np.prod(L))
+    lat = O.Lattice(L)
+    rng = np.random.default_rng(4)
+    hc = LT.hisq_coeff_vector(LT.hisq_bench_coeffs()).copy()
+    hc[11], hc[12] = 0.13, -0.21                  # difference one-link, Naik
+    hc[13], hc[4] = fat7_lepage, 0.07             # optional fat7 Lepage term
+    eps_naik = [0.0, 0.3]
+    U = [np.asarray(u) for u in gauge(L, 0.3, 5)]
+    midF = [[LT.from_complex(_cgauss(rng, (V, 3, 3))) for _ in range(4)] for _ in range(2)]
+    midN = [[LT.from_complex(_cgauss(rng, (V, 3, 3))) for _ in range(4)] for _ in range(2)]
+    der = lat.hisq_deriv(hc, U, eps_naik, midF, midN)
+    dU = [_cgauss(rng, (V, 3, 3)) for _ in range(4)]
+    h = 1e-5
+    Up = [LT.from_complex(LT.to_complex(U[m]) + h * dU[m]) for m in range(4)]
+    Um = [LT.from_complex(LT.to_complex(U[m]) - h * dU[m]) for m in range(4)]
+    fd = (_hisq_E(lat, hc, Up, eps_naik, midF, midN) - _hisq_E(lat, hc, Um, eps_naik, midF, midN)) / (2 * h)
+    an = sum(np.sum(np.conj(LT.to_complex(der[m])) * dU[m]).real for m in range(4))
+    assert abs(fd - an) <= 1e-6 * abs(an), (fd, an)
+
+
+def test_hisq_force_groups_and_projection():
+    """HISQ force = TA(U (2 deriv)^+) with mids from the sources of each Naik
+    group (group 0: all sources; lib/hisq_force_fnmat2_p.c:52-75), residues as
+    weights, scale +1 and the sign flip on odd sites."""
+    L = (4, 4, 4, 6)
+    V = int(np.prod(L))
+    lat = O.Lattice(L)
+    hc = LT.hisq_coeff_vector(LT.hisq_bench_coeffs()).copy()
+    hc[11], hc[12] = 0.13, -0.21
+    eps_naik = [0.0, 0.3]
+    n_orders = [2, 1]
+    U = [np.asarray(u) for u in gauge(L, 0.3, 5)]
+    xs = [LT.gaussian_vector(L, 90 + i) for i in range(3)]
+    res = [0.5, -0.25, 0.75]
+    F = lat.hisq_force(hc, U, eps_naik, res, xs, n_orders)
+    sgn = np.where(LT.parity_mask(L), 1.0, -1.0)
+    groups = [range(0, 3), range(2, 3)]
+    midF, midN = [], []
+    for grp in groups:
+        gf, gn = [], []
+        for mu in range(4):
+            mf = np.zeros((V, 3, 3), complex)
+            mn = np.zeros((V, 3, 3), complex)
+            for i in grp:
+                xc = LT.to_complex(xs[i])
+                mf += res[i] * np.einsum("va,vb->vab", xc, np.conj(xc[_shift(L, mu, 1)]))
+                mn += res[i] * np.einsum("va,vb->vab", xc, np.conj(xc[_shift(L, mu, 3)]))
+            gf.append(LT.from_complex(sgn[:, None, None] * mf))
+            gn.append(LT.from_complex(sgn[:, None, None] * mn))
+        midF.append(gf)
+        midN.append(gn)
+    der = lat.hisq_deriv(hc, U, eps_naik, midF, midN)
+    for mu in range(4):
+        A = LT.to_complex(U[mu]) @ np.conj(np.transpose(2 * LT.to_complex(der[mu]), (0, 2, 1)))
+        T = 0.5 * (A - np.conj(np.transpose(A, (0, 2, 1))))
+        T -= np.trace(T, axis1=1, axis2=2)[:, None, None] / 3 * np.eye(3)
+        assert np.max(np.abs(LT.to_complex(F[mu]) - T)) <= 1e-12 * np.max(np.abs(T))
