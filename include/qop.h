@@ -256,6 +256,9 @@ void QOP_##PC##_asqtad_force(QOP_info_t *info, QOP_##PC##_GaugeField *gauge,   \
 void QOP_##PC##_asqtad_force_multi(QOP_info_t *info, QOP_##PC##_GaugeField *gauge, \
     QOP_##PC##_Force *force, QOP_asqtad_coeffs_t *coef, REAL eps[],            \
     QOP_##PC##_ColorVector *in_pt[], int nsrc);                                \
+void QOP_##PC##_hisq_force_multi(QOP_info_t *info, QOP_##PC##_FermionLinksHisq *flh, \
+    QOP_##PC##_Force *force, QOP_hisq_coeffs_t *coef, REAL eps[],              \
+    QOP_##PC##_ColorVector *in_pt[], int *n_orders_naik);                      \
 /* HISQ links (qop_f3.h:473-483) */                                            \
 QOP_##PC##_FermionLinksHisq *QOP_##PC##_hisq_create_L_from_G(QOP_info_t *info, \
     QOP_hisq_coeffs_t *coeffs, QOP_##PC##_GaugeField *gauge);                  \
@@ -293,6 +296,7 @@ typedef QOP_D_Real QOP_Real;
 #define QOP_destroy_F                   QOPB_GEN(destroy_F)
 #define QOP_asqtad_force                QOPB_GEN(asqtad_force)
 #define QOP_asqtad_force_multi          QOPB_GEN(asqtad_force_multi)
+#define QOP_hisq_force_multi            QOPB_GEN(hisq_force_multi)
 #define QOP_extract_G_to_raw            QOPB_GEN(extract_G_to_raw)
 #define QOP_destroy_G                   QOPB_GEN(destroy_G)
 #define QOP_rephase_G                   QOPB_GEN(rephase_G)

@@ -349,6 +349,28 @@ void force_multi(QOP_info_t *info, GaugeT<T> *G, GaugeT<T> *F, QOP_asqtad_coeffs
   }
   asqtad_force<T>(info, G, F, coef, e.data(), in, nsrc);
 }
+template <typename T, typename R>
+void hisq_force_multi(QOP_info_t *info, HisqT<T> *h, GaugeT<T> *F, QOP_hisq_coeffs_t *coef, const R *eps,
+                      VecT<T> *const *in, const int *n_orders) {
+  require_init("hisq_force_multi");
+  need_handle<T>(h, "FermionLinksHisq");
+  need_handle<T>(F, "Force");
+  if (!coef || !eps || !in || !n_orders) fail(QOP_FAIL, "hisq_force_multi: NULL coefficients / eps / sources / orders");
+  if (coef->n_naiks < 1 || coef->n_naiks > QOP_MAX_NAIK || coef->n_naiks != h->n_naiks)
+    fail(QOP_FAIL, "hisq_force_multi: n_naiks %d does not match the links (%d)", coef->n_naiks, h->n_naiks);
+  int nterms = 0;
+  for (int k = 0; k < coef->n_naiks; k++) {
+    if (n_orders[k] < 0) fail(QOP_FAIL, "hisq_force_multi: negative n_orders_naik");
+    nterms += n_orders[k];
+  }
+  if (nterms < 1) fail(QOP_FAIL, "hisq_force_multi: no sources");
+  std::vector<double> e(nterms);
+  for (int i = 0; i < nterms; i++) {
+    need_handle<T>(in[i], "ColorVector");
+    e[i] = (double)eps[i];
+  }
+  hisq_force<T>(info, h, F, coef, e.data(), in, n_orders);
+}
 }  // namespace
 
 #define QOPB_DEFINE_FORCE(PC, T, REAL)                                                                            \
@@ -366,6 +388,13 @@ void force_multi(QOP_info_t *info, GaugeT<T> *G, GaugeT<T> *F, QOP_asqtad_coeffs
                                                 QOP_##PC##_ColorVector *in_pt[], int nsrc) {                      \
     TRY force_multi<T, REAL>(info, ig<T>(gauge), reinterpret_cast<GaugeT<T> *>(force), coef, eps,                  \
                              reinterpret_cast<VecT<T> *const *>(in_pt), nsrc);                                     \
+    CATCHV(info)                                                                                                    \
+  }                                                                                                                 \
+  extern "C" void QOP_##PC##_hisq_force_multi(QOP_info_t *info, QOP_##PC##_FermionLinksHisq *flh,                \
+                                              QOP_##PC##_Force *force, QOP_hisq_coeffs_t *coef, REAL eps[],       \
+                                              QOP_##PC##_ColorVector *in_pt[], int *n_orders_naik) {              \
+    TRY hisq_force_multi<T, REAL>(info, ih<T>(flh), reinterpret_cast<GaugeT<T> *>(force), coef, eps,             \
+                                  reinterpret_cast<VecT<T> *const *>(in_pt), n_orders_naik);                       \
     CATCHV(info)                                                                                                    \
   }                                                                                                                 \
   extern "C" void QOP_##PC##_asqtad_force(QOP_info_t *info, QOP_##PC##_GaugeField *gauge, QOP_##PC##_Force *force, \

@@ -32,5 +32,10 @@ void sloppy_invalidate(void *fla_any);   // drop reduced-precision copies (mixed
 template <typename T>
 void asqtad_force(QOP_info_t *info, GaugeT<T> *G, GaugeT<T> *F, const QOP_asqtad_coeffs_t *cf, const double *eps,
                   VecT<T> *const *x, int nsrc);
+// force.cu: HISQ force (F_mu += TA(U_mu (2 deriv_mu)^+)) from the handle's
+// auxiliary U, V, W fields; sources grouped by Naik epsilon (n_orders)
+template <typename T>
+void hisq_force(QOP_info_t *info, HisqT<T> *h, GaugeT<T> *F, const QOP_hisq_coeffs_t *cf, const double *res,
+                VecT<T> *const *x, const int *n_orders);
 
 }  // namespace qopb

@@ -130,16 +130,17 @@ __global__ void k_field_axpby(double2 *d, double a, const double2 *s, double b, 
   d[k] = make_double2(a * x.x + b * y.x, a * x.y + b * y.y);
 }
 
-// midF_mu(x) = -s(x) sum_i eps_i x_i(x) x_i(x+mu)^+ (midN: x+3mu), s = -1 on odd sites;
+// midF_mu(x) = sgn(x) sum_i eps_i x_i(x) x_i(x+mu)^+ (midN: x+3mu) with
+// sgn = even_sign on even and -even_sign on odd sites (asqtad: -1, HISQ: +1);
 // vectors are [parity][colour][site]
 template <typename T>
 __global__ void k_force_mid(double2 *midF, double2 *midN, const c2<T> *const *xs, const double *eps, int nsrc,
-                            Geom g) {
+                            double even_sign, Geom g) {
   const i64 s = blockIdx.x * (i64)blockDim.x + threadIdx.x;
   if (s >= 2 * g.Vh) return;
   int p, i, x[4];
   site_of(g, s, p, i, x);
-  const double sgn = p ? 1.0 : -1.0;
+  const double sgn = p ? -even_sign : even_sign;
   const i64 Vh = g.Vh;
   for (int mu = 0; mu < 4; mu++) {
     for (int k = 0; k < 2; k++) {
@@ -173,9 +174,9 @@ __global__ void k_force_mid(double2 *midF, double2 *midN, const c2<T> *const *xs
   }
 }
 
-// F_mu(x) += -2 TA(U_mu(x) D_mu(x)^+), TA = traceless anti-Hermitian part
+// F_mu(x) += fac TA(U_mu(x) D_mu(x)^+), TA = traceless anti-Hermitian part
 template <typename T>
-__global__ void k_force_ta(c2<T> *F, const double2 *U, const double2 *D, Geom g) {
+__global__ void k_force_ta(c2<T> *F, const double2 *U, const double2 *D, double fac, Geom g) {
   const i64 s = blockIdx.x * (i64)blockDim.x + threadIdx.x;
   if (s >= 8 * g.Vh) return;           // [4 mu][2 parities][Vh]
   const i64 Vh = g.Vh;
@@ -193,9 +194,140 @@ __global__ void k_force_ta(c2<T> *F, const double2 *U, const double2 *D, Geom g)
       double re = 0.5 * (x.x - y.x), im = 0.5 * (x.y + y.y);
       if (r == c) im -= tri / 3.0;
       c2<T> &f = F[off + (i64)(3 * r + c) * Vh];
-      f.x = (T)((double)f.x - 2.0 * re);
-      f.y = (T)((double)f.y - 2.0 * im);
+      f.x = (T)((double)f.x + fac * re);
+      f.y = (T)((double)f.y + fac * im);
     }
+}
+
+// adjoint of the U(3) projection W = V f(Q), Q = V^+V, f(q) = q^-1/2:
+// GV = GW f + V (B + B^+),  B = Z [(Z^+ V^+ GW Z) o Gamma] Z^+,
+// Gamma_ij = (f(w_i) - f(w_j)) / (w_i - w_j) = -1 / (s_i s_j (s_i + s_j)), s = sqrt(w)
+__global__ void k_reunit_adj(double2 *GV, const double2 *V, const double2 *GW, i64 n4) {
+  const i64 s = blockIdx.x * (i64)blockDim.x + threadIdx.x;   // over [4 mu][2 parities][Vh]
+  if (s >= n4) return;
+  const i64 Vh = n4 / 8, blk = s / Vh, i = s % Vh, off = blk * 9 * Vh + i;
+  const M3 v = ld3(V + off, Vh), gw = ld3(GW + off, Vh);
+  M3 Z;
+  double w[3], sq[3];
+  herm_eig3(mul_an(v, v), w, Z);
+#pragma unroll
+  for (int k = 0; k < 3; k++) sq[k] = sqrt(w[k]);
+  M3 f;
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+#pragma unroll
+    for (int b = 0; b < 3; b++) {
+      double2 acc = make_double2(0, 0);
+#pragma unroll
+      for (int k = 0; k < 3; k++) {   // Z_ak conj(Z_bk) / s_k
+        const double2 za = Z.e[3 * a + k], zb = Z.e[3 * b + k];
+        acc.x += (za.x * zb.x + za.y * zb.y) / sq[k];
+        acc.y += (za.y * zb.x - za.x * zb.y) / sq[k];
+      }
+      f.e[3 * a + b] = acc;
+    }
+  M3 At = mul(mul_an(Z, mul_an(v, gw)), Z);
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+#pragma unroll
+    for (int b = 0; b < 3; b++) {
+      const double gm = -1.0 / (sq[a] * sq[b] * (sq[a] + sq[b]));
+      At.e[3 * a + b] = make_double2(gm * At.e[3 * a + b].x, gm * At.e[3 * a + b].y);
+    }
+  const M3 B = mul_na(mul(Z, At), Z);
+  M3 t;
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+#pragma unroll
+    for (int b = 0; b < 3; b++)
+      t.e[3 * a + b] = make_double2(B.e[3 * a + b].x + B.e[3 * b + a].x, B.e[3 * a + b].y - B.e[3 * b + a].y);
+  M3 r = mul(gw, f);
+  const M3 u = mul(v, t);
+#pragma unroll
+  for (int e = 0; e < 9; e++) r.e[e] = make_double2(r.e[e].x + u.e[e].x, r.e[e].y + u.e[e].y);
+  st3(GV + off, Vh, r);
+}
+
+// Work fields of the reverse sweep ([2][9][Vh] each)
+struct SweepWork {
+  double2 *S3, *S5, *G3, *G5;
+};
+
+// D += derivative of Re sum tr[midF^+ fat + midN^+ long] with (fat, long) =
+// make_imp_links(c, U): the reverse sweep over its staple sums and the Naik
+// products; midN may be null.  Returns the number of kernels launched.
+int smear_adjoint(const double2 *U, const double c[6], const double2 *mid, const double2 *midN, double2 *D,
+                  const SweepWork &w) {
+  Context &cx = ctx();
+  const Geom &g = cx.g;
+  const i64 F1 = 18 * g.Vh;
+  const int grid2 = grid_for(2 * g.Vh, 128), gridF = grid_for(F1, 256);
+  const double c1 = c[0] - 6 * c[4], c3 = c[1], c5 = c[2], c7 = c[3], cL = c[4];
+  const bool have5 = c5 != 0 || c7 != 0 || cL != 0, have3 = c3 != 0 || have5;
+  auto Uf = [&](int d) { return U + d * F1; };
+  auto Df = [&](int d) { return D + d * F1; };
+  int nk = 0;
+  for (int mu = 0; mu < 4; mu++) {
+    const double2 *M = mid + mu * F1;
+    k_field_axpby<<<gridF, 256, 0, cx.s>>>(Df(mu), 1.0, M, c1, F1);
+    nk++;
+    if (!have3) continue;
+    for (int nu = 0; nu < 4; nu++) {
+      if (nu == mu) continue;
+      k_fstaple<<<grid2, 128, 0, cx.s>>>(w.S3, Uf(mu), Uf(nu), mu, nu, g);
+      k_field_axpby<<<gridF, 256, 0, cx.s>>>(w.G3, 0.0, M, c3, F1);
+      nk += 2;
+      if (cL != 0) {
+        k_adj_in<<<grid2, 128, 0, cx.s>>>(w.G3, M, Uf(nu), mu, nu, cL, g);
+        k_adj_link<<<grid2, 128, 0, cx.s>>>(Df(nu), M, w.S3, Uf(nu), mu, nu, cL, g);
+        nk += 2;
+      }
+      if (c5 != 0 || c7 != 0) {
+        for (int rho = 0; rho < 4; rho++) {
+          if (rho == mu || rho == nu) continue;
+          k_fstaple<<<grid2, 128, 0, cx.s>>>(w.S5, w.S3, Uf(rho), mu, rho, g);
+          k_field_axpby<<<gridF, 256, 0, cx.s>>>(w.G5, 0.0, M, c5, F1);
+          nk += 2;
+          if (c7 != 0)
+            for (int sig = 0; sig < 4; sig++) {
+              if (sig == mu || sig == nu || sig == rho) continue;
+              k_adj_in<<<grid2, 128, 0, cx.s>>>(w.G5, M, Uf(sig), mu, sig, c7, g);
+              k_adj_link<<<grid2, 128, 0, cx.s>>>(Df(sig), M, w.S5, Uf(sig), mu, sig, c7, g);
+              nk += 2;
+            }
+          k_adj_in<<<grid2, 128, 0, cx.s>>>(w.G3, w.G5, Uf(rho), mu, rho, 1.0, g);
+          k_adj_link<<<grid2, 128, 0, cx.s>>>(Df(rho), w.G5, w.S3, Uf(rho), mu, rho, 1.0, g);
+          nk += 2;
+        }
+      }
+      k_adj_in<<<grid2, 128, 0, cx.s>>>(Df(mu), w.G3, Uf(nu), mu, nu, 1.0, g);
+      k_adj_link<<<grid2, 128, 0, cx.s>>>(Df(nu), w.G3, Uf(mu), Uf(nu), mu, nu, 1.0, g);
+      nk += 2;
+    }
+  }
+  if (midN && c[5] != 0)
+    for (int mu = 0; mu < 4; mu++) {
+      k_adj_naik<<<grid2, 128, 0, cx.s>>>(Df(mu), midN + mu * F1, Uf(mu), mu, c[5], g);
+      nk++;
+    }
+  QLAUNCHN(nk);
+  return nk;
+}
+
+// outer products of sources [first, first + n) into mid (and midN)
+template <typename T>
+void force_mids(double2 *mid, double2 *midN, VecT<T> *const *x, const double *w, int n, double even_sign) {
+  Context &cx = ctx();
+  std::vector<const c2<T> *> hx(n);
+  for (int k = 0; k < n; k++) hx[k] = x[k]->d;
+  const c2<T> **dx = dalloc<const c2<T> *>(n);
+  double *dw = dalloc<double>(n);
+  QCHECK(cudaMemcpyAsync(dx, hx.data(), sizeof(void *) * n, cudaMemcpyHostToDevice, cx.s));
+  QCHECK(cudaMemcpyAsync(dw, w, sizeof(double) * n, cudaMemcpyHostToDevice, cx.s));
+  k_force_mid<T><<<grid_for(2 * cx.g.Vh, 128), 128, 0, cx.s>>>(mid, midN, dx, dw, n, even_sign, cx.g);
+  QLAUNCH();
+  dfree(dx);
+  dfree(dw);
 }
 
 }  // namespace
@@ -207,82 +339,78 @@ void asqtad_force(QOP_info_t *info, GaugeT<T> *G, GaugeT<T> *F, const QOP_asqtad
   const Geom &g = c.g;
   const double t0 = wtime();
   const i64 Vh = g.Vh, F1 = 18 * Vh, F4 = 72 * Vh;
-  const int grid2 = grid_for(2 * Vh, 128);
   bool own = false;
   double2 *U = gauge_fp64(G, own);
   const bool naik = cf->naik != 0;
   double2 *mid = dalloc<double2>(naik ? 2 * F4 : F4), *D = dalloc<double2>(F4);
   dzero(D, sizeof(double2) * F4);
-  double2 *S3 = dalloc<double2>(F1), *S5 = dalloc<double2>(F1), *G3 = dalloc<double2>(F1), *G5 = dalloc<double2>(F1);
-  // outer products
-  std::vector<const c2<T> *> hx(nsrc);
-  for (int n = 0; n < nsrc; n++) hx[n] = x[n]->d;
-  const c2<T> **dx = dalloc<const c2<T> *>(nsrc);
-  double *deps = dalloc<double>(nsrc);
-  QCHECK(cudaMemcpyAsync(dx, hx.data(), sizeof(void *) * nsrc, cudaMemcpyHostToDevice, c.s));
-  QCHECK(cudaMemcpyAsync(deps, eps, sizeof(double) * nsrc, cudaMemcpyHostToDevice, c.s));
-  k_force_mid<T><<<grid2, 128, 0, c.s>>>(mid, naik ? mid + F4 : nullptr, dx, deps, nsrc, g);
+  const SweepWork w{dalloc<double2>(F1), dalloc<double2>(F1), dalloc<double2>(F1), dalloc<double2>(F1)};
+  force_mids<T>(mid, naik ? mid + F4 : nullptr, x, eps, nsrc, -1.0);   // scale -1 (fnmat_p.c:497)
+  const double co[6] = {cf->one_link, cf->three_staple, cf->five_staple, cf->seven_staple, cf->lepage, cf->naik};
+  const int nk = smear_adjoint(U, co, mid, naik ? mid + F4 : nullptr, D, w);
+  k_force_ta<T><<<grid_for(8 * Vh, 128), 128, 0, c.s>>>(F->d, U, D, -2.0, g);
   QLAUNCH();
-  // reverse sweep over the staple sums of make_imp_links
-  const double c1 = cf->one_link - 6 * cf->lepage, c3 = cf->three_staple, c5 = cf->five_staple,
-               c7 = cf->seven_staple, cL = cf->lepage;
-  const bool have5 = c5 != 0 || c7 != 0 || cL != 0, have3 = c3 != 0 || have5;
-  const int gridF = grid_for(F1, 256);
-  auto Uf = [&](int d) { return U + d * F1; };
-  auto Df = [&](int d) { return D + d * F1; };
-  int nk = 0;
-  for (int mu = 0; mu < 4; mu++) {
-    const double2 *M = mid + mu * F1;
-    k_field_axpby<<<gridF, 256, 0, c.s>>>(Df(mu), 1.0, M, c1, F1);
-    nk++;
-    if (!have3) continue;
-    for (int nu = 0; nu < 4; nu++) {
-      if (nu == mu) continue;
-      k_fstaple<<<grid2, 128, 0, c.s>>>(S3, Uf(mu), Uf(nu), mu, nu, g);
-      k_field_axpby<<<gridF, 256, 0, c.s>>>(G3, 0.0, M, c3, F1);
-      nk += 2;
-      if (cL != 0) {
-        k_adj_in<<<grid2, 128, 0, c.s>>>(G3, M, Uf(nu), mu, nu, cL, g);
-        k_adj_link<<<grid2, 128, 0, c.s>>>(Df(nu), M, S3, Uf(nu), mu, nu, cL, g);
-        nk += 2;
-      }
-      if (c5 != 0 || c7 != 0) {
-        for (int rho = 0; rho < 4; rho++) {
-          if (rho == mu || rho == nu) continue;
-          k_fstaple<<<grid2, 128, 0, c.s>>>(S5, S3, Uf(rho), mu, rho, g);
-          k_field_axpby<<<gridF, 256, 0, c.s>>>(G5, 0.0, M, c5, F1);
-          nk += 2;
-          if (c7 != 0)
-            for (int sig = 0; sig < 4; sig++) {
-              if (sig == mu || sig == nu || sig == rho) continue;
-              k_adj_in<<<grid2, 128, 0, c.s>>>(G5, M, Uf(sig), mu, sig, c7, g);
-              k_adj_link<<<grid2, 128, 0, c.s>>>(Df(sig), M, S5, Uf(sig), mu, sig, c7, g);
-              nk += 2;
-            }
-          k_adj_in<<<grid2, 128, 0, c.s>>>(G3, G5, Uf(rho), mu, rho, 1.0, g);
-          k_adj_link<<<grid2, 128, 0, c.s>>>(Df(rho), G5, S3, Uf(rho), mu, rho, 1.0, g);
-          nk += 2;
-        }
-      }
-      k_adj_in<<<grid2, 128, 0, c.s>>>(Df(mu), G3, Uf(nu), mu, nu, 1.0, g);
-      k_adj_link<<<grid2, 128, 0, c.s>>>(Df(nu), G3, Uf(mu), Uf(nu), mu, nu, 1.0, g);
-      nk += 2;
-    }
-  }
-  if (naik)
-    for (int mu = 0; mu < 4; mu++) {
-      k_adj_naik<<<grid2, 128, 0, c.s>>>(Df(mu), mid + F4 + mu * F1, Uf(mu), mu, cf->naik, g);
-      nk++;
-    }
-  k_force_ta<T><<<grid_for(8 * Vh, 128), 128, 0, c.s>>>(F->d, U, D, g);
-  QLAUNCHN(nk + 1);
   sync();
-  dfree(dx); dfree(deps); dfree(mid); dfree(D); dfree(S3); dfree(S5); dfree(G3); dfree(G5);
+  dfree(mid); dfree(D); dfree(w.S3); dfree(w.S5); dfree(w.G3); dfree(w.G5);
   if (own) dfree(U);
   if (info) {
     info->final_sec = wtime() - t0;
-    // outer products, adjoint staples and projection (per site, all directions)
-    info->final_flop = (double)g.V * (4.0 * (naik ? 2 : 1) * 72 * nsrc + (double)nk / 4.0 * 4 * 216 + 4 * 264);
+    // outer products, adjoint staples (~4 matrix products each) and projection
+    info->final_flop = (double)g.V * (4.0 * (naik ? 2 : 1) * 72 * nsrc + nk * 216.0 + 4 * 264);
+    info->status = QOP_SUCCESS;
+  }
+}
+
+template <typename T>
+void hisq_force(QOP_info_t *info, HisqT<T> *h, GaugeT<T> *F, const QOP_hisq_coeffs_t *cf, const double *res,
+                VecT<T> *const *x, const int *n_orders) {
+  Context &c = ctx();
+  const Geom &g = c.g;
+  const double t0 = wtime();
+  if (!h->U || !h->V || !h->W)
+    fail(QOP_FAIL, "hisq_force: the HISQ links carry no auxiliary U/V/W fields "
+                   "(create them with QOP_hisq_links_set_opts want_aux = 1)");
+  const i64 Vh = g.Vh, F1 = 18 * Vh, F4 = 72 * Vh;
+  bool oU = false, oV = false, oW = false;
+  double2 *U = gauge_fp64(h->U, oU), *V = gauge_fp64(h->V, oV), *W = gauge_fp64(h->W, oW);
+  double2 *mid = dalloc<double2>(2 * F4), *GW = dalloc<double2>(F4), *T1 = dalloc<double2>(F4);
+  double2 *D = dalloc<double2>(F4);
+  dzero(GW, sizeof(double2) * F4);
+  dzero(D, sizeof(double2) * F4);
+  const SweepWork w{dalloc<double2>(F1), dalloc<double2>(F1), dalloc<double2>(F1), dalloc<double2>(F1)};
+  int nterms = 0;
+  for (int k = 0; k < cf->n_naiks; k++) nterms += n_orders[k];
+  const double ca[6] = {cf->asqtad_one_link, cf->asqtad_three_staple, cf->asqtad_five_staple,
+                        cf->asqtad_seven_staple, cf->asqtad_lepage, cf->asqtad_naik};
+  const double cd[6] = {cf->difference_one_link, 0, 0, 0, 0, cf->difference_naik};
+  int nk = 0, shift = 0;
+  for (int k = 0; k < cf->n_naiks; k++) {
+    // group 0 takes every source with the asqtad coefficients, group k >= 1
+    // its own sources with the difference coefficients (fnmat2_p.c:52-113)
+    const int first = k == 0 ? 0 : shift, count = k == 0 ? nterms : n_orders[k];
+    shift += n_orders[k];
+    if (count == 0) continue;
+    force_mids<T>(mid, mid + F4, x + first, res + first, count, 1.0);
+    dzero(T1, sizeof(double2) * F4);
+    nk += smear_adjoint(W, k == 0 ? ca : cd, mid, mid + F4, T1, w);
+    k_field_axpby<<<grid_for(F4, 256), 256, 0, c.s>>>(GW, 1.0, T1, k == 0 ? 1.0 : cf->eps_naik[k], F4);
+    QLAUNCH();
+  }
+  k_reunit_adj<<<grid_for(8 * Vh, 128), 128, 0, c.s>>>(T1, V, GW, 8 * Vh);   // T1 = GV
+  QLAUNCH();
+  const double c7[6] = {cf->fat7_one_link, cf->fat7_three_staple, cf->fat7_five_staple, cf->fat7_seven_staple,
+                        c.opt.use_fat7_lepage ? cf->fat7_lepage : 0.0, 0.0};
+  nk += smear_adjoint(U, c7, T1, nullptr, D, w);
+  k_force_ta<T><<<grid_for(8 * Vh, 128), 128, 0, c.s>>>(F->d, U, D, 2.0, g);   // deriv = 2 D
+  QLAUNCH();
+  sync();
+  dfree(mid); dfree(GW); dfree(T1); dfree(D); dfree(w.S3); dfree(w.S5); dfree(w.G3); dfree(w.G5);
+  if (oU) dfree(U);
+  if (oV) dfree(V);
+  if (oW) dfree(W);
+  if (info) {
+    info->final_sec = wtime() - t0;
+    info->final_flop = (double)g.V * (8.0 * 72 * nterms + nk * 216.0 + 4 * 1500 + 4 * 264);
     info->status = QOP_SUCCESS;
   }
 }
@@ -291,5 +419,9 @@ template void asqtad_force<float>(QOP_info_t *, GaugeT<float> *, GaugeT<float> *
                                   const double *, VecT<float> *const *, int);
 template void asqtad_force<double>(QOP_info_t *, GaugeT<double> *, GaugeT<double> *, const QOP_asqtad_coeffs_t *,
                                    const double *, VecT<double> *const *, int);
+template void hisq_force<float>(QOP_info_t *, HisqT<float> *, GaugeT<float> *, const QOP_hisq_coeffs_t *,
+                                const double *, VecT<float> *const *, const int *);
+template void hisq_force<double>(QOP_info_t *, HisqT<double> *, GaugeT<double> *, const QOP_hisq_coeffs_t *,
+                                 const double *, VecT<double> *const *, const int *);
 
 }  // namespace qopb

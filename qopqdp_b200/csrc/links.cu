@@ -139,44 +139,6 @@ __device__ double2 det3(const M3 &u) {
   return cadd<double>(d, cmul<double>(u.e[2], m2));
 }
 
-// Hermitian Jacobi diagonalisation Q = Z diag(w) Z^+ (SVD stand-in)
-__device__ void herm_eig3(const M3 &Qin, double w[3], M3 &Z) {
-  M3 A = Qin;
-  for (int k = 0; k < 9; k++) Z.e[k] = make_double2(k % 4 == 0 ? 1.0 : 0.0, 0.0);
-  for (int sweep = 0; sweep < 60; sweep++) {
-    double off = 0;
-    for (int p = 0; p < 3; p++)
-      for (int q = p + 1; q < 3; q++) off += A.e[3 * p + q].x * A.e[3 * p + q].x + A.e[3 * p + q].y * A.e[3 * p + q].y;
-    if (off < 1e-34) break;
-    for (int p = 0; p < 3; p++)
-      for (int q = p + 1; q < 3; q++) {
-        double2 apq = A.e[3 * p + q];
-        double r = hypot(apq.x, apq.y);
-        if (r < 1e-300) continue;
-        double app = A.e[4 * p].x, aqq = A.e[4 * q].x;
-        double2 ph = make_double2(apq.x / r, apq.y / r);
-        double theta = 0.5 * atan2(2 * r, aqq - app);
-        double c = cos(theta), s = sin(theta);
-        double2 gpp = make_double2(c, 0), gpq = make_double2(s * ph.x, s * ph.y);
-        double2 gqp = make_double2(-s * ph.x, s * ph.y), gqq = make_double2(c, 0);
-        for (int k = 0; k < 3; k++) {
-          double2 akp = A.e[3 * k + p], akq = A.e[3 * k + q];
-          A.e[3 * k + p] = cadd<double>(cmul<double>(akp, gpp), cmul<double>(akq, gqp));
-          A.e[3 * k + q] = cadd<double>(cmul<double>(akp, gpq), cmul<double>(akq, gqq));
-          double2 zkp = Z.e[3 * k + p], zkq = Z.e[3 * k + q];
-          Z.e[3 * k + p] = cadd<double>(cmul<double>(zkp, gpp), cmul<double>(zkq, gqp));
-          Z.e[3 * k + q] = cadd<double>(cmul<double>(zkp, gpq), cmul<double>(zkq, gqq));
-        }
-        for (int k = 0; k < 3; k++) {
-          double2 apk = A.e[3 * p + k], aqk = A.e[3 * q + k];
-          A.e[3 * p + k] = cadd<double>(cconjmul<double>(gpp, apk), cconjmul<double>(gqp, aqk));
-          A.e[3 * q + k] = cadd<double>(cconjmul<double>(gpq, apk), cconjmul<double>(gqq, aqk));
-        }
-      }
-  }
-  for (int i = 0; i < 3; i++) w[i] = A.e[4 * i].x;
-}
-
 struct ReunitOpt { int allow_svd, svd_only; double rel, abs; };
 
 __device__ int u3_un_analytic(const M3 &V, M3 &W, const ReunitOpt o) {

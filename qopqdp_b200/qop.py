@@ -156,6 +156,7 @@ def load_library(path=None):
         sig("extract_F_to_raw", [rpp, vp, ip])
         sig("destroy_F", [vp])
         sig("asqtad_force_multi", [info, vp, vp, C.POINTER(QOP_asqtad_coeffs_t), rp, C.POINTER(vp), ip])
+        sig("hisq_force_multi", [info, vp, vp, C.POINTER(QOP_hisq_coeffs_t), rp, C.POINTER(vp), C.POINTER(ip)])
         sig("extract_G_to_raw", [rpp, vp, ip])
         sig("destroy_G", [vp])
         sig("rephase_G", [vp, C.POINTER(C.c_int), C.POINTER(QOP_bc_t), C.POINTER(QOP_staggered_sign_t)])
@@ -316,6 +317,15 @@ class Qop:
         e = (self.real * len(eps))(*eps)
         v = (C.c_void_p * len(vecs))(*vecs)
         self.f("asqtad_force_multi")(C.byref(info), gauge, force, C.byref(c), e, v, len(vecs))
+        return info
+
+    def hisq_force(self, hisq, force, hcoef, eps, vecs, n_orders, info=None):
+        """QOP_*_hisq_force_multi: force += TA(U (2 deriv)^+)."""
+        info = info or QOP_info_t()
+        e = (self.real * len(eps))(*eps)
+        v = (C.c_void_p * len(vecs))(*vecs)
+        no = (C.c_int * len(n_orders))(*n_orders)
+        self.f("hisq_force_multi")(C.byref(info), hisq, force, C.byref(hcoef), e, v, no)
         return info
 
     def destroy_G(self, h):

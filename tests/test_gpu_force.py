@@ -76,3 +76,45 @@ def test_force_errors_and_options():
     q.destroy_V(hv)
     q.destroy_F(F)
     q.destroy_G(G)
+
+
+@pytest.mark.parametrize("prec,tol", [("D", 1e-10), ("F", 5e-5)])
+def test_hisq_force_matches_oracle(prec, tol):
+    """QOP_*_hisq_force_multi (lib/hisq_force_p.c:50-80) with two Naik
+    epsilon groups: asqtad level on W, difference terms weighted by
+    eps_naik, the U(3) projection adjoint and the fat7 level, against the
+    oracle on the same gauge field and sources."""
+    q = gpu_lattice(L, prec)
+    hc = LT.hisq_bench_coeffs()
+    hc.n_naiks = 2
+    hc.eps_naik[1] = 0.3
+    hc.difference_one_link, hc.difference_naik = 0.13, -0.21
+    U = [np.asarray(u) for u in gauge(L, 0.3, 5)]
+    xs = [LT.gaussian_vector(L, 95 + i) for i in range(3)]
+    res, n_orders = [0.5, -0.25, 0.75], [2, 1]
+    rng = np.random.default_rng(6)
+    f0 = [rng.standard_normal((V, 3, 3, 2)) * 0.1 for _ in range(4)]
+    ref = O.Lattice(L).hisq_force(LT.hisq_coeff_vector(hc), U, [0.0, 0.3], res, xs, n_orders, force=f0)
+    dt = q.dtype
+    q.set_hisq_opts(want_aux=1)
+    G = q.create_G([u.astype(dt) for u in U])
+    H = q.hisq_create_L_from_G(hc, G)
+    F = q.create_F([f.astype(dt) for f in f0])
+    hv = [q.create_V(x.astype(dt)) for x in xs]
+    info = q.hisq_force(H, F, hc, res, hv, n_orders)
+    got = q.extract_F(F, V)
+    assert info.status == 0
+    scale = max(np.max(np.abs(r - f)) for r, f in zip(ref, f0))
+    for g_, r in zip(got, ref):
+        assert np.max(np.abs(g_.astype(np.float64) - r)) <= tol * scale
+    # without the auxiliary fields the force is refused
+    q.set_hisq_opts(want_aux=0)
+    H2 = q.hisq_create_L_from_G(hc, G)
+    assert q.hisq_force(H2, F, hc, res, hv, n_orders).status != 0
+    q.set_hisq_opts(want_aux=1)
+    for h in hv:
+        q.destroy_V(h)
+    q.hisq_destroy_L(H)
+    q.hisq_destroy_L(H2)
+    q.destroy_F(F)
+    q.destroy_G(G)
