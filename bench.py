@@ -23,6 +23,7 @@ by the batched int16 solver, compared with the same call in FP64):
   --workload multisrc    asqtad 32^4 (eps 0.4), 16 sources, mass 0.005
   --workload small       F3 asqtad 8^4: the nine Dslash cases and the eo CG,
                          GPU and oracle times, Dslash parity
+  --workload force       HISQ and asqtad fermion forces, 24^3x48, 8 sources
   --workload serve       the solve service (QOPB_serve_*) with HISQ 16^4,
                          24^3x48 and 32^3x64 resident, Poisson arrivals
 """
@@ -61,7 +62,7 @@ def parse():
     ap.add_argument("--cpu-iters", type=int, default=12, help="CG iterations timed on the host")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--quick", action="store_true", help="skip FP64 baseline and e2e (development)")
-    ap.add_argument("--workload", default="single", choices=["single", "multimass", "multisrc", "serve", "small"],
+    ap.add_argument("--workload", default="single", choices=["single", "multimass", "multisrc", "serve", "small", "force"],
                     help="single: the headline solve; multimass / multisrc: batched invert_multi workloads; "
                          "serve: the solve service under Poisson load")
     ap.add_argument("--serve-burst", type=int, default=12, help="requests of the peak-throughput burst")
@@ -673,6 +674,83 @@ def run_small(a):
     q.destroy_L(fla)
 
 
+def run_force(a):
+    """Fermion forces (QOP_D3_hisq_force_multi and QOP_D3_asqtad_force_multi)
+    on HISQ / asqtad links of a 24^3x48 gauge field (eps 0.5) with 8 sources
+    (one Naik group), FP64: device time per call (CUDA events, mean of
+    --steps after --warmup) and the oracle's time for the same call on a
+    12^4 lattice scaled by the volume ratio (the work is local per site)."""
+    import torch
+    torch.cuda.set_device(0)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from qopqdp_b200 import lattice as LT
+    from qopqdp_b200.qop import Qop, load_library
+    L = tuple(int(x) for x in a.lattice.split(",")) if a.lattice else (24, 24, 24, 48)
+    V = int(np.prod(L))
+    nsrc = 8
+    q = Qop("D")
+    assert q.init(L) == 0
+    lib = load_library()
+    lib.QOPB_stream.restype = __import__("ctypes").c_void_p
+    stream = torch.cuda.ExternalStream(lib.QOPB_stream())
+    U = LT.random_gauge(L, a.eps, a.seed, device="cuda")
+    G = q.create_G(U)
+    del U
+    q.rephase_G(G, LT.BENCH_R0, LT.BENCH_BC, LT.BENCH_SIGNMASK)
+    q.set_hisq_opts(want_aux=1)
+    hc = LT.hisq_bench_coeffs()
+    H = q.hisq_create_L_from_G(hc, G)
+    F = q.create_F([np.zeros((V, 3, 3, 2)) for _ in range(4)])
+    hv = [q.create_V(LT.gaussian_vector(L, a.seed + i)) for i in range(nsrc)]
+    res = [0.1 * (i + 1) for i in range(nsrc)]
+    acoef = LT.ASQTAD_BENCH_COEFFS
+
+    def ev():
+        e = torch.cuda.Event(enable_timing=True)
+        e.record(stream)
+        return e
+
+    out = {}
+    for name, call in (("hisq", lambda: q.hisq_force(H, F, hc, res, hv, [nsrc])),
+                       ("asqtad", lambda: q.asqtad_force(G, F, acoef, res, hv))):
+        for _ in range(a.warmup):
+            assert call().status == 0
+        e0 = ev()
+        for _ in range(a.steps):
+            call()
+        e1 = ev()
+        e1.synchronize()
+        out[name] = {"ms": e0.elapsed_time(e1) / a.steps}
+    # the oracle on a 12^4 lattice, scaled by volume
+    Lc = (12, 12, 12, 12)
+    Vc = int(np.prod(Lc))
+    lat = O.Lattice(Lc)
+    Uc = lat.rephase_G(LT.random_gauge(Lc, a.eps, a.seed, device="cpu"), LT.BENCH_R0, LT.BENCH_BC, LT.BENCH_SIGNMASK)
+    xs = [LT.gaussian_vector(Lc, a.seed + i) for i in range(nsrc)]
+    t0 = time.perf_counter()
+    lat.hisq_force(LT.hisq_coeff_vector(hc), Uc, [0.0], res, xs, [nsrc])
+    out["hisq"]["cpu_ms"] = (time.perf_counter() - t0) * 1e3 * V / Vc
+    t0 = time.perf_counter()
+    lat.asqtad_force(acoef, Uc, res, xs)
+    out["asqtad"]["cpu_ms"] = (time.perf_counter() - t0) * 1e3 * V / Vc
+    for k in out:
+        out[k]["speedup_vs_cpu"] = out[k]["cpu_ms"] / out[k]["ms"]
+    line = {"metric": "fermion force ms per call (8 sources, FP64)", "value": out["hisq"]["ms"], "unit": "ms",
+            "n_gpus": 1, "steps": a.steps, "warmup": a.warmup, "ms_per_step": out["hisq"]["ms"],
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "force", "lattice": L, "sources": nsrc, "eps": a.eps},
+            "forces": out,
+            "cpu_baseline": {"kind": "port", "cores": O.get_threads(),
+                             "sample": "one oracle force call on 12^4, scaled by the volume ratio"}}
+    print(json.dumps(line), flush=True)
+    for h in hv:
+        q.destroy_V(h)
+    q.destroy_F(F)
+    q.hisq_destroy_L(H)
+    q.destroy_G(G)
+
+
 SERVE_LATTICES = [(16, 16, 16, 16), (24, 24, 24, 48), (32, 32, 32, 64)]
 
 
@@ -806,6 +884,8 @@ def main():
         run_serve(a)
     elif a.workload == "small":
         run_small(a)
+    elif a.workload == "force":
+        run_force(a)
     elif a.workload != "single":
         run_multi(a)
     else:
