@@ -284,3 +284,27 @@ def test_every_batch_kernel_variant():
     for v, it in its.items():
         assert all(abs(a - b) <= 0.03 * b + 3 for a, b in zip(it, its[7])), its
     q.destroy_L(fla)
+
+
+@pytest.mark.parametrize("L", [(6, 6, 6, 6), (4, 6, 4, 10)])
+def test_mixed_ragged_site_blocks(L):
+    """Lattices whose sites per parity are not a multiple of the 128-site
+    link blocks (padded last block): single-system and batched int16 solves
+    both meet the FP64 target and agree with the oracle."""
+    V = int(np.prod(L))
+    q = gpu_lattice(L, "D")
+    fat, lng, _, _ = hisq_links(L, 0.5, 9)
+    fo = O.Fla(O.Lattice(L), fat, lng)
+    fla = q.create_L_from_raw(fat, lng)
+    srcs = [LT.gaussian_vector(L, 700 + s) for s in range(3)]
+    assert q.set_opts(prec_sloppy=16) == 0
+    st, _, got = _single_iters(q, fla, srcs[0], 0.05, L)
+    assert st == 0 and eo_residual(fo, 0.05, got, srcs[0], L, 0) <= 1.05e-20
+    info, ras, outs = _run_multi(q, fla, [[0.05], [0.1], [0.05]], srcs, 1e-20)
+    assert info.status == 0
+    for s, m in enumerate([0.05, 0.1, 0.05]):
+        assert eo_residual(fo, m, outs[s][0], srcs[s], L, 0) <= 1.05e-20
+        ref, _ = fo.invert(m, srcs[s], O.InvertArg(1e9, 20000, 20000, 5, 0), O.ResidArg(1e-20, 0, 0, 0, 0, 0))
+        assert rel_norm_err(half(outs[s][0], L, 0), half(ref, L, 0)) <= max(1e-6, 30 * 1e-10 / m ** 2)
+    assert q.set_opts(prec_sloppy=64) == 0
+    q.destroy_L(fla)
