@@ -50,6 +50,15 @@ unsigned long long QOPB_launch_count(void);
 double QOPB_D3_asqtad_ddagd_norm2_noalloc(QOP_info_t *info, QOP_D3_FermionLinksAsqtad *asqtad, double mass,
                                           QOP_D3_ColorVector *out, QOP_D3_ColorVector *in, QOP_evenodd_t eo);
 
+/* eigCG (QOP_asqtad_invert_set_opts tag "cg" = 1) keeps, in each link
+   handle, one space of approximate low eigenvectors of m^2 - D_pq D_qp per
+   solve parity p.  QOPB_*_eigcg_values copies up to `max` of the stored
+   eigenvalues for parity eo (QOP_EVEN or QOP_ODD; ascending, at the mass of
+   the last eigCG solve on that parity) into l and returns how many are
+   stored: 0 before the first eigCG solve, -1 on error. */
+int QOPB_F3_eigcg_values(QOP_F3_FermionLinksAsqtad *L, QOP_evenodd_t eo, double *l, int max);
+int QOPB_D3_eigcg_values(QOP_D3_FermionLinksAsqtad *L, QOP_evenodd_t eo, double *l, int max);
+
 /* Several lattices in one process (no counterpart in the reference, whose
    QOP_init fixes one geometry per process).  QOP_init defines lattice 0;
    QOPB_lattice_create adds a geometry (extents even and >= 4) and returns

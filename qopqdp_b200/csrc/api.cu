@@ -405,6 +405,19 @@ void hisq_force_multi(QOP_info_t *info, HisqT<T> *h, GaugeT<T> *F, QOP_hisq_coef
 QOPB_DEFINE_FORCE(F3, float, float)
 QOPB_DEFINE_FORCE(D3, double, double)
 
+// eigCG space introspection (no counterpart in the reference)
+#define QOPB_DEFINE_EIGCG(PC, T)                                                                                   \
+  extern "C" int QOPB_##PC##_eigcg_values(QOP_##PC##_FermionLinksAsqtad *L, QOP_evenodd_t eo, double *l, int max) { \
+    TRY require_init("eigcg_values");                                                                              \
+    need_handle<T>(L, "FermionLinksAsqtad");                                                                       \
+    if (eo != QOP_EVEN && eo != QOP_ODD) fail(QOP_FAIL, "eigcg_values: eo must be QOP_EVEN or QOP_ODD");           \
+    if (max > 0 && !l) fail(QOP_FAIL, "eigcg_values: NULL output");                                                \
+    return eigcg_values<T>(reinterpret_cast<FlaT<T> *>(L), eo, l, max);                                            \
+    CATCH(nullptr, -1)                                                                                             \
+  }
+QOPB_DEFINE_EIGCG(F3, float)
+QOPB_DEFINE_EIGCG(D3, double)
+
 // lib/asqtad_force.c:19-41: validated and kept; the device force has one
 // algorithm for every number of sources, so they select nothing here
 extern "C" QOP_status_t QOP_asqtad_force_set_opts(QOP_opt_t opts[], int nopts) {

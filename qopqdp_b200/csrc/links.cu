@@ -365,6 +365,7 @@ template <typename T>
 void fla_destroy(FlaT<T> *f) {
   if (!f) return;
   sloppy_invalidate((void *)f);
+  if (f->eigcg && f->eigcg_free) f->eigcg_free(f->eigcg);
   dfree(f->d);
   handle_forget(f);
   delete f;

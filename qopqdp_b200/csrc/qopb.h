@@ -164,6 +164,8 @@ template <typename T> struct FlaT {       // QOP_*_FermionLinksAsqtad
   c2<T> *d = nullptr;                     // [2][nlinks][9][Vh], x 1/2, double stored
   SloppyLinks *sl = nullptr;
   void *shadow32 = nullptr;               // FlaT<float>* copy used by mixed solves
+  void *eigcg = nullptr;                  // eigCG vector space (eigcg.cu), kept across solves
+  void (*eigcg_free)(void *) = nullptr;
 };
 template <typename T> struct HisqT {      // QOP_*_FermionLinksHisq
   int n_naiks = 1;

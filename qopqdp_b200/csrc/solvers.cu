@@ -479,7 +479,8 @@ void invert(QOP_info_t *info, FlaT<T> *f, QOP_invert_arg_t *ia, QOP_resid_arg_t 
   ia->max_restarts = 0;
   do {
     double t0 = wtime();
-    cg<T>(L, ia, ra, qout, qin, cgp, cgeo);
+    if (ctx().opt.cgtype == 1) eigcg<T>(L, ia, ra, qout, qin, cgp, cgeo, f);   // asqtad_invert_p.c:767-770
+    else cg<T>(L, ia, ra, qout, qin, cgp, cgeo);
     dtime += wtime() - t0;
     iter += ra->final_iter;
     B::copy(cgr, qout, cs);                                      // reconstruct (:92-100)

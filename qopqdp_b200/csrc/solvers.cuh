@@ -21,6 +21,15 @@ template <typename T>
 void cgms(LinOp<T> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t **ra, const double *shifts, int ns, c2<T> **out,
           const c2<T> *in, c2<T> *p, int eo);
 
+// eigCG (cgtype 1): CG that accumulates low eigenvectors of A in the link
+// handle and deflates the starting guess of later solves (eigcg.cu)
+template <typename T>
+void eigcg(LinOp<T> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t *ra, c2<T> *out, const c2<T> *in, c2<T> *p, int eo,
+           FlaT<T> *f);
+// eigenvalues of the space stored for parity eo (at the mass of the last
+// solve); copies up to max of them and returns how many are stored
+template <typename T> int eigcg_values(FlaT<T> *f, int eo, double *l, int max);
+
 template <typename T>
 void invert(QOP_info_t *info, FlaT<T> *f, QOP_invert_arg_t *ia, QOP_resid_arg_t *ra, double mass, c2<T> *out,
             const c2<T> *in);

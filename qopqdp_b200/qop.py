@@ -443,6 +443,17 @@ class Qop:
         self.f("asqtad_invert_multi")(C.byref(info), fla, C.byref(inv_arg), ra, mp, nm, op, ip_, nsrc)
         return info
 
+    def eigcg_values(self, fla, eo, max_values=1024):
+        """Stored eigCG eigenvalues for solve parity eo (ascending)."""
+        buf = (C.c_double * max_values)()
+        fn = getattr(self.lib, "QOPB_%s_eigcg_values" % self.pc)
+        fn.restype = C.c_int
+        fn.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double), C.c_int]
+        n = fn(fla, eo, buf, max_values)
+        if n < 0:
+            raise RuntimeError("QOPB_%s_eigcg_values failed" % self.pc)
+        return np.array(buf[:min(n, max_values)])
+
     # ------------------------------------------------------------ lattices and the solve service
     def lattice_create(self, L):
         return self.lib.QOPB_lattice_create((C.c_int * 4)(*L))
