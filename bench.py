@@ -26,6 +26,11 @@ by the batched int16 solver, compared with the same call in FP64):
   --workload force       HISQ and asqtad fermion forces, 24^3x48, 8 sources
   --workload serve       the solve service (QOPB_serve_*) with HISQ 16^4,
                          24^3x48 and 32^3x64 resident, Poisson arrivals
+  --workload dd          the decomposed lattice: FP64 CG (reference
+                         algorithm) on HISQ 32^3x64; one GPU: directions
+                         --dd-mask exchange halos with themselves through
+                         NCCL, timed against the undecomposed solve; N GPUs
+                         (torchrun): the lattice split over the GPUs
 """
 import argparse
 import json
@@ -62,7 +67,9 @@ def parse():
     ap.add_argument("--cpu-iters", type=int, default=12, help="CG iterations timed on the host")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--quick", action="store_true", help="skip FP64 baseline and e2e (development)")
-    ap.add_argument("--workload", default="single", choices=["single", "multimass", "multisrc", "serve", "small", "force"],
+    ap.add_argument("--dd-mask", type=int, default=15, help="dd workload on one GPU: self-split directions")
+    ap.add_argument("--workload", default="single",
+                    choices=["single", "multimass", "multisrc", "serve", "small", "force", "dd"],
                     help="single: the headline solve; multimass / multisrc: batched invert_multi workloads; "
                          "serve: the solve service under Poisson load")
     ap.add_argument("--serve-burst", type=int, default=12, help="requests of the peak-throughput burst")
@@ -751,6 +758,133 @@ def run_force(a):
     q.destroy_G(G)
 
 
+def run_dd(a):
+    """Decomposed lattice.  Links: HISQ smeared on each process's block
+    (periodic within the block: synthetic links of the production form),
+    made on the undecomposed block lattice and passed node-local to the
+    decomposed one.  One step = one FP64 CG solve (QOP_D3_asqtad_invert,
+    EVEN source, reference algorithm) to |r|/|b| <= --tol.  On one GPU the
+    directions of --dd-mask are decomposed with the process as its own
+    neighbour (every hop packs, exchanges through NCCL and reads halos) and
+    the same solve is timed on the undecomposed lattice; with N processes
+    the lattice is split as the reference's layout splits it.  Device time
+    on the library stream, max over ranks."""
+    import ctypes as C
+    import datetime
+    import torch
+    rank, local, world = rank_info()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    from qopqdp_b200 import lattice as LT
+    from qopqdp_b200.qop import Qop, QOP_invert_arg_t, QOP_resid_arg_t, QOP_EVEN, load_library, layout_hyper
+    lib = load_library()
+    lib.QOPB_stream.restype = C.c_void_p
+
+    class KStat(C.Structure):
+        _fields_ = [("name", C.c_char * 32), ("launches", C.c_int), ("total_ms", C.c_double),
+                    ("bytes_per_launch", C.c_double)]
+
+    lib.QOPB_prof_end.argtypes = [C.POINTER(KStat), C.c_int]
+    L = tuple(int(x) for x in (a.lattice or "32,32,32,64").split(","))
+    P = layout_hyper(L, world) if world > 1 else (1, 1, 1, 1)
+    B = tuple(L[i] // P[i] for i in range(4))
+    Vb = int(np.prod(B))
+    q = Qop("D")
+    # links of this block, smeared on the block lattice
+    assert q.init(B) == 0
+    U = LT.random_gauge(B, a.eps, a.seed + rank, device="cuda")
+    G = q.create_G(U)
+    del U
+    q.rephase_G(G, LT.BENCH_R0, LT.BENCH_BC, LT.BENCH_SIGNMASK)
+    q.set_hisq_opts(want_aux=0)
+    H = q.hisq_create_L_from_G(LT.hisq_bench_coeffs(), G)
+    q.destroy_G(G)
+    fat, lng = q.extract_L(q.hisq_asqtad_links(H, 0), Vb)
+    q.hisq_destroy_L(H)
+    q.finalize()
+    src = LT.gaussian_vector(B, a.seed + 100 + rank)
+    src[Vb // 2:] = 0
+    rsq = a.tol * a.tol
+
+    def measure(label):
+        stream = torch.cuda.ExternalStream(lib.QOPB_stream())
+        fla = q.create_L_from_raw(fat, lng)
+        hin, hout = q.create_V(src), q.create_V(np.zeros_like(src))
+        q.set_opts(prec_sloppy=64, cg=0)
+
+        def solve():
+            q.dslash(fla, 0.0, hout, hout, QOP_EVEN, QOP_EVEN)   # zero initial guess
+            ra = QOP_resid_arg_t(rsq, 0, 0, 0, 0, 0)
+            inf = q.invert(fla, a.mass, hout, hin, QOP_invert_arg_t(1e9, 200000, 200000, 10, QOP_EVEN), ra)
+            assert inf.status == 0
+            return ra
+
+        for _ in range(a.warmup):
+            solve()
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        lib.QOPB_prof_begin()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        its = [solve().final_iter for _ in range(a.steps)]
+        e1.record(stream)
+        e1.synchronize()
+        buf = (KStat * 32)()
+        n = lib.QOPB_prof_end(buf, 32)
+        kst = {buf[i].name.decode(): (buf[i].launches, buf[i].total_ms) for i in range(min(n, 32))}
+        ms = reduce_max(e0.elapsed_time(e1) / a.steps, dist, "cuda")
+        q.destroy_V(hin)
+        q.destroy_V(hout)
+        q.destroy_L(fla)
+        hop = {k: {"launches": v[0], "us_per_launch": 1e3 * v[1] / max(v[0], 1)} for k, v in kst.items()
+               if k.startswith("hop_f64")}
+        return {"label": label, "ms_per_solve": ms, "iters": int(np.median(its)), "hop": hop}
+
+    runs = []
+    if world == 1:
+        assert q.init(L) == 0
+        runs.append(measure("undecomposed"))
+        q.finalize()
+        uid = q.comm_unique_id()
+    else:
+        uid = q.comm_unique_id() if rank == 0 else None
+        obj = [uid]
+        dist.broadcast_object_list(obj, src=0)
+        uid = obj[0]
+    assert q.comm_init(uid, world, rank) == 0
+    if world == 1:
+        assert q.dd_self_split(a.dd_mask) == 0
+        assert q.init(L) == 0
+    else:
+        assert q.init(L, machsize=P) == 0
+    info = q.dd_info()
+    runs.append(measure("decomposed"))
+    q.finalize()
+    q.dd_self_split(0)
+    q.comm_finalize()
+    dd = runs[-1]
+    value = world * 1e3 / dd["ms_per_solve"] if world > 1 else 1e3 / dd["ms_per_solve"]
+    if rank == 0:
+        line = {"metric": "FP64 CG solves/s @%g, decomposed lattice" % a.tol, "value": value, "unit": "solves/s",
+                "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": dd["ms_per_solve"],
+                "higher_is_better": True, "scaling": "strong" if world > 1 else "weak", "vs_baseline": None,
+                "dtype": "f64", "data": "synthetic",
+                "config": {"workload": "dd", "lattice": L, "grid": P, "block": B, "mask": info["mask"],
+                           "mass": a.mass, "tol": a.tol, "eps": a.eps},
+                "runs": runs}
+        if world == 1:
+            line["overhead_vs_undecomposed"] = dd["ms_per_solve"] / runs[0]["ms_per_solve"]
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
 SERVE_LATTICES = [(16, 16, 16, 16), (24, 24, 24, 48), (32, 32, 32, 64)]
 
 
@@ -886,6 +1020,8 @@ def main():
         run_small(a)
     elif a.workload == "force":
         run_force(a)
+    elif a.workload == "dd":
+        run_dd(a)
     elif a.workload != "single":
         run_multi(a)
     else:

@@ -59,6 +59,38 @@ double QOPB_D3_asqtad_ddagd_norm2_noalloc(QOP_info_t *info, QOP_D3_FermionLinksA
 int QOPB_F3_eigcg_values(QOP_F3_FermionLinksAsqtad *L, QOP_evenodd_t eo, double *l, int max);
 int QOPB_D3_eigcg_values(QOP_D3_FermionLinksAsqtad *L, QOP_evenodd_t eo, double *l, int max);
 
+/* Decomposed lattice, one process per GPU (the reference does this through
+   QDP/QMP: lib/common.c:40-83, lib/layout_user.c:79-258).  Before QOP_init,
+   rank 0 makes an NCCL id with QOPB_comm_unique_id, the host sends it to the
+   other processes (e.g. through torch.distributed), and every process calls
+   QOPB_comm_init(id, nranks, rank) with its GPU current.  QOP_init then
+   splits the lattice as layout->machsize says (machdim 4), or, when machdim
+   is <= 0, as the reference's hypercubic layout does (QOPB_layout_hyper).
+   Every block must have even extents of at least 4.  Raw fields are
+   node-local: QOP_sites_on_node_raw_V sites in the order of
+   QOP_node_index_raw_V, and QOP_node_number_raw names the owning process.
+   Dslash, dslash_dir, ddagd(_norm2), diaginv, invert, invert_multi and eigCG
+   run on the decomposed lattice, with halos exchanged by NCCL on the library
+   stream and reductions summed by an NCCL all-reduce.  The solvers use the
+   reference algorithm there (prec_sloppy acts as 64).  Link smearing, HISQ
+   links, forces, the no-alloc entry point, extra lattices and the solve
+   service report QOP_FAIL (or -1).  QOPB_comm_finalize (after QOP_finalize)
+   frees the communicator.  QOPB_dd_self_split(mask), called before
+   QOP_init, marks directions as decomposed with this process as its own
+   neighbour (halos still packed and exchanged: a one-GPU test of the
+   decomposed path).  QOPB_dd_info returns this process's rank and fills the
+   grid, its block coordinates, the local extents and the decomposed
+   directions.  The QOPB_layout_* functions need no GPU and no QOP_init. */
+int QOPB_comm_unique_id(unsigned char id[128]);
+int QOPB_comm_init(const unsigned char id[128], int nranks, int rank);
+int QOPB_comm_finalize(void);
+int QOPB_dd_self_split(int mask);
+int QOPB_dd_info(int nsquares[4], int coords[4], int local[4], int *mask);
+int QOPB_layout_hyper(const int latsize[4], int nranks, int nsquares[4]);
+int QOPB_layout_node_number(const int latsize[4], const int nsquares[4], const int coords[4]);
+long QOPB_layout_node_index(const int latsize[4], const int nsquares[4], const int coords[4]);
+int QOPB_layout_neighbors(const int nsquares[4], int rank, int nbr[8]);
+
 /* Several lattices in one process (no counterpart in the reference, whose
    QOP_init fixes one geometry per process).  QOP_init defines lattice 0;
    QOPB_lattice_create adds a geometry (extents even and >= 4) and returns

@@ -339,6 +339,7 @@ template <typename T, typename R>
 void force_multi(QOP_info_t *info, GaugeT<T> *G, GaugeT<T> *F, QOP_asqtad_coeffs_t *coef, const R *eps,
                  VecT<T> *const *in, int nsrc) {
   require_init("asqtad_force");
+  dd_refuse("asqtad_force");
   need_handle<T>(G, "GaugeField");
   need_handle<T>(F, "Force");
   if (!coef || !eps || !in || nsrc < 1) fail(QOP_FAIL, "asqtad_force: NULL coefficients / eps / sources or nsrc < 1");
@@ -353,6 +354,7 @@ template <typename T, typename R>
 void hisq_force_multi(QOP_info_t *info, HisqT<T> *h, GaugeT<T> *F, QOP_hisq_coeffs_t *coef, const R *eps,
                       VecT<T> *const *in, const int *n_orders) {
   require_init("hisq_force_multi");
+  dd_refuse("hisq_force_multi");
   need_handle<T>(h, "FermionLinksHisq");
   need_handle<T>(F, "Force");
   if (!coef || !eps || !in || !n_orders) fail(QOP_FAIL, "hisq_force_multi: NULL coefficients / eps / sources / orders");

@@ -114,7 +114,7 @@ void handle_check(const void *h, const char *what) {
 }
 
 // extents even and >= 4 (eo preconditioning and the 3-hop Naik term), V < 2^31
-static bool make_geom(const int *ls, Geom &g) {
+static bool make_geom(const int *ls, Geom &g, bool global = false) {
   g = Geom{};
   g.V = 1;
   for (int i = 0; i < 4; i++) {
@@ -123,10 +123,12 @@ static bool make_geom(const int *ls, Geom &g) {
       return false;
     }
     g.L[i] = ls[i];
+    g.GL[i] = ls[i];
+    g.O[i] = 0;
     g.V *= ls[i];
   }
   g.Vh = g.V / 2;
-  if (g.V >= (1LL << 31)) {
+  if (!global && g.V >= (1LL << 31)) {
     fprintf(stderr, "QOP: volume too large for one device\n");
     return false;
   }
@@ -169,9 +171,17 @@ QOP_status_t QOP_init(QOP_layout_t *layout) {
     return QOP_FAIL;
   }
   Geom g{};
-  if (!make_geom(layout->latsize, g)) return QOP_FAIL;
+  if (!make_geom(layout->latsize, g, true)) return QOP_FAIL;
   OPT_TRY
   ensure_ready();
+  // a machine size (or a communicator of several processes) decomposes the
+  // lattice; g becomes this process's block
+  if (!dd_setup(layout, g)) return QOP_FAIL;
+  if (g.V >= (1LL << 31)) {
+    fprintf(stderr, "QOP: volume too large for one device\n");
+    dd_free();
+    return QOP_FAIL;
+  }
   ensure_partials(g);
   OPT_CATCH(QOP_FAIL)
   c.g = g;
@@ -185,7 +195,7 @@ QOP_status_t QOP_init(QOP_layout_t *layout) {
 
 int QOPB_lattice_create(const int latsize[4]) {
   Context &c = ctx();
-  if (!c.inited || !latsize) return -1;
+  if (!c.inited || !latsize || c.dd) return -1;
   Geom g{};
   if (!make_geom(latsize, g)) return -1;
   OPT_TRY
@@ -209,6 +219,7 @@ QOP_status_t QOP_finalize(void) {
   Context &c = ctx();
   if (!c.inited) return QOP_FAIL;
   if (c.s) cudaStreamSynchronize(c.s);
+  dd_free();
   c.inited = 0;
   return QOP_SUCCESS;
 }
@@ -231,8 +242,8 @@ int QOP_profcontrol(int level) {
   return old;
 }
 
-// single process: every site lives on node 0 (lib/common.c:134-139)
-int QOP_node_number_raw(int coords[]) { (void)coords; return 0; }
+// the process holding a site (lib/common.c:134-139); 0 unless decomposed
+int QOP_node_number_raw(int coords[]) { return ctx().inited ? dd_node_number(coords) : -1; }
 
 // raw index of a site: even sites first (lib/layout_user.c:237-258)
 static int raw_index(const int x[]) {
@@ -242,8 +253,10 @@ static int raw_index(const int x[]) {
   for (int i = 0; i < 4; i++) { l = l * g.L[i] + x[i]; s += x[i]; }
   return (int)((s & 1) ? (l + g.V) / 2 : l / 2);
 }
-int QOP_node_index_raw_V(int coords[], QOP_evenodd_t eo) { (void)eo; return ctx().inited ? raw_index(coords) : -1; }
-int QOP_node_index_raw_G(int coords[], QOP_evenodd_t eo) { (void)eo; return ctx().inited ? raw_index(coords) : -1; }
+// node-local raw index of a site given by global coordinates
+static int node_index(const int x[]) { return ctx().dd ? (int)dd_node_index(x) : raw_index(x); }
+int QOP_node_index_raw_V(int coords[], QOP_evenodd_t eo) { (void)eo; return ctx().inited ? node_index(coords) : -1; }
+int QOP_node_index_raw_G(int coords[], QOP_evenodd_t eo) { (void)eo; return ctx().inited ? node_index(coords) : -1; }
 int QOP_sites_on_node_raw_V(QOP_evenodd_t eo) { (void)eo; return (int)ctx().g.V; }
 int QOP_sites_on_node_raw_G(QOP_evenodd_t eo) { (void)eo; return (int)ctx().g.V; }
 

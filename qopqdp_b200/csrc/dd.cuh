@@ -1,0 +1,48 @@
+// dd.cuh -- halos of a decomposed lattice for the hop kernels (dd.cu).
+//
+// Each process holds a block of the global lattice with even local extents
+// at an even global origin, so a local site's parity is its global parity
+// and the node-local raw order is the single-lattice raw order of the block
+// (lib/layout_user.c:238-258 with even blocks).  A hop from an output site
+// x leaves the block along a decomposed direction mu when x_mu + d is < 0 or
+// >= L_mu; the term then comes from a halo received before the hop:
+//   up[mu]: the input vector at the sites x_mu = L_mu + j (j < depth) of the
+//           +mu neighbour, multiplied by the local forward link as usual;
+//   dn[mu]: -U_mu(y)^+ psi(y) at the sites y of the -mu neighbour, formed by
+//           the neighbour with its own forward links (slab 0: fat link at
+//           y_mu = -1; slab 1 + j: long link at y_mu = -1 - j), added as is.
+// So the backward links of the boundary sites never leave their owner and
+// no link halos exist.  Halo element (slab s, colour c, face site f) sits
+// at [(s * 3 + c) * fh + f], f = floor(lex'/2) with lex' the lexicographic
+// index of the three other coordinates (x0 slowest).  Every local extent is
+// even, so lex' and lex'+1 of one pair have opposite parities and f is a
+// bijection onto one parity's face sites.
+#pragma once
+#include "qopb.h"
+
+namespace qopb {
+
+template <typename T> struct DdGhost {
+  const c2<T> *up[4];
+  const c2<T> *dn[4];
+  int fh[4];    // sites of one parity in one face slab of direction mu
+  int mask;     // decomposed directions (bit mu)
+};
+
+// halo slabs: depth of the raw halo and number of product slabs
+__host__ __device__ inline int dd_depth(int nl) { return nl == 16 ? 3 : 1; }
+__host__ __device__ inline int dd_nprod(int nl) { return nl == 16 ? 4 : 1; }
+
+__device__ __forceinline__ int dd_face_index(const Geom &g, const int x[4], int mu) {
+  int l = 0;
+#pragma unroll
+  for (int nu = 0; nu < 4; nu++)
+    if (nu != mu) l = l * g.L[nu] + x[nu];
+  return l >> 1;
+}
+
+// packs the input halo of parity q (in: the parity-q block [colour][Vh]) and
+// exchanges it with the neighbours; returns the halos for the hop kernels
+template <typename T> DdGhost<T> dd_halo(FlaT<T> *f, const c2<T> *in, int q);
+
+}  // namespace qopb

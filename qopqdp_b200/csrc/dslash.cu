@@ -4,6 +4,7 @@
 // (mass term), :1106-1138 (ddagd, ddagd_norm2), :1166-1191 (dslash_dir).
 #include "reduce.cuh"
 #include "dslash.cuh"
+#include "dd.cuh"
 #include "prof.cuh"
 
 namespace qopb {
@@ -15,28 +16,52 @@ enum HopMode {
   HOP_M2_MINUS = 3  // out = mass*same - hop   (ddagd epilogue, mass = m^2)
 };
 
-// RED: 0 none, 1 = sum |out|^2, 2 = sum |same|^2
-template <typename T, int NL, int MODE, int RED>
+// neighbour (mu, d) of site x for a hop: the input vector, or on a
+// decomposed lattice the up halo when the hop leaves the block upwards.
+// Returns false when the term is a down-halo product, already added to a.
+template <typename T, bool DD>
+__device__ __forceinline__ bool hop_input(const Geom &g, const int x[4], int mu, int d, const c2<T> *src,
+                                          const DdGhost<T> &gh, c2<T> &v0, c2<T> &v1, c2<T> &v2, c2<T> *a) {
+  const i64 Vh = g.Vh;
+  if (DD && (gh.mask >> mu & 1) && (unsigned)(x[mu] + d) >= (unsigned)g.L[mu]) {
+    const int y = x[mu] + d, fh = gh.fh[mu], fi = dd_face_index(g, x, mu);
+    if (y < 0) {   // slab 0: the fat product at y = -1; slab -y: the long product
+      const c2<T> *G = gh.dn[mu] + (i64)((d == -1 ? 0 : -y) * 3) * fh + fi;
+      a[0] = cadd<T>(a[0], G[0]); a[1] = cadd<T>(a[1], G[fh]); a[2] = cadd<T>(a[2], G[2 * fh]);
+      return false;
+    }
+    const c2<T> *G = gh.up[mu] + (i64)((y - g.L[mu]) * 3) * fh + fi;
+    v0 = G[0]; v1 = G[fh]; v2 = G[2 * fh];
+    return true;
+  }
+  const int j = nbr_index(g, x, mu, d);
+  v0 = src[j]; v1 = src[Vh + j]; v2 = src[2 * Vh + j];
+  return true;
+}
+
+// RED: 0 none, 1 = sum |out|^2, 2 = sum |same|^2; DD: read halos (dd.cuh)
+template <typename T, int NL, int MODE, int RED, bool DD = false>
 __global__ void __launch_bounds__(128)
 k_hop(c2<T> *__restrict__ out, const c2<T> *__restrict__ src, const c2<T> *__restrict__ lk,
       const c2<T> *__restrict__ same, T mass, Geom g, int p,
-      double *part, unsigned *count, double *res) {
+      double *part, unsigned *count, double *res, DdGhost<T> gh = DdGhost<T>()) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const i64 Vh = g.Vh;
   double racc[1] = {0.0};
   if (i < Vh) {
     int x[4];
     site_coords(g, i, p, x);
-    c2<T> a0 = mk<T>(0, 0), a1 = a0, a2 = a0;
+    c2<T> a[3] = {mk<T>(0, 0), mk<T>(0, 0), mk<T>(0, 0)};
 #pragma unroll
     for (int k = 0; k < NL; k++) {
-      const int j = nbr_index(g, x, slot_mu<NL>(k), slot_disp<NL>(k));
-      const c2<T> v0 = src[j], v1 = src[Vh + j], v2 = src[2 * Vh + j];
+      c2<T> v0, v1, v2;
+      if (!hop_input<T, DD>(g, x, slot_mu<NL>(k), slot_disp<NL>(k), src, gh, v0, v1, v2, a)) continue;
       const c2<T> *U = lk + (i64)k * 9 * Vh + i;
-      cfma<T>(a0, U[0], v0); cfma<T>(a0, U[Vh], v1); cfma<T>(a0, U[2 * Vh], v2);
-      cfma<T>(a1, U[3 * Vh], v0); cfma<T>(a1, U[4 * Vh], v1); cfma<T>(a1, U[5 * Vh], v2);
-      cfma<T>(a2, U[6 * Vh], v0); cfma<T>(a2, U[7 * Vh], v1); cfma<T>(a2, U[8 * Vh], v2);
+      cfma<T>(a[0], U[0], v0); cfma<T>(a[0], U[Vh], v1); cfma<T>(a[0], U[2 * Vh], v2);
+      cfma<T>(a[1], U[3 * Vh], v0); cfma<T>(a[1], U[4 * Vh], v1); cfma<T>(a[1], U[5 * Vh], v2);
+      cfma<T>(a[2], U[6 * Vh], v0); cfma<T>(a[2], U[7 * Vh], v1); cfma<T>(a[2], U[8 * Vh], v2);
     }
+    const c2<T> a0 = a[0], a1 = a[1], a2 = a[2];
     c2<T> r0, r1, r2;
     if (MODE == HOP_SET) { r0 = a0; r1 = a1; r2 = a2; }
     else if (MODE == HOP_MASS_ALIAS) {
@@ -67,9 +92,9 @@ k_hop(c2<T> *__restrict__ out, const c2<T> *__restrict__ src, const c2<T> *__res
 }
 
 // one direction, weighted, accumulating (style-1 dslash_dir)
-template <typename T, int NL>
+template <typename T, int NL, bool DD = false>
 __global__ void k_hop_dir(c2<T> *__restrict__ out, const c2<T> *__restrict__ src, const c2<T> *__restrict__ lk,
-                          int k0, int nk, T w0, T w1, Geom g, int p) {
+                          int k0, int nk, T w0, T w1, Geom g, int p, DdGhost<T> gh = DdGhost<T>()) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const i64 Vh = g.Vh;
   if (i >= Vh) return;
@@ -79,8 +104,13 @@ __global__ void k_hop_dir(c2<T> *__restrict__ out, const c2<T> *__restrict__ src
   for (int kk = 0; kk < nk; kk++) {
     const int k = k0 + kk;
     const T w = kk == 0 ? w0 : w1;
-    const int j = nbr_index(g, x, slot_mu<NL>(k), slot_disp<NL>(k));
-    c2<T> v[3] = {cscale<T>(w, src[j]), cscale<T>(w, src[Vh + j]), cscale<T>(w, src[2 * Vh + j])};
+    c2<T> u0, u1, u2;
+    c2<T> h[3] = {mk<T>(0, 0), mk<T>(0, 0), mk<T>(0, 0)};
+    if (!hop_input<T, DD>(g, x, slot_mu<NL>(k), slot_disp<NL>(k), src, gh, u0, u1, u2, h)) {
+      for (int r = 0; r < 3; r++) a[r] = cadd<T>(a[r], cscale<T>(w, h[r]));   // w (-U^+ psi)
+      continue;
+    }
+    c2<T> v[3] = {cscale<T>(w, u0), cscale<T>(w, u1), cscale<T>(w, u2)};
     const c2<T> *U = lk + (i64)k * 9 * Vh + i;
     for (int r = 0; r < 3; r++)
       for (int c = 0; c < 3; c++) cfma<T>(a[r], U[(3 * r + c) * Vh], v[c]);
@@ -115,6 +145,18 @@ static void launch_hop(FlaT<T> *f, c2<T> *out, const c2<T> *in, const c2<T> *sam
   // plus the same-parity input of the fused mass / m^2 epilogues
   const double bytes = (double)g.Vh * sizeof(T) * 2 *
                        (f->nlinks * 9 + 3 + 3 + ((MODE == HOP_MASS || MODE == HOP_M2_MINUS) ? 3 : 0));
+  if (dd_active()) {
+    const DdGhost<T> gh = dd_halo<T>(f, src, 1 - p);
+    ProfScope ps(sizeof(T) == 8 ? "hop_f64_dd" : "hop_f32_dd", bytes);
+    if (f->nlinks == 16)
+      k_hop<T, 16, MODE, RED, true><<<grid, HOP_BLOCK, 0, c.s>>>(o, src, lk, sm, (T)mass, g, p, c.d_part, c.d_count,
+                                                                 res, gh);
+    else
+      k_hop<T, 8, MODE, RED, true><<<grid, HOP_BLOCK, 0, c.s>>>(o, src, lk, sm, (T)mass, g, p, c.d_part, c.d_count,
+                                                                res, gh);
+    QLAUNCH();
+    return;
+  }
   ProfScope ps(sizeof(T) == 8 ? "hop_f64" : "hop_f32", bytes);
   if (f->nlinks == 16)
     k_hop<T, 16, MODE, RED><<<grid, HOP_BLOCK, 0, c.s>>>(o, src, lk, sm, (T)mass, g, p, c.d_part, c.d_count, res);
@@ -201,6 +243,17 @@ void Dslash<T>::dslash_dir(FlaT<T> *f, int dir, int fb, double wtfat, double wtl
   for (int p = 0; p < 2; p++) {
     if (eo_out != QOP_EVENODD && eo_out != p) continue;
     int grid = grid_for(g.Vh, HOP_BLOCK);
+    if (dd_active()) {
+      const DdGhost<T> gh = dd_halo<T>(f, src + par_off(g, 1 - p), 1 - p);
+      if (f->nlinks == 16)
+        k_hop_dir<T, 16, true><<<grid, HOP_BLOCK, 0, c.s>>>(out + par_off(g, p), src + par_off(g, 1 - p),
+                                                            f->d + p * lk_par, k0, nk, (T)wtfat, (T)wtlong, g, p, gh);
+      else
+        k_hop_dir<T, 8, true><<<grid, HOP_BLOCK, 0, c.s>>>(out + par_off(g, p), src + par_off(g, 1 - p),
+                                                           f->d + p * lk_par, k0, nk, (T)wtfat, (T)wtlong, g, p, gh);
+      QLAUNCH();
+      continue;
+    }
     if (f->nlinks == 16)
       k_hop_dir<T, 16><<<grid, HOP_BLOCK, 0, c.s>>>(out + par_off(g, p), src + par_off(g, 1 - p), f->d + p * lk_par,
                                                      k0, nk, (T)wtfat, (T)wtlong, g, p);
@@ -224,6 +277,7 @@ double Dslash<T>::ddagd(FlaT<T> *f, double mass, c2<T> *out, const c2<T> *in, in
   }
   launch_hop<T, HOP_SET, 1>(f, tmp, in, nullptr, 0.0, q, c.d_res);
   launch_hop<T, HOP_M2_MINUS, 2>(f, out, tmp, in, (double)m2, p, c.d_res + 1);
+  dd_allreduce(c.d_res, 2);
   QCHECK(cudaMemcpyAsync(c.h_res, c.d_res, 2 * sizeof(double), cudaMemcpyDeviceToHost, c.s));
   QCHECK(cudaStreamSynchronize(c.s));
   // the reference returns |D in|^2 + m^2 |in|^2 in the working precision

@@ -321,7 +321,7 @@ void eigcg(LinOp<T> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t *ra, c2<T> *out, c
     total++;
     B::axpby(r, 1.0, in, -1.0, Mp, q);
     rsq = B::norm2(r, q);
-    if (ra->relmin > 0) relnorm = Blas<T>::relnorm_sum(r, out, eo) / (double)ctx().g.Vh;
+    if (ra->relmin > 0) relnorm = Blas<T>::relnorm_sum(r, out, eo) / (double)global_vh(ctx().g);
   };
   Window W(m, nev);
   c2<T> **v = nullptr;
@@ -407,7 +407,7 @@ void eigcg(LinOp<T> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t *ra, c2<T> *out, c
       }
       oldrsq = rsq;
       rsq = B::cg_update(out, r, a, p, Mp, q);
-      if (ra->relmin > 0) relnorm = Blas<T>::relnorm_sum(r, out, eo) / (double)ctx().g.Vh;
+      if (ra->relmin > 0) relnorm = Blas<T>::relnorm_sum(r, out, eo) / (double)global_vh(ctx().g);
       log0(QOP_VERB_HI, "eigCG: iter %d rsq = %g rel = %g\n", total, rsq, relnorm);
       if (done()) break;
       b = rsq / oldrsq;

@@ -78,9 +78,10 @@ __global__ void k_rephase_G(c2<T> *m, Geom g, int bc_dir, int org, double phr, d
   int p = (int)(s / g.Vh), i = (int)(s % g.Vh);
   int x[4];
   site_coords(g, i, p, x);
+  for (int j = 0; j < 4; j++) x[j] += g.O[j];   // global coordinates
   double fr = 1, fi = 0;
   if (bc_dir >= 0) {
-    int n = g.L[bc_dir];
+    int n = g.GL[bc_dir];
     int rshift = (x[bc_dir] + n - org) % n;
     if (rshift == n - 1) { fr = phr; fi = phi; }
   }

@@ -287,10 +287,11 @@ __global__ void k_rephase_L(c2<T> *lk, int nl, Geom g, int dir, int bc_dir, doub
   if (kind == 1 && nl != 16) return;
   int x[4];
   site_coords(g, i, p, x);
+  for (int j = 0; j < 4; j++) x[j] += g.O[j];   // global coordinates
   const int r0a[4] = {r0.x, r0.y, r0.z, r0.w};
   double fr = 1, fi = 0;
   if (bc_dir >= 0) {
-    int n = g.L[bc_dir];
+    int n = g.GL[bc_dir];
     int rshift = (x[bc_dir] + n - r0a[bc_dir]) % n;
     bool hit = kind == 0 ? (rshift == n - 1) : (rshift >= n - 3);
     if (hit) { fr = phr; fi = phi; }
@@ -298,7 +299,7 @@ __global__ void k_rephase_L(c2<T> *lk, int nl, Geom g, int dir, int bc_dir, doub
   if (bits) {
     int sgn = 0;
     for (int j = 0; j < 4; j++) {
-      int n = g.L[j];
+      int n = g.GL[j];
       sgn += ((bits >> j) & 1) * ((x[j] + n - r0a[j]) % n);
     }
     if (sgn & 1) { fr = -fr; fi = -fi; }
@@ -458,6 +459,7 @@ template double2 *gauge_fp64<double>(GaugeT<double> *, bool &);
 
 template <typename T>
 FlaT<T> *fla_from_G(QOP_info_t *info, const QOP_asqtad_coeffs_t *coef, GaugeT<T> *gfat, GaugeT<T> *glong) {
+  dd_refuse("asqtad_create_L_from_G");   // staples reach across the block faces
   const Geom &g = ctx().g;
   double t0 = wtime();
   bool o1, o2 = false;
@@ -478,6 +480,7 @@ FlaT<T> *fla_from_G(QOP_info_t *info, const QOP_asqtad_coeffs_t *coef, GaugeT<T>
 // hisq_links_p.c:62-256 with the reference's coefficient mapping
 template <typename T>
 HisqT<T> *hisq_from_G(QOP_info_t *info, const QOP_hisq_coeffs_t *c, GaugeT<T> *gauge) {
+  dd_refuse("hisq_create_L_from_G");
   const Geom &g = ctx().g;
   const Options &o = ctx().opt;
   double t0 = wtime(), flop = 0;

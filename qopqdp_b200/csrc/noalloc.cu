@@ -56,6 +56,7 @@ extern "C" double QOPB_D3_asqtad_ddagd_norm2_noalloc(QOP_info_t *info, QOP_D3_Fe
                                                      QOP_evenodd_t eo) {
   try {
     require_init("QOPB_D3_asqtad_ddagd_norm2_noalloc");
+    dd_refuse("QOPB_D3_asqtad_ddagd_norm2_noalloc");
     FlaT<double> *f = reinterpret_cast<FlaT<double> *>(asqtad);
     VecT<double> *o = reinterpret_cast<VecT<double> *>(out), *i = reinterpret_cast<VecT<double> *>(in);
     if (!f || !o || !i) fail(QOP_FAIL, "QOPB_D3_asqtad_ddagd_norm2_noalloc: NULL handle");

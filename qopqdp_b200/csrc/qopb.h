@@ -50,7 +50,13 @@ void count_launches(int n);
 struct Geom {
   int L[4];
   i64 V, Vh;
+  // a decomposed lattice: this process holds the block of extents L at
+  // global origin O (every O[mu] even) of the global lattice GL;
+  // otherwise O = 0 and GL = L
+  int O[4];
+  int GL[4];
 };
+inline i64 global_vh(const Geom &g) { return (i64)g.GL[0] * g.GL[1] * g.GL[2] * g.GL[3] / 2; }
 
 // ---------------------------------------------------------------- complex
 template <typename T> struct Cx;
@@ -130,6 +136,7 @@ struct Context {
   // `g` is the geometry of the current one (QOPB_lattice_use)
   std::vector<Geom> lats;
   int lat = 0;
+  struct Dd *dd = nullptr;   // domain decomposition of lattice 0 (dd.cu)
 };
 Context &ctx();
 void require_init(const char *fn);
@@ -143,6 +150,24 @@ void dzero(void *p, size_t bytes);
 void sync();
 
 int grid_for(i64 n, int block);
+
+// ---------------------------------------------------------------- decomposition (dd.cu)
+// true while lattice 0 is decomposed and current: hops exchange halos and
+// reductions are summed over processes
+bool dd_active();
+// sums n doubles of a device buffer over the processes (stream ordered)
+void dd_allreduce(double *d, int n);
+// QOP_init: decomposes the lattice when the layout or the communicator asks
+// for it (g becomes the local block); false when the layout is unusable
+bool dd_setup(const QOP_layout_t *layout, Geom &g);
+void dd_free();
+int dd_node_number(const int x[4]);
+long dd_node_index(const int x[4]);
+// entry points without a decomposed form refuse with QOP_FAIL
+void dd_refuse(const char *what);
+// the sloppy precision the solvers use (64 on a decomposed lattice: the
+// 16- and 32-bit sloppy kernels are single-domain)
+int sloppy_prec();
 
 // every handle remembers the lattice it was created on; entry points refuse
 // handles of another lattice (their device arrays have another size)

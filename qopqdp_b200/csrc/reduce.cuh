@@ -105,6 +105,7 @@ void run_reduce(const F &f, i64 n, double *out) {
   Context &c = ctx();
   k_reduce<N, F><<<red_grid(n), RED_THREADS, 0, c.s>>>(f, n, c.d_part, c.d_count, c.d_res);
   QLAUNCH();
+  dd_allreduce(c.d_res, N);
   QCHECK(cudaMemcpyAsync(c.h_res, c.d_res, sizeof(double) * N, cudaMemcpyDeviceToHost, c.s));
   QCHECK(cudaStreamSynchronize(c.s));
   for (int k = 0; k < N; k++) out[k] = c.h_res[k];

@@ -155,7 +155,7 @@ extern "C" {
 int QOPB_serve_start(void) {
   Service &S = g_srv;
   std::lock_guard<std::mutex> lk(S.mu);
-  if (S.running || !ctx().inited) return -1;
+  if (S.running || !ctx().inited || ctx().dd) return -1;
   try {
     ensure_ready();
   } catch (Fail &) {

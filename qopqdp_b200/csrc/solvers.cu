@@ -22,7 +22,7 @@ template <typename T> struct Tmp {   // scoped full-volume device vector
 
 template <typename T> static double relnorm2(const c2<T> *r, const c2<T> *x, int eo) {
   const Geom &g = ctx().g;
-  double n = eo == QOP_EVENODD ? (double)g.V : (double)g.Vh;
+  double n = eo == QOP_EVENODD ? 2.0 * global_vh(g) : (double)global_vh(g);
   return Blas<T>::relnorm_sum(r, x, eo) / n;
 }
 
@@ -274,7 +274,7 @@ template <typename T>
 static void inner_cgms(FlaT<T> *f, LinOp<T> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t **xra, const double *m2s, int nm,
                        c2<T> **x, c2<T> *rhs, c2<T> *cgp, int ineo, bool mixed) {
   const Geom &g = ctx().g;
-  const int prec = ctx().opt.sloppy_prec;
+  const int prec = sloppy_prec();
   if constexpr (std::is_same<T, double>::value) {
     if (prec < 64 && mixed_cgms(L, ia, xra, m2s, nm, x, rhs, ineo, prec)) return;
   }
@@ -310,7 +310,7 @@ void solve_multi(QOP_info_t *info, FlaT<T> *f, QOP_invert_arg_t *ia, QOP_resid_a
     return;
   }
   if constexpr (std::is_same<T, double>::value) {
-    if (ctx().opt.sloppy_prec < 64 && nsolve > 1) {
+    if (sloppy_prec() < 64 && nsolve > 1) {
       solve_multi_mixed(info, f, ia, ra, masses, out, in, nsolve);
       return;
     }

@@ -123,6 +123,14 @@ def load_library(path=None):
     lib.QOP_node_index_raw_V.restype = ip
     lib.QOP_sites_on_node_raw_V.argtypes = [ip]
     lib.QOP_sites_on_node_raw_V.restype = ip
+    lib.QOPB_comm_unique_id.argtypes = [C.POINTER(C.c_ubyte)]
+    lib.QOPB_comm_init.argtypes = [C.POINTER(C.c_ubyte), ip, ip]
+    lib.QOPB_dd_info.argtypes = [C.POINTER(C.c_int)] * 3 + [C.POINTER(C.c_int)]
+    lib.QOPB_layout_hyper.argtypes = [C.POINTER(C.c_int), ip, C.POINTER(C.c_int)]
+    lib.QOPB_layout_node_number.argtypes = [C.POINTER(C.c_int)] * 3
+    lib.QOPB_layout_node_index.argtypes = [C.POINTER(C.c_int)] * 3
+    lib.QOPB_layout_node_index.restype = C.c_long
+    lib.QOPB_layout_neighbors.argtypes = [C.POINTER(C.c_int), ip, C.POINTER(C.c_int)]
     lib.QOPB_lattice_create.argtypes = [C.POINTER(C.c_int)]
     lib.QOPB_lattice_create.restype = ip
     lib.QOPB_lattice_use.argtypes = [ip]
@@ -231,14 +239,42 @@ class Qop:
         return getattr(self.lib, "QOP_%s_%s" % (self.pc, name))
 
     # ------------------------------------------------------------ library
-    def init(self, L):
+    def init(self, L, machsize=None):
+        """QOP_init; machsize (4 ints) decomposes the lattice over the
+        processes of the communicator made by comm_init."""
         ls = (C.c_int * 4)(*L)
         lay = QOP_layout_t()
         lay.latdim = 4
         lay.latsize = ls
         lay.machdim = -1
+        if machsize is not None:
+            ms = (C.c_int * 4)(*machsize)
+            lay.machdim = 4
+            lay.machsize = ms
         st = self.lib.QOP_init(C.byref(lay))
         return st
+
+    # ------------------------------------------------------------ decomposition
+    def comm_unique_id(self):
+        buf = (C.c_ubyte * 128)()
+        if self.lib.QOPB_comm_unique_id(buf) != 0:
+            raise RuntimeError("QOPB_comm_unique_id failed")
+        return bytes(buf)
+
+    def comm_init(self, uid, nranks, rank):
+        buf = (C.c_ubyte * 128).from_buffer_copy(uid)
+        return self.lib.QOPB_comm_init(buf, nranks, rank)
+
+    def comm_finalize(self):
+        return self.lib.QOPB_comm_finalize()
+
+    def dd_self_split(self, mask):
+        return self.lib.QOPB_dd_self_split(mask)
+
+    def dd_info(self):
+        P, m, loc, mask = (C.c_int * 4)(), (C.c_int * 4)(), (C.c_int * 4)(), C.c_int()
+        r = self.lib.QOPB_dd_info(P, m, loc, C.byref(mask))
+        return dict(rank=r, nsquares=tuple(P), coords=tuple(m), local=tuple(loc), mask=mask.value)
 
     def finalize(self):
         return self.lib.QOP_finalize()
@@ -488,3 +524,27 @@ class Qop:
         if rc == 0:
             self._pending.pop(ticket, None)
         return rc, res
+
+
+# ---------------------------------------------------------------- layout (host only)
+def layout_hyper(L, nranks):
+    """The reference's split of lattice L over nranks processes."""
+    P = (C.c_int * 4)()
+    if load_library().QOPB_layout_hyper((C.c_int * 4)(*L), nranks, P) != 0:
+        raise ValueError("bad layout arguments")
+    return tuple(P)
+
+
+def layout_node_number(L, P, x):
+    return load_library().QOPB_layout_node_number((C.c_int * 4)(*L), (C.c_int * 4)(*P), (C.c_int * 4)(*x))
+
+
+def layout_node_index(L, P, x):
+    return load_library().QOPB_layout_node_index((C.c_int * 4)(*L), (C.c_int * 4)(*P), (C.c_int * 4)(*x))
+
+
+def layout_neighbors(P, rank):
+    """[(-mu rank, +mu rank) for mu in 0..3]."""
+    nb = (C.c_int * 8)()
+    load_library().QOPB_layout_neighbors((C.c_int * 4)(*P), rank, nb)
+    return [(nb[2 * i], nb[2 * i + 1]) for i in range(4)]
