@@ -659,7 +659,8 @@ k_mix_hop_q16a(uint4 *__restrict__ out, const uint4 *__restrict__ src, const uns
 
 // PERSIST: a grid of (SMs x MINB) blocks strides over the site blocks, so
 // no partial last wave of blocks leaves SMs idle
-template <int NL, int KIND, int BATCH, bool RECON, int MINB = 1, bool PERSIST = false>
+// PK: packed FP32x2 arithmetic (q16_slot_pk)
+template <int NL, int KIND, int BATCH, bool RECON, int MINB = 1, bool PERSIST = false, bool PK = false>
 __global__ void __launch_bounds__(QB, MINB)
 k_mix_hop_q16r(uint4 *__restrict__ out, const uint4 *__restrict__ src, const unsigned char *__restrict__ lk,
                const uint4 *__restrict__ same, Geom g, NbrGeom ng, int p, MixState *st, double *part,
@@ -678,6 +679,7 @@ k_mix_hop_q16r(uint4 *__restrict__ out, const uint4 *__restrict__ src, const uns
     site_coords(g, i, p, x);
     const int lex = ((x[0] * g.L[1] + x[1]) * g.L[2] + x[2]) * g.L[3] + x[3];
     float2 a[3] = {make_float2(0, 0), make_float2(0, 0), make_float2(0, 0)};
+    float2 pt[3] = {make_float2(0, 0), make_float2(0, 0), make_float2(0, 0)}, ps[3] = {pt[0], pt[1], pt[2]};
 #pragma unroll
     for (int k0 = 0; k0 < NL; k0 += BATCH) {
       uint4 ua[BATCH], ub[BATCH], nb[BATCH];
@@ -699,12 +701,19 @@ k_mix_hop_q16r(uint4 *__restrict__ out, const uint4 *__restrict__ src, const uns
       }
 #pragma unroll
       for (int s = 0; s < BATCH; s++) {
-        if (RECON && ((k0 + s) & 1))
+        if (PK) {
+          if (RECON && ((k0 + s) & 1))
+            q16_slot_recon_pk(ua[s], make_uint2(ub[s].x, ub[s].y), __uint_as_float(uc[s].x), nb[s], c_long, pt, ps);
+          else
+            q16_slot_pk(ua[s], ub[s], uc[s], nb[s], pt, ps);
+        } else if (RECON && ((k0 + s) & 1)) {
           q16_slot_recon(ua[s], make_uint2(ub[s].x, ub[s].y), __uint_as_float(uc[s].x), nb[s], c_long, a);
-        else
+        } else {
           q16_slot(ua[s], ub[s], uc[s], nb[s], a);
+        }
       }
     }
+    if (PK) q16_pk_rows(pt, ps, a);
     acc1[0] += q16_epilogue<KIND>(out, same, i, Vh, (float)st->m2, a);
   }
   } while (PERSIST && (sb += gridDim.x) < nsb);
@@ -806,6 +815,12 @@ LinksSloppy links_parity(SloppyLinks *s, int lkfmt, int p) {
 // 17-19 = persistent with a per-thread cp.async ring 3 / 2 / 4 slots ahead
 // (6 / 8 / 5 blocks per SM): 157-170 us, the 4-5 small asynchronous copies
 // per slot and thread cost more issue slots than the latency they hide.
+// 20-26 = persistent with packed FP32x2 arithmetic (q16_slot_pk): 2 slots
+// and 6 / 7 / 8 blocks per SM, 4 slots and 6 / 7 / 5, 8 slots and 6.  At
+// 32^3x64: 109.1-109.4 us with 25 (4 slots, 5 blocks, 96 registers; the
+// default), 110.0 with 23, 111.2 with 20 / 21, 112-113 with 22, 24, 26,
+// against 117.3 for the scalar variant 15 (a third fewer instructions per
+// slot; the kernel was issue-bound at 62 % issue-active).
 template <int KIND>
 static void launch_q16(int variant, int nl, bool recon, float c_long, int grid, uint4 *out, const uint4 *src,
                        const unsigned char *lk, const uint4 *same, const Geom &g, const NbrGeom &ng, int par,
@@ -830,6 +845,13 @@ static void launch_q16(int variant, int nl, bool recon, float c_long, int grid, 
     else if (recon) k_mix_hop_q16r<16, KIND, B, true, M, true><<<gp, QB, 0, c.s>>>(Q16_ARGS, c_long);    \
     else k_mix_hop_q16r<16, KIND, B, false, M, true><<<gp, QB, 0, c.s>>>(Q16_ARGS, c_long);              \
   } while (0)
+#define Q16RPK(B, M)                                                                                           \
+  do {                                                                                                         \
+    const int gp = std::min(grid, (c.red_blocks / 8) * M);                                                     \
+    if (nl != 16) k_mix_hop_q16r<8, KIND, B, false, M, true, true><<<gp, QB, 0, c.s>>>(Q16_ARGS, c_long);     \
+    else if (recon) k_mix_hop_q16r<16, KIND, B, true, M, true, true><<<gp, QB, 0, c.s>>>(Q16_ARGS, c_long);   \
+    else k_mix_hop_q16r<16, KIND, B, false, M, true, true><<<gp, QB, 0, c.s>>>(Q16_ARGS, c_long);             \
+  } while (0)
 #define Q16A(RR, M)                                                                                       \
   do {                                                                                                    \
     const int gp = std::min(grid, (c.red_blocks / 8) * M);                                                \
@@ -853,6 +875,13 @@ static void launch_q16(int variant, int nl, bool recon, float c_long, int grid, 
     case 17: Q16A(3, 6); break;    // cp.async ring of 3 slots ahead
     case 18: Q16A(2, 8); break;
     case 19: Q16A(4, 5); break;
+    case 20: Q16RPK(2, 6); break;   // persistent, packed FP32x2 arithmetic
+    case 21: Q16RPK(2, 7); break;
+    case 22: Q16RPK(2, 8); break;
+    case 23: Q16RPK(4, 6); break;
+    case 24: Q16RPK(4, 7); break;
+    case 25: Q16RPK(4, 5); break;
+    case 26: Q16RPK(8, 6); break;
     case 1:
       if (nl == 16) k_mix_hop_q16<16, KIND, 2><<<grid, QB, 4 * QSLOT, c.s>>>(Q16_ARGS);
       else k_mix_hop_q16<8, KIND, 2><<<grid, QB, 4 * QSLOT, c.s>>>(Q16_ARGS);

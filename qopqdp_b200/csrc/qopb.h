@@ -105,7 +105,7 @@ struct Options {
   int half_format = 0;           // 16-bit storage: 0 int16 fixed point, 1 IEEE FP16, 2 FP16 links
   double ru_delta = 0.3;         // reliable-update threshold on |r| (0.3-0.5 measured best)
   int chunk = 16;                // iterations launched per host check
-  int hop_kernel = 15;           // int16 hop variant (mixed.cu launch_q16); 15 measured fastest
+  int hop_kernel = 25;           // int16 hop variant (mixed.cu launch_q16); 25 measured fastest
   int recon_long = 1;            // int16 long links as two rows + det phase when exact
   int batch_kernel = 7;          // batched int16 hop variant (batch.cu kBhop); 7 measured fastest
   int multi_shift = 0;           // int16 multi-mass: 1 = sloppy multi-shift CG before the batched refinement
