@@ -107,7 +107,7 @@ struct Options {
   int chunk = 16;                // iterations launched per host check
   int hop_kernel = 25;           // int16 hop variant (mixed.cu launch_q16); 25 measured fastest
   int recon_long = 1;            // int16 long links as two rows + det phase when exact
-  int batch_kernel = 7;          // batched int16 hop variant (batch.cu kBhop); 7 measured fastest
+  int batch_kernel = -1;         // batched int16 hop variant (batch.cu kBhop); -1: by the number of systems
   int multi_shift = 0;           // int16 multi-mass: 1 = sloppy multi-shift CG before the batched refinement
   // QOP_asqtad_force_set_opts (lib/asqtad_force.c:3-41)
   int force_fnmat_src_min = 2, force_veclength = 4;

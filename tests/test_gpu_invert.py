@@ -63,9 +63,39 @@ def test_invert_eo_source(prec, rsq, eo):
         # FP64 rounding differs between the device reductions and the oracle's
         # OpenMP reductions (whose order depends on the host's thread count)
         assert abs(ra.final_iter - ora.final_iter) <= 0.02 * ora.final_iter + 3
+    # examples/asqtad_test.c:101-127: re-solving from the solution needs
+    # (almost) no iterations
+    ia2, ra2 = args(eo, rsq)
+    assert q.invert(fla, m, hout, hin, ia2, ra2).status == 0
+    assert ra2.final_iter <= 2, ra2.final_iter
     q.destroy_V(hin)
     q.destroy_V(hout)
     q.destroy_L(fla)
+
+
+@pytest.mark.parametrize("eo", [0, 1])
+def test_mixed_solver_restart_from_solution(eo):
+    """The int16 mixed solver started from a converged FP64 solution stops
+    after its first true-residual check (asqtad_test.c:101-127)."""
+    q, fla, fo = links("D")
+    m = 0.05
+    src = LT.gaussian_vector(L, 60 + eo)
+    hin, hout = q.create_V(src), q.create_V(np.zeros_like(src))
+    try:
+        assert q.set_opts(prec_sloppy=16) == 0
+        ia, ra = args(eo, 1e-20)
+        assert q.invert(fla, m, hout, hin, ia, ra).status == 0
+        first = ra.final_iter
+        ia2, ra2 = args(eo, 1e-20)
+        assert q.invert(fla, m, hout, hin, ia2, ra2).status == 0
+        got = q.extract_V(hout, V)
+        assert eo_residual(fo, m, got, src, L, eo) <= 1.05e-20
+        assert ra2.final_iter <= 2, (first, ra2.final_iter)
+    finally:
+        q.set_opts(prec_sloppy=64)
+        q.destroy_V(hin)
+        q.destroy_V(hout)
+        q.destroy_L(fla)
 
 
 @pytest.mark.parametrize("prec,rsq", [("D", 1e-20), ("F", 1e-10)])
