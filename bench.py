@@ -68,6 +68,8 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--quick", action="store_true", help="skip FP64 baseline and e2e (development)")
     ap.add_argument("--dd-mask", type=int, default=15, help="dd workload on one GPU: self-split directions")
+    ap.add_argument("--hop-kernel", type=int, default=None, help="int16 hop variant (library default if unset)")
+    ap.add_argument("--batch-kernel", type=int, default=None, help="batched hop variant (chosen by batch size if unset)")
     ap.add_argument("--workload", default="single",
                     choices=["single", "multimass", "multisrc", "serve", "small", "force", "dd"],
                     help="single: the headline solve; multimass / multisrc: batched invert_multi workloads; "
@@ -75,6 +77,16 @@ def parse():
     ap.add_argument("--serve-burst", type=int, default=12, help="requests of the peak-throughput burst")
     ap.add_argument("--serve-seconds", type=float, default=20.0, help="arrival window per load level")
     return ap.parse_args()
+
+
+def kernel_opts(a):
+    """Kernel-variant options given on the command line (else library defaults)."""
+    o = {}
+    if a.hop_kernel is not None:
+        o["hop_kernel"] = a.hop_kernel
+    if a.batch_kernel is not None:
+        o["batch_kernel"] = a.batch_kernel
+    return o
 
 
 def rank_info():
@@ -280,7 +292,7 @@ def run_b200(a):
     big = 1 << 30
 
     def solve(hout, hin, prec):
-        q.set_opts(prec_sloppy=prec, half_format=0, ru_delta=a.ru_delta)
+        q.set_opts(prec_sloppy=prec, half_format=0, ru_delta=a.ru_delta, **kernel_opts(a))
         q.dslash(fla, 0.0, hout, hout, QOP_EVEN, QOP_EVEN)          # zero initial guess
         ia = QOP_invert_arg_t(1e9, 200000, 200000, 10, QOP_EVEN)
         ra = QOP_resid_arg_t(rsq, 0, 0, 0, 0, 0)
@@ -494,7 +506,7 @@ def run_multi(a):
     rsq = a.tol * a.tol
 
     def step(prec, ms=masses, ins=hins):
-        q.set_opts(prec_sloppy=prec, half_format=0, ru_delta=a.ru_delta)
+        q.set_opts(prec_sloppy=prec, half_format=0, ru_delta=a.ru_delta, **kernel_opts(a))
         outs = [[q.create_V(np.zeros_like(srcs[0])) for _ in m] for m in ms]
         ras = [[QOP_resid_arg_t(rsq, 0, 0, 0, 0, 0) for _ in m] for m in ms]
         ia = QOP_invert_arg_t(1e9, 200000, 200000, 50, QOP_EVEN)

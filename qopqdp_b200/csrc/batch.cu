@@ -65,13 +65,38 @@ __device__ __forceinline__ float q16_link_recon(const uint4 ua, const uint2 ub, 
   return cl * (1.0f / 32767.0f);
 }
 
+// the same two decodes with the (re, im) pairs formed by one packed add
+__device__ __forceinline__ float q16_link_pk(const uint4 ua, const uint4 ub, const uint2 uc, float2 U[9]) {
+  U[0] = u16_pair(ua.x); U[1] = u16_pair(ua.y); U[2] = u16_pair(ua.z); U[3] = u16_pair(ua.w);
+  U[4] = u16_pair(ub.x); U[5] = u16_pair(ub.y); U[6] = u16_pair(ub.z); U[7] = u16_pair(ub.w);
+  U[8] = u16_pair(uc.x);
+  return __uint_as_float(uc.y) * (1.0f / 32767.0f);
+}
+__device__ __forceinline__ float q16_link_recon_pk(const uint4 ua, const uint2 ub, const float phase, const float cl,
+                                                   float2 U[9]) {
+  U[0] = u16_pair(ua.x); U[1] = u16_pair(ua.y); U[2] = u16_pair(ua.z); U[3] = u16_pair(ua.w);
+  U[4] = u16_pair(ub.x); U[5] = u16_pair(ub.y);
+  float sn, cs;
+  __sincosf(phase, &sn, &cs);
+  const float2 z = make_float2(cs * (1.0f / 32767.0f), sn * (1.0f / 32767.0f));
+  const float2 c0 = csub<float>(cmul<float>(U[1], U[5]), cmul<float>(U[2], U[4]));
+  const float2 c1 = csub<float>(cmul<float>(U[2], U[3]), cmul<float>(U[0], U[5]));
+  const float2 c2 = csub<float>(cmul<float>(U[0], U[4]), cmul<float>(U[1], U[3]));
+  U[6] = cmul<float>(z, make_float2(c0.x, -c0.y));
+  U[7] = cmul<float>(z, make_float2(c1.x, -c1.y));
+  U[8] = cmul<float>(z, make_float2(c2.x, -c2.y));
+  return cl * (1.0f / 32767.0f);
+}
+
 // Blocks are (site block sb, system group grp) flattened with the group
 // fastest, so the blocks that share a site block's links run together and
 // the links come from HBM once.  Vectors are [system][Vh] int16 sites.
 // BG systems per thread (and per block); MINB resident blocks per SM; UNR
 // slots unrolled (NL: straight-line code; 1: a loop over the slots, less
-// code and fewer registers)
-template <int NL, int KIND, bool RECON, int BG, int MINB, int UNR = NL>
+// code and fewer registers); PK: the link pairs multiply pre-scaled,
+// duplicated site components into two packed accumulators per row
+// (q16_pk_mul in mixed.cuh) instead of the duplicated, negated link copies
+template <int NL, int KIND, bool RECON, int BG, int MINB, int UNR = NL, bool PK = false>
 __global__ void __launch_bounds__(QB, MINB)
 k_bhop(uint4 *__restrict__ out, const uint4 *__restrict__ src, const unsigned char *__restrict__ lk,
        const uint4 *__restrict__ same, Geom g, NbrGeom ng, int p, MixState *st, int nsys, int ngrp, double *part,
@@ -97,9 +122,13 @@ k_bhop(uint4 *__restrict__ out, const uint4 *__restrict__ src, const unsigned ch
     site_coords(g, i, p, x);
     const int x0 = x[0], x1 = x[1], x2 = x[2], x3 = x[3];
     const int lex = ((x0 * g.L[1] + x1) * g.L[2] + x2) * g.L[3] + x3;
-    float2 a[BG][3];
+    float2 a[BG][3], pt[PK ? BG : 1][3], ps[PK ? BG : 1][3];
 #pragma unroll
     for (int b = 0; b < BG; b++) a[b][0] = a[b][1] = a[b][2] = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int b = 0; b < (PK ? BG : 1); b++)
+#pragma unroll
+      for (int r = 0; r < 3; r++) pt[b][r] = ps[b][r] = make_float2(0.f, 0.f);
     const unsigned char *gl = lk + (size_t)sb * q16_block_bytes(NL, RECON);
 #pragma unroll UNR
     for (int k = 0; k < NL; k++) {
@@ -110,12 +139,12 @@ k_bhop(uint4 *__restrict__ out, const uint4 *__restrict__ src, const unsigned ch
         const uint4 ua = __ldcs(reinterpret_cast<const uint4 *>(ls) + tid);
         const uint2 ub = __ldcs(reinterpret_cast<const uint2 *>(ls + 16 * QB) + tid);
         const float ph = __ldcs(reinterpret_cast<const float *>(ls + 24 * QB) + tid);
-        sl = q16_link_recon(ua, ub, ph, c_long, U);
+        sl = PK ? q16_link_recon_pk(ua, ub, ph, c_long, U) : q16_link_recon(ua, ub, ph, c_long, U);
       } else {
         const uint4 ua = __ldcs(reinterpret_cast<const uint4 *>(ls) + tid);
         const uint4 ub = __ldcs(reinterpret_cast<const uint4 *>(ls + 16 * QB) + tid);
         const uint2 uc = __ldcs(reinterpret_cast<const uint2 *>(ls + 32 * QB) + tid);
-        sl = q16_link(ua, ub, uc, U);
+        sl = PK ? q16_link_pk(ua, ub, uc, U) : q16_link(ua, ub, uc, U);
       }
       int nbi;
       if constexpr (UNR == NL) nbi = nbr_fast(ng, x, lex, slot_mu<NL>(k), slot_disp<NL>(k));
@@ -123,6 +152,16 @@ k_bhop(uint4 *__restrict__ out, const uint4 *__restrict__ src, const unsigned ch
       uint4 nb[BG];
 #pragma unroll
       for (int b = 0; b < BG; b++) nb[b] = act[b] ? src[(i64)(j0 + b) * Vh + nbi] : make_uint4(0, 0, 0, 0);
+      if constexpr (PK) {
+#pragma unroll
+        for (int b = 0; b < BG; b++) {
+          if (!act[b]) continue;
+          float2 vx[3], vy[3];
+          q16_pk_site(nb[b], sl, vx, vy);
+          q16_pk_mul(U, vx, vy, pt[b], ps[b]);
+        }
+        continue;
+      }
       // packed FP32x2 FMAs (sm_100): t += (Re u, Re u)(v.x, v.y) + (-Im u, Im u)(v.y, v.x)
       // rounds every lane exactly as the scalar complex FMA sequence does
       float2 ur[9], ui[9];
@@ -149,6 +188,10 @@ k_bhop(uint4 *__restrict__ out, const uint4 *__restrict__ src, const unsigned ch
           a[b][r] = __ffma2_rn(sc2, t, a[b][r]);
         }
       }
+    }
+    if constexpr (PK) {
+#pragma unroll
+      for (int b = 0; b < BG; b++) q16_pk_rows(pt[b], ps[b], a[b]);
     }
 #pragma unroll
     for (int b = 0; b < BG; b++) {
@@ -253,13 +296,18 @@ k_bp(uint4 *__restrict__ p, const uint4 *__restrict__ r, i64 Vh, const MixState 
 // with 11 and 4 (16 / 8 systems, fully unrolled: ~240 registers).  The
 // kernel issues ~60-90 instructions per system and slot at ~55% issue
 // utilisation; HBM traffic equals the compulsory bytes (ncu), so it is
-// instruction- and latency-bound, not HBM-bound.
+// instruction- and latency-bound, not HBM-bound.  12-15 use the packed pair
+// form of the one-system hop (q16_pk_mul): 550 us with 4 systems per thread
+// (12, against 577 for 1), but 625 / 810 us with 8 (13 / 14: two
+// accumulators per row and system exceed the register budget), so 7 stays
+// the choice for 16 systems; at 24^3x48 with 12 systems 12 and 1 tie
+// (114.0 / 113.8 us).
 struct BhopShape { int bg, minb; };
 static const BhopShape kBhop[] = {{4, 1}, {4, 5}, {2, 8}, {2, 1}, {8, 1}, {4, 6}, {4, 5}, {8, 3}, {8, 2},
-                                  {8, 3}, {8, 4}, {16, 2}};
+                                  {8, 3}, {8, 4}, {16, 2}, {4, 5}, {8, 3}, {8, 2}, {4, 4}};
 constexpr int N_BHOP = (int)(sizeof(kBhop) / sizeof(kBhop[0]));
 
-template <int KIND, int BG, int MINB, int UNR = 16>
+template <int KIND, int BG, int MINB, int UNR = 16, bool PK = false>
 static void launch_bhop_t(int nl, bool recon, int ngrp, int nsb, uint4 *out, const uint4 *src,
                           const unsigned char *lk, const uint4 *same, const Geom &g, const NbrGeom &ng, int par,
                           MixState *st, int nsys, double *part, unsigned *count, float c_long) {
@@ -267,9 +315,9 @@ static void launch_bhop_t(int nl, bool recon, int ngrp, int nsb, uint4 *out, con
   const int grid = ngrp * nsb;
 #define BH_ARGS out, src, lk, same, g, ng, par, st, nsys, ngrp, part, count, c_long
   constexpr int U8 = UNR < 8 ? UNR : 8;
-  if (nl != 16) k_bhop<8, KIND, false, BG, MINB, U8><<<grid, QB, 0, c.s>>>(BH_ARGS);
-  else if (recon) k_bhop<16, KIND, true, BG, MINB, UNR><<<grid, QB, 0, c.s>>>(BH_ARGS);
-  else k_bhop<16, KIND, false, BG, MINB, UNR><<<grid, QB, 0, c.s>>>(BH_ARGS);
+  if (nl != 16) k_bhop<8, KIND, false, BG, MINB, U8, PK><<<grid, QB, 0, c.s>>>(BH_ARGS);
+  else if (recon) k_bhop<16, KIND, true, BG, MINB, UNR, PK><<<grid, QB, 0, c.s>>>(BH_ARGS);
+  else k_bhop<16, KIND, false, BG, MINB, UNR, PK><<<grid, QB, 0, c.s>>>(BH_ARGS);
 #undef BH_ARGS
 }
 
@@ -291,6 +339,10 @@ static void launch_bhop(int variant, int nl, bool recon, int ngrp, int nsb, uint
     case 9: BH_CALL(8, 3, 4); break;
     case 10: BH_CALL(8, 4, 1); break;
     case 11: BH_CALL(16, 2, 1); break;
+    case 12: BH_CALL(4, 5, 16, true); break;   // packed pairs (q16_pk_mul)
+    case 13: BH_CALL(8, 3, 2, true); break;
+    case 14: BH_CALL(8, 2, 1, true); break;
+    case 15: BH_CALL(4, 4, 2, true); break;
     default: BH_CALL(4, 1); break;
   }
 #undef BH_CALL

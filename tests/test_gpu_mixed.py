@@ -262,7 +262,7 @@ def test_every_hop_kernel_variant():
 
 
 def test_every_batch_kernel_variant():
-    """Each selectable batched hop (option batch_kernel 0-11) solves a
+    """Each selectable batched hop (option batch_kernel 0-15) solves a
     four-source batch to the FP64 target with the iteration counts of the
     default variant."""
     L = (8, 8, 8, 8)
@@ -273,14 +273,14 @@ def test_every_batch_kernel_variant():
     srcs = [LT.gaussian_vector(L, 340 + s) for s in range(4)]
     ms = [[0.03], [0.05], [0.03], [0.1]]
     its = {}
-    for v in range(12):
+    for v in range(16):
         assert q.set_opts(prec_sloppy=16, batch_kernel=v) == 0
         info, ras, outs = _run_multi(q, fla, ms, srcs, 1e-20)
         assert info.status == 0
         for s in range(4):
             assert eo_residual(fo, ms[s][0], outs[s][0], srcs[s], L, 0) <= 1.05e-20, (v, s)
         its[v] = [r[0].final_iter for r in ras]
-    assert q.set_opts(batch_kernel=12) != 0
+    assert q.set_opts(batch_kernel=16) != 0
     assert q.set_opts(prec_sloppy=64, batch_kernel=-1) == 0
     for v, it in its.items():
         assert all(abs(a - b) <= 0.03 * b + 3 for a, b in zip(it, its[7])), its
