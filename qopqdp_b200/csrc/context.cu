@@ -292,6 +292,8 @@ QOP_status_t QOP_asqtad_invert_set_opts(QOP_opt_t opts[], int nopts) {
       n.batch_kernel = (int)v;
     } else if (!strcmp(t, "multi_shift")) {
       n.multi_shift = v != 0;
+    } else if (!strcmp(t, "fuse_update")) {
+      n.fuse_update = v != 0;
     } else if (!strcmp(t, "recon_long")) {
       n.recon_long = v != 0;
     } else if (!strcmp(t, "hop_kernel")) {

@@ -138,6 +138,40 @@ k_mix_p(typename Sp::elem *__restrict__ p, const typename Sp::elem *__restrict__
   Sp::store(p, i, Vh, pv);
 }
 
+// x += alpha p, r -= alpha Ap and p = r + beta p in one pass (fused update:
+// the scalars come from the KIND 3 hop).  Runs only for the iteration whose
+// hop recorded `seq` in tok; when that hop set MIX_UPDATE, p is left to the
+// reliable update, which recomputes beta from the true residual.
+template <class Sp>
+__global__ void __launch_bounds__(256)
+k_mix_update_p(float2 *__restrict__ xs, typename Sp::elem *__restrict__ r, typename Sp::elem *__restrict__ p,
+               const typename Sp::elem *__restrict__ Ap, i64 Vh, const MixState *st, int seq) {
+  if (st->tok != seq) return;
+  const int fl = st->flag;
+  if (fl != MIX_RUN && fl != MIX_UPDATE) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= Vh) return;
+  const float al = (float)st->alpha, be = (float)st->beta;
+  float2 pv[3], av[3], rv[3];
+  Sp::load(p, i, Vh, pv);
+  Sp::load(Ap, i, Vh, av);
+  Sp::load(r, i, Vh, rv);
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    float2 xv = xs[c * Vh + i];
+    xv.x = fmaf(al, pv[c].x, xv.x);
+    xv.y = fmaf(al, pv[c].y, xv.y);
+    xs[c * Vh + i] = xv;
+    rv[c].x = fmaf(-al, av[c].x, rv[c].x);
+    rv[c].y = fmaf(-al, av[c].y, rv[c].y);
+  }
+  Sp::store(r, i, Vh, rv);
+  if (fl != MIX_RUN) return;
+#pragma unroll
+  for (int c = 0; c < 3; c++) pv[c] = make_float2(fmaf(be, pv[c].x, rv[c].x), fmaf(be, pv[c].y, rv[c].y));
+  Sp::store(p, i, Vh, pv);
+}
+
 // ---------------------------------------------------------------- multi-shift
 // Shifted systems (A + sigma_s) x_s = b ride on the base recursion with the
 // multi-shift CG recurrences of lib/invert_cg_p.c:234-252 and :356-362:
@@ -478,6 +512,39 @@ __device__ __forceinline__ void q16_finish(double (&acc1)[1], double *part, unsi
   }
 }
 
+// KIND 3 (fused update): the KIND 2 hop that also reduces <r, Ap> and
+// |Ap|^2, so that its last block knows alpha, the new |r|^2 =
+// |r|^2 - 2 alpha <r, Ap> + alpha^2 |Ap|^2 and beta before the update runs
+__device__ __forceinline__ void q16_epilogue3(uint4 *out, const uint4 *same, const uint4 *rres, int i, i64 Vh,
+                                              float m2, float2 a[3], double (&acc)[3]) {
+  acc[0] += q16_epilogue<2>(out, same, i, Vh, m2, a);   // a becomes Ap
+  float2 rv[3];
+  SpQ16::load(rres, i, Vh, rv);
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    acc[1] += (double)rv[c].x * a[c].x + (double)rv[c].y * a[c].y;
+    acc[2] += (double)a[c].x * a[c].x + (double)a[c].y * a[c].y;
+  }
+}
+
+__device__ __forceinline__ void q16_finish3(double (&acc)[3], double *part, unsigned *count, MixState *st, int seq) {
+  if (grid_sum<3>(acc, part, count, st->red3)) {
+    if (st->flag != MIX_RUN) return;
+    const double pAp = st->dp2 + st->m2 * st->red3[0];
+    if (!(pAp > 0)) { st->flag = MIX_BREAK; return; }
+    const double al = st->rsq / pAp;
+    const double rn = st->rsq - 2.0 * al * st->red3[1] + al * al * st->red3[2];
+    st->alpha = al;
+    st->iter += 1;
+    st->rsq_old = st->rsq;
+    st->rsq = rn;
+    st->beta = rn / st->rsq_old;
+    if (rn > st->maxr2) st->maxr2 = rn;
+    st->tok = seq;
+    if (!(rn > 0) || rn < st->delta2 * st->maxr2 || rn <= st->stop || st->iter >= st->max_iter) st->flag = MIX_UPDATE;
+  }
+}
+
 template <int NL, int KIND, int GRP>
 __global__ void __launch_bounds__(QB)
 k_mix_hop_q16(uint4 *__restrict__ out, const uint4 *__restrict__ src, const unsigned char *__restrict__ lk,
@@ -664,12 +731,14 @@ template <int NL, int KIND, int BATCH, bool RECON, int MINB = 1, bool PERSIST = 
 __global__ void __launch_bounds__(QB, MINB)
 k_mix_hop_q16r(uint4 *__restrict__ out, const uint4 *__restrict__ src, const unsigned char *__restrict__ lk,
                const uint4 *__restrict__ same, Geom g, NbrGeom ng, int p, MixState *st, double *part,
-               unsigned *count, float c_long) {
+               unsigned *count, float c_long, const uint4 *__restrict__ rres = nullptr, int seq = 0) {
   if (st->flag) return;
   const int tid = threadIdx.x;
   const i64 Vh = g.Vh;
   const int nsb = PERSIST ? (int)((Vh + QB - 1) / QB) : 0;
-  double acc1[1] = {0.0};
+  double acc1[KIND == 3 ? 3 : 1];
+#pragma unroll
+  for (int k = 0; k < (KIND == 3 ? 3 : 1); k++) acc1[k] = 0.0;
   int sb = blockIdx.x;
   do {
   const int i = sb * QB + tid;
@@ -714,10 +783,12 @@ k_mix_hop_q16r(uint4 *__restrict__ out, const uint4 *__restrict__ src, const uns
       }
     }
     if (PK) q16_pk_rows(pt, ps, a);
-    acc1[0] += q16_epilogue<KIND>(out, same, i, Vh, (float)st->m2, a);
+    if constexpr (KIND == 3) q16_epilogue3(out, same, rres, i, Vh, (float)st->m2, a, acc1);
+    else acc1[0] += q16_epilogue<KIND>(out, same, i, Vh, (float)st->m2, a);
   }
   } while (PERSIST && (sb += gridDim.x) < nsb);
-  q16_finish<KIND>(acc1, part, count, st);
+  if constexpr (KIND == 3) q16_finish3(acc1, part, count, st, seq);
+  else q16_finish<KIND>(acc1, part, count, st);
 }
 
 
@@ -821,6 +892,32 @@ LinksSloppy links_parity(SloppyLinks *s, int lkfmt, int p) {
 // default), 110.0 with 23, 111.2 with 20 / 21, 112-113 with 22, 24, 26,
 // against 117.3 for the scalar variant 15 (a third fewer instructions per
 // slot; the kernel was issue-bound at 62 % issue-active).
+// KIND 3 hops (fused update) exist for the persistent packed variants 20-26
+static void launch_q16_fused(int variant, int nl, bool recon, float c_long, int grid, uint4 *out, const uint4 *src,
+                             const unsigned char *lk, const uint4 *same, const Geom &g, const NbrGeom &ng, int par,
+                             MixState *st, const uint4 *rres, int seq) {
+  Context &c = ctx();
+#define Q16_ARGS3 out, src, lk, same, g, ng, par, st, c.d_part, c.d_count, c_long, rres, seq
+#define Q16RPK3(B, M)                                                                                          \
+  do {                                                                                                         \
+    const int gp = std::min(grid, (c.red_blocks / 8) * M);                                                     \
+    if (nl != 16) k_mix_hop_q16r<8, 3, B, false, M, true, true><<<gp, QB, 0, c.s>>>(Q16_ARGS3);               \
+    else if (recon) k_mix_hop_q16r<16, 3, B, true, M, true, true><<<gp, QB, 0, c.s>>>(Q16_ARGS3);             \
+    else k_mix_hop_q16r<16, 3, B, false, M, true, true><<<gp, QB, 0, c.s>>>(Q16_ARGS3);                       \
+  } while (0)
+  switch (variant) {
+    case 20: Q16RPK3(2, 6); break;
+    case 21: Q16RPK3(2, 7); break;
+    case 22: Q16RPK3(2, 8); break;
+    case 23: Q16RPK3(4, 6); break;
+    case 24: Q16RPK3(4, 7); break;
+    case 26: Q16RPK3(8, 6); break;
+    default: Q16RPK3(4, 5); break;
+  }
+#undef Q16RPK3
+#undef Q16_ARGS3
+}
+
 template <int KIND>
 static void launch_q16(int variant, int nl, bool recon, float c_long, int grid, uint4 *out, const uint4 *src,
                        const unsigned char *lk, const uint4 *same, const Geom &g, const NbrGeom &ng, int par,
@@ -1003,6 +1100,11 @@ static void run_mixed(LinOp<double> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t *r
   int nru = 0, stalls = 0;
   double r2 = b2;
   const int chunk = c.opt.chunk;
+  // fused update (option fuse_update): the second hop reduces what the
+  // update needs and one kernel updates x, r and p
+  constexpr bool q16v = std::is_same<Lk, LkQ16B>::value && std::is_same<Sp, SpQ16>::value;
+  const bool fuse = q16v && ns == 1 && c.opt.fuse_update && c.opt.hop_kernel >= 20;
+  int seq = 0;
   while (true) {
     const int it0 = h.iter;
     int prof0 = -1;
@@ -1020,8 +1122,12 @@ static void run_mixed(LinOp<double> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t *r
         recs.push_back(ps1.idx);
       }
       {
-        ProfScope ps2(hname, hop_bytes + (double)Vh * Sp::site_bytes);
-        if constexpr (std::is_same<Lk, LkQ16B>::value) {
+        ProfScope ps2(hname, hop_bytes + (double)Vh * Sp::site_bytes * (fuse ? 2 : 1));
+        if constexpr (q16v) {
+          const unsigned char *lp = (const unsigned char *)lk_p.a;
+          if (fuse) launch_q16_fused(c.opt.hop_kernel, nl, recon, c_long, gridq, Aps, ts, lp, ps, g, ng, p, dst, rs, ++seq);
+          else launch_q16<2>(c.opt.hop_kernel, nl, recon, c_long, gridq, Aps, ts, lp, ps, g, ng, p, dst);
+        } else if constexpr (std::is_same<Lk, LkQ16B>::value) {
           const unsigned char *lp = (const unsigned char *)lk_p.a;
           launch_q16<2>(c.opt.hop_kernel, nl, recon, c_long, gridq, Aps, ts, lp, ps, g, ng, p, dst);
         } else {
@@ -1033,11 +1139,15 @@ static void run_mixed(LinOp<double> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t *r
       if (ns > 1) {
         k_ms_update<Sp><<<gridv, 256, 0, c.s>>>(xs, rs, ps, Aps, Vh, dst, c.d_part, c.d_count, dsh, ns, mv);
         k_ms_p<Sp><<<gridv, 256, 0, c.s>>>(ps, rs, Vh, dst, dsh, ns, mv);
+        QLAUNCHN(4);
+      } else if (fuse) {
+        k_mix_update_p<Sp><<<gridv, 256, 0, c.s>>>(xs, rs, ps, Aps, Vh, dst, seq);
+        QLAUNCHN(3);
       } else {
         k_mix_update<Sp><<<gridv, 256, 0, c.s>>>(xs, rs, ps, Aps, Vh, dst, c.d_part, c.d_count);
         k_mix_p<Sp><<<gridv, 256, 0, c.s>>>(ps, rs, Vh, dst);
+        QLAUNCHN(4);
       }
-      QLAUNCHN(4);
     }
     (void)prof0;
     QCHECK(cudaMemcpyAsync(&h, dst, sizeof h, cudaMemcpyDeviceToHost, c.s));

@@ -162,7 +162,8 @@ struct LkF16 {
 enum { MIX_RUN = 0, MIX_UPDATE = 1, MIX_BREAK = 2 };
 struct MixState {
   double rsq, rsq_old, alpha, beta, dp2, maxr2, stop, delta2, m2, red;
-  int iter, max_iter, flag, pad;
+  int iter, max_iter, flag, tok;   // tok: iteration whose hop set alpha (fused update)
+  double red3[3];
 };
 
 __device__ __forceinline__ void cfmaf(float2 &a, float2 u, float2 v) {

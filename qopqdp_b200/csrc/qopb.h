@@ -109,6 +109,7 @@ struct Options {
   int recon_long = 1;            // int16 long links as two rows + det phase when exact
   int batch_kernel = -1;         // batched int16 hop variant (batch.cu kBhop); -1: by the number of systems
   int multi_shift = 0;           // int16 multi-mass: 1 = sloppy multi-shift CG before the batched refinement
+  int fuse_update = 1;           // int16 hop variants 20-26: 1 = the second hop reduces for a fused x / r / p update
   // QOP_asqtad_force_set_opts (lib/asqtad_force.c:3-41)
   int force_fnmat_src_min = 2, force_veclength = 4;
   // QOP_hisq_links_set_opts (lib/hisq_links.c:4-78)

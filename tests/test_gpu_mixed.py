@@ -224,8 +224,8 @@ def test_mixed_multi_source(L, kind):
     q.destroy_L(fla)
 
 
-def _single_iters(q, fla, src, m, L):
-    ia = QOP_invert_arg_t(1e9, 20000, 20000, 5, 0)
+def _single_iters(q, fla, src, m, L, eo=0):
+    ia = QOP_invert_arg_t(1e9, 20000, 20000, 5, eo)
     ra = QOP_resid_arg_t(1e-20, 0, 0, 0, 0, 0)
     hin, hout = q.create_V(src), q.create_V(np.zeros_like(src))
     info = q.invert(fla, m, hout, hin, ia, ra)
@@ -259,6 +259,33 @@ def test_every_hop_kernel_variant():
     ref = its[25]
     assert all(abs(i - ref) <= 0.03 * ref + 3 for i in its.values()), its
     q.destroy_L(fla)
+
+
+def test_fused_update_solves_like_the_four_kernel_iteration():
+    """Option fuse_update (packed hop variants 20-26): the second hop also
+    reduces <r, Ap> and |Ap|^2 and one kernel updates x, r and p; the
+    solves reach the FP64 target with the iteration counts of the
+    four-kernel iteration (within rounding noise)."""
+    L = (8, 8, 8, 8)
+    q = gpu_lattice(L, "D")
+    fat, lng, _, _ = hisq_links(L, 0.5, 9)
+    fo = O.Fla(O.Lattice(L), fat, lng)
+    fla = q.create_L_from_raw(fat, lng)
+    try:
+        for v in (20, 23, 25):
+            its = []
+            for fuse in (0, 1):
+                assert q.set_opts(prec_sloppy=16, hop_kernel=v, fuse_update=fuse) == 0
+                for eo, mass, seed in ((0, 0.03, 331), (1, 0.01, 332)):
+                    src = LT.gaussian_vector(L, seed)
+                    st, it, got = _single_iters(q, fla, src, mass, L, eo)
+                    assert st == 0
+                    assert eo_residual(fo, mass, got, src, L, eo) <= 1.05e-20, (v, fuse, eo)
+                    its.append(it)
+            assert all(abs(a - b) <= 0.03 * b + 3 for a, b in zip(its[2:], its[:2])), (v, its)
+    finally:
+        assert q.set_opts(prec_sloppy=64, hop_kernel=25, fuse_update=1) == 0
+        q.destroy_L(fla)
 
 
 def test_every_batch_kernel_variant():
