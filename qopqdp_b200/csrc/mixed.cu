@@ -1073,8 +1073,9 @@ static void run_mixed(LinOp<double> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t *r
   const double hop_bytes = (double)Vh * (link_site + 2 * Sp::site_bytes);
   const bool recon = sl->recon != 0;
   const float c_long = (float)sl->c_long;
-  char hname[32];
+  char hname[32], hname3[40];
   snprintf(hname, sizeof hname, "hop_%s_link%s", Sp::name(), Lk::name());
+  snprintf(hname3, sizeof hname3, "hop_%s_upd_link%s", Sp::name(), Lk::name());   // the fused-update hop
 
   auto refresh = [&](double r2) {   // sloppy r <- r, new residual reference
     k_to_sloppy<Sp><<<gridv, 256, 0, c.s>>>(rs, r + is.off, Vh);
@@ -1122,7 +1123,7 @@ static void run_mixed(LinOp<double> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t *r
         recs.push_back(ps1.idx);
       }
       {
-        ProfScope ps2(hname, hop_bytes + (double)Vh * Sp::site_bytes * (fuse ? 2 : 1));
+        ProfScope ps2(fuse ? hname3 : hname, hop_bytes + (double)Vh * Sp::site_bytes * (fuse ? 2 : 1));
         if constexpr (q16v) {
           const unsigned char *lp = (const unsigned char *)lk_p.a;
           if (fuse) launch_q16_fused(c.opt.hop_kernel, nl, recon, c_long, gridq, Aps, ts, lp, ps, g, ng, p, dst, rs, ++seq);
