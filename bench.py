@@ -70,6 +70,8 @@ def parse():
     ap.add_argument("--dd-mask", type=int, default=15, help="dd workload on one GPU: self-split directions")
     ap.add_argument("--hop-kernel", type=int, default=None, help="int16 hop variant (library default if unset)")
     ap.add_argument("--batch-kernel", type=int, default=None, help="batched hop variant (chosen by batch size if unset)")
+    ap.add_argument("--ab", default=None, help="A/B of a 0/1 solver option (e.g. fuse_update) on the headline solve: "
+                                               "--steps pairs of solves interleaved in one process, clocks sampled")
     ap.add_argument("--workload", default="single",
                     choices=["single", "multimass", "multisrc", "serve", "small", "force", "dd"],
                     help="single: the headline solve; multimass / multisrc: batched invert_multi workloads; "
@@ -770,6 +772,62 @@ def run_force(a):
     q.destroy_G(G)
 
 
+def run_ab(a):
+    """Interleaved A/B of a 0/1 option of QOP_asqtad_invert_set_opts on the
+    headline solve (the single workload's lattice, links, source and
+    target): --steps rounds, each timing two solves with the option 0 and
+    two with 1 (order alternating between rounds), CUDA events on the
+    library stream, SM clock and power sampled during each pair."""
+    import ctypes as C
+    import torch
+    torch.cuda.set_device(0)
+    from qopqdp_b200 import lattice as LT
+    from qopqdp_b200.qop import Qop, QOP_invert_arg_t, QOP_resid_arg_t, QOP_EVEN, load_library
+    L = tuple(int(x) for x in (a.lattice or "32,32,32,64").split(","))
+    q = Qop("D")
+    assert q.init(L) == 0
+    lib = load_library()
+    lib.QOPB_stream.restype = C.c_void_p
+    U = LT.random_gauge(L, a.eps, a.seed, device="cuda")
+    G = q.create_G(U)
+    del U
+    q.rephase_G(G, LT.BENCH_R0, LT.BENCH_BC, LT.BENCH_SIGNMASK)
+    q.set_hisq_opts(want_aux=0)
+    H = q.hisq_create_L_from_G(LT.hisq_bench_coeffs(), G)
+    q.destroy_G(G)
+    fla = q.hisq_asqtad_links(H, 0)
+    src = LT.gaussian_vector(L, a.seed)
+    hin, hout = q.create_V(src, QOP_EVEN), q.create_V(np.zeros_like(src))
+    stream = torch.cuda.ExternalStream(lib.QOPB_stream())
+
+    def solve(v):
+        q.set_opts(prec_sloppy=a.prec, **{a.ab: v})
+        q.dslash(fla, 0.0, hout, hout, QOP_EVEN, QOP_EVEN)
+        ra = QOP_resid_arg_t(a.tol * a.tol, 0, 0, 0, 0, 0)
+        assert q.invert(fla, a.mass, hout, hin, QOP_invert_arg_t(1e9, 200000, 200000, 10, QOP_EVEN), ra).status == 0
+        return ra.final_iter
+
+    for v in (0, 1):
+        solve(v)
+    res = {0: [], 1: []}
+    for rnd in range(a.steps):
+        for v in ((0, 1) if rnd % 2 == 0 else (1, 0)):
+            with Clocks(0) as clk:
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                its = [solve(v) for _ in range(2)]
+                e1.record(stream)
+                e1.synchronize()
+            c = clk.summary()
+            res[v].append({"ms_per_solve": e0.elapsed_time(e1) / 2, "iters": its[0], "sm_mhz": c.get("sm_mhz")})
+    out = {}
+    for v in (0, 1):
+        ms = [r["ms_per_solve"] for r in res[v]]
+        out[str(v)] = {"ms_per_solve_mean": float(np.mean(ms)), "ms_per_solve": ms, "iters": res[v][0]["iters"],
+                       "sm_mhz": [r["sm_mhz"] for r in res[v]]}
+    print(json.dumps({"ab": a.ab, "workload": workload_name(a, L), "rounds": a.steps, "results": out}), flush=True)
+
+
 def run_dd(a):
     """Decomposed lattice.  Links: HISQ smeared on each process's block
     (periodic within the block: synthetic links of the production form),
@@ -1032,6 +1090,8 @@ def main():
         run_small(a)
     elif a.workload == "force":
         run_force(a)
+    elif a.ab:
+        run_ab(a)
     elif a.workload == "dd":
         run_dd(a)
     elif a.workload != "single":
