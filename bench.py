@@ -26,10 +26,10 @@ by the batched int16 solver, compared with the same call in FP64):
   --workload force       HISQ and asqtad fermion forces, 24^3x48, 8 sources
   --workload serve       the solve service (QOPB_serve_*) with HISQ 16^4,
                          24^3x48 and 32^3x64 resident, Poisson arrivals
-  --workload dd          the decomposed lattice: FP64 CG (reference
-                         algorithm) on HISQ 32^3x64; one GPU: directions
+  --workload dd          the decomposed lattice: the int16 mixed solver and
+                         FP64 CG on HISQ 32^3x64; one GPU: directions
                          --dd-mask exchange halos with themselves through
-                         NCCL, timed against the undecomposed solve; N GPUs
+                         NCCL, timed against the undecomposed solves; N GPUs
                          (torchrun): the lattice split over the GPUs
 """
 import argparse
@@ -832,8 +832,9 @@ def run_dd(a):
     """Decomposed lattice.  Links: HISQ smeared on each process's block
     (periodic within the block: synthetic links of the production form),
     made on the undecomposed block lattice and passed node-local to the
-    decomposed one.  One step = one FP64 CG solve (QOP_D3_asqtad_invert,
-    EVEN source, reference algorithm) to |r|/|b| <= --tol.  On one GPU the
+    decomposed one.  One step = one solve (QOP_D3_asqtad_invert, EVEN
+    source) to |r|/|b| <= --tol, with the int16 mixed solver (the value) and
+    with FP64 CG (the reference algorithm).  On one GPU the
     directions of --dd-mask are decomposed with the process as its own
     neighbour (every hop packs, exchanges through NCCL and reads halos) and
     the same solve is timed on the undecomposed lattice; with N processes
@@ -880,11 +881,11 @@ def run_dd(a):
     src[Vb // 2:] = 0
     rsq = a.tol * a.tol
 
-    def measure(label):
+    def measure(label, prec):
         stream = torch.cuda.ExternalStream(lib.QOPB_stream())
         fla = q.create_L_from_raw(fat, lng)
         hin, hout = q.create_V(src), q.create_V(np.zeros_like(src))
-        q.set_opts(prec_sloppy=64, cg=0)
+        q.set_opts(prec_sloppy=prec, cg=0)
 
         def solve():
             q.dslash(fla, 0.0, hout, hout, QOP_EVEN, QOP_EVEN)   # zero initial guess
@@ -913,13 +914,14 @@ def run_dd(a):
         q.destroy_V(hout)
         q.destroy_L(fla)
         hop = {k: {"launches": v[0], "us_per_launch": 1e3 * v[1] / max(v[0], 1)} for k, v in kst.items()
-               if k.startswith("hop_f64")}
-        return {"label": label, "ms_per_solve": ms, "iters": int(np.median(its)), "hop": hop}
+               if k.startswith("hop_")}
+        return {"label": label, "prec_sloppy": prec, "ms_per_solve": ms, "iters": int(np.median(its)), "hop": hop}
 
     runs = []
     if world == 1:
         assert q.init(L) == 0
-        runs.append(measure("undecomposed"))
+        runs.append(measure("undecomposed", 16))
+        runs.append(measure("undecomposed", 64))
         q.finalize()
         uid = q.comm_unique_id()
     else:
@@ -934,22 +936,24 @@ def run_dd(a):
     else:
         assert q.init(L, machsize=P) == 0
     info = q.dd_info()
-    runs.append(measure("decomposed"))
+    runs.append(measure("decomposed", 16))
+    runs.append(measure("decomposed", 64))
     q.finalize()
     q.dd_self_split(0)
     q.comm_finalize()
-    dd = runs[-1]
+    dd = runs[-2]
     value = world * 1e3 / dd["ms_per_solve"] if world > 1 else 1e3 / dd["ms_per_solve"]
     if rank == 0:
-        line = {"metric": "FP64 CG solves/s @%g, decomposed lattice" % a.tol, "value": value, "unit": "solves/s",
+        line = {"metric": "mixed-prec CG solves/s @%g, decomposed lattice" % a.tol, "value": value, "unit": "solves/s",
                 "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": dd["ms_per_solve"],
                 "higher_is_better": True, "scaling": "strong" if world > 1 else "weak", "vs_baseline": None,
-                "dtype": "f64", "data": "synthetic",
+                "dtype": "f32", "data": "synthetic",
                 "config": {"workload": "dd", "lattice": L, "grid": P, "block": B, "mask": info["mask"],
                            "mass": a.mass, "tol": a.tol, "eps": a.eps},
                 "runs": runs}
         if world == 1:
-            line["overhead_vs_undecomposed"] = dd["ms_per_solve"] / runs[0]["ms_per_solve"]
+            line["overhead_vs_undecomposed"] = {"int16": runs[2]["ms_per_solve"] / runs[0]["ms_per_solve"],
+                                                "fp64": runs[3]["ms_per_solve"] / runs[1]["ms_per_solve"]}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()

@@ -11,6 +11,7 @@
 #include "qopb.h"
 #include "dslash.cuh"
 #include "dd.cuh"
+#include "mixed.cuh"
 #include <dlfcn.h>
 #include <nccl.h>
 
@@ -148,7 +149,14 @@ void dd_refuse(const char *what) {
   if (ctx().dd) fail(QOP_FAIL, "%s is not available on a decomposed lattice", what);
 }
 
-int sloppy_prec() { return ctx().dd ? 64 : ctx().opt.sloppy_prec; }
+// on a decomposed lattice only the fused int16 single-mass iteration has
+// halo-reading kernels; every other sloppy form falls back to FP64
+int sloppy_prec() {
+  const Context &c = ctx();
+  if (!c.dd) return c.opt.sloppy_prec;
+  const Options &o = c.opt;
+  return (o.sloppy_prec == 16 && o.half_format == 0 && o.fuse_update && o.hop_kernel >= 20) ? 16 : 64;
+}
 
 void dd_allreduce(double *d, int n) {
   if (!dd_active()) return;
@@ -287,6 +295,34 @@ __global__ void k_dd_pack(const c2<T> *__restrict__ in, const c2<T> *__restrict_
   }
 }
 
+// moves the packed halos: every process posts the same sequence per
+// direction (raw slabs to -mu, up halo from +mu, products to +mu, down halo
+// from -mu), and NCCL matches the sends and receives between two processes
+// in posting order.  rec_raw / rec_prod: bytes per face site and slab.
+static void dd_exchange(Dd &d, int nl, size_t rec_raw, size_t rec_prod) {
+  Context &c = ctx();
+  const int depth = dd_depth(nl), np = dd_nprod(nl);
+  if (d.nccl) {
+    ncheck(g_nccl.GroupStart(), "ncclGroupStart");
+    for (int mu = 0; mu < 4; mu++) {
+      if (!(d.mask >> mu & 1)) continue;
+      const size_t rb = (size_t)depth * d.fh[mu] * rec_raw, pb = (size_t)np * d.fh[mu] * rec_prod;
+      ncheck(g_nccl.Send(d.sraw[mu], rb, ncclUint8, d.nbr[mu][0], g_comm.comm, c.s), "ncclSend");
+      ncheck(g_nccl.Recv(d.gup[mu], rb, ncclUint8, d.nbr[mu][1], g_comm.comm, c.s), "ncclRecv");
+      ncheck(g_nccl.Send(d.sprod[mu], pb, ncclUint8, d.nbr[mu][1], g_comm.comm, c.s), "ncclSend");
+      ncheck(g_nccl.Recv(d.gdn[mu], pb, ncclUint8, d.nbr[mu][0], g_comm.comm, c.s), "ncclRecv");
+    }
+    ncheck(g_nccl.GroupEnd(), "ncclGroupEnd");
+  } else {   // one process without a communicator: it is its own neighbour
+    for (int mu = 0; mu < 4; mu++) {
+      if (!(d.mask >> mu & 1)) continue;
+      const size_t rb = (size_t)depth * d.fh[mu] * rec_raw, pb = (size_t)np * d.fh[mu] * rec_prod;
+      QCHECK(cudaMemcpyAsync(d.gup[mu], d.sraw[mu], rb, cudaMemcpyDeviceToDevice, c.s));
+      QCHECK(cudaMemcpyAsync(d.gdn[mu], d.sprod[mu], pb, cudaMemcpyDeviceToDevice, c.s));
+    }
+  }
+}
+
 template <typename T> DdGhost<T> dd_halo(FlaT<T> *f, const c2<T> *in, int q) {
   Context &c = ctx();
   Dd &d = *c.dd;
@@ -305,28 +341,75 @@ template <typename T> DdGhost<T> dd_halo(FlaT<T> *f, const c2<T> *in, int q) {
     h.up[mu] = (const c2<T> *)d.gup[mu];
     h.dn[mu] = (const c2<T> *)d.gdn[mu];
   }
-  // every process posts the same sequence per direction: raw to -mu, up
-  // halo from +mu, products to +mu, down halo from -mu; NCCL matches the
-  // sends and receives between two processes in posting order
-  if (d.nccl) {
-    ncheck(g_nccl.GroupStart(), "ncclGroupStart");
-    for (int mu = 0; mu < 4; mu++) {
-      if (!(d.mask >> mu & 1)) continue;
-      const size_t rb = (size_t)depth * 3 * d.fh[mu] * sizeof(c2<T>), pb = (size_t)np * 3 * d.fh[mu] * sizeof(c2<T>);
-      ncheck(g_nccl.Send(d.sraw[mu], rb, ncclUint8, d.nbr[mu][0], g_comm.comm, c.s), "ncclSend");
-      ncheck(g_nccl.Recv(d.gup[mu], rb, ncclUint8, d.nbr[mu][1], g_comm.comm, c.s), "ncclRecv");
-      ncheck(g_nccl.Send(d.sprod[mu], pb, ncclUint8, d.nbr[mu][1], g_comm.comm, c.s), "ncclSend");
-      ncheck(g_nccl.Recv(d.gdn[mu], pb, ncclUint8, d.nbr[mu][0], g_comm.comm, c.s), "ncclRecv");
-    }
-    ncheck(g_nccl.GroupEnd(), "ncclGroupEnd");
-  } else {   // one process without a communicator: it is its own neighbour
-    for (int mu = 0; mu < 4; mu++) {
-      if (!(d.mask >> mu & 1)) continue;
-      const size_t rb = (size_t)depth * 3 * d.fh[mu] * sizeof(c2<T>), pb = (size_t)np * 3 * d.fh[mu] * sizeof(c2<T>);
-      QCHECK(cudaMemcpyAsync(d.gup[mu], d.sraw[mu], rb, cudaMemcpyDeviceToDevice, c.s));
-      QCHECK(cudaMemcpyAsync(d.gdn[mu], d.sprod[mu], pb, cudaMemcpyDeviceToDevice, c.s));
-    }
+  dd_exchange(d, nl, sizeof(c2<T>) * 3, sizeof(c2<T>) * 3);
+  return h;
+}
+
+// int16 records: raw slabs copy the records; product slabs decode the
+// record, apply -U^+ with the FP64 forward link and store a new record
+__global__ void k_dd_pack_q16(const uint4 *__restrict__ in, const double2 *__restrict__ lk, Geom g, int mu, int q,
+                              int nl, int fh, uint4 *__restrict__ sraw, uint4 *__restrict__ sprod) {
+  const int depth = dd_depth(nl), np = dd_nprod(nl);
+  const i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x;
+  if (t >= (i64)(depth + np) * fh) return;
+  const int s = (int)(t / fh), fi = (int)(t % fh);
+  int xm, slot = -1;
+  if (s < depth) {
+    xm = s;
+  } else {
+    const int j = s - depth;
+    xm = g.L[mu] - 1 - (j == 0 ? 0 : j - 1);
+    slot = nl == 16 ? (j == 0 ? 4 * mu : 4 * mu + 1) : 2 * mu;
   }
+  int x[4];
+  int rem = 2 * fi;
+  for (int nu = 3; nu >= 0; nu--)
+    if (nu != mu) { x[nu] = rem % g.L[nu]; rem /= g.L[nu]; }
+  x[mu] = xm;
+  if (((x[0] + x[1] + x[2] + x[3]) & 1) != q) x[mu == 3 ? 2 : 3] += 1;
+  const i64 Vh = g.Vh;
+  const int i = site_index(g, x[0], x[1], x[2], x[3]);
+  if (slot < 0) {
+    sraw[(i64)s * fh + fi] = in[i];
+    return;
+  }
+  float2 v[3];
+  SpQ16::load(in, i, Vh, v);
+  const double2 *U = lk + (i64)slot * 9 * Vh + i;
+  float2 o[3];
+#pragma unroll
+  for (int r = 0; r < 3; r++) {   // -(U^+ v)_r = -sum_c conj(U_cr) v_c
+    double ax = 0, ay = 0;
+#pragma unroll
+    for (int cc = 0; cc < 3; cc++) {
+      const double2 u = U[(3 * cc + r) * Vh];
+      ax += u.x * v[cc].x + u.y * v[cc].y;
+      ay += u.x * v[cc].y - u.y * v[cc].x;
+    }
+    o[r] = make_float2((float)-ax, (float)-ay);
+  }
+  SpQ16::store(sprod + (i64)(s - depth) * fh, fi, fh, o);
+}
+
+DdQ16Ghost dd_halo_q16(FlaT<double> *f, const uint4 *in, int q) {
+  Context &c = ctx();
+  Dd &d = *c.dd;
+  const Geom &g = c.g;
+  DdQ16Ghost h{};
+  h.mask = d.mask;
+  const int nl = f->nlinks, depth = dd_depth(nl), np = dd_nprod(nl);
+  const double2 *lk = f->d + (i64)q * nl * 9 * g.Vh;
+  for (int mu = 0; mu < 4; mu++) {
+    h.fh[mu] = d.fh[mu];
+    if (!(d.mask >> mu & 1)) continue;
+    const i64 n = (i64)(depth + np) * d.fh[mu];
+    k_dd_pack_q16<<<grid_for(n, 128), 128, 0, c.s>>>(in, lk, g, mu, q, nl, d.fh[mu], (uint4 *)d.sraw[mu],
+                                                      (uint4 *)d.sprod[mu]);
+    QLAUNCH();
+    h.up[mu] = (const uint4 *)d.gup[mu];
+    h.dn[mu] = (const uint4 *)d.gdn[mu];
+  }
+  dd_exchange(d, nl, sizeof(uint4), sizeof(uint4));
   return h;
 }
 

@@ -27,6 +27,7 @@
 #include "prof.cuh"
 #include "fields.cuh"
 #include "mixed.cuh"
+#include "dd.cuh"
 #include <algorithm>
 #include <map>
 #include <vector>
@@ -527,8 +528,10 @@ __device__ __forceinline__ void q16_epilogue3(uint4 *out, const uint4 *same, con
   }
 }
 
-__device__ __forceinline__ void q16_finish3(double (&acc)[3], double *part, unsigned *count, MixState *st, int seq) {
-  if (grid_sum<3>(acc, part, count, st->red3)) {
+// alpha, the new |r|^2, beta and the reliable-update test from the sums in
+// dp2 and red3 (one thread)
+__device__ __forceinline__ void mix_scalars3(MixState *st, int seq) {
+  {
     if (st->flag != MIX_RUN) return;
     const double pAp = st->dp2 + st->m2 * st->red3[0];
     if (!(pAp > 0)) { st->flag = MIX_BREAK; return; }
@@ -544,6 +547,15 @@ __device__ __forceinline__ void q16_finish3(double (&acc)[3], double *part, unsi
     if (!(rn > 0) || rn < st->delta2 * st->maxr2 || rn <= st->stop || st->iter >= st->max_iter) st->flag = MIX_UPDATE;
   }
 }
+
+// DDQ (decomposed lattice): the sums are summed over the processes first,
+// so the scalars come from k_mix_scalars3 after the all-reduce
+template <bool DDQ>
+__device__ __forceinline__ void q16_finish3(double (&acc)[3], double *part, unsigned *count, MixState *st, int seq) {
+  if (grid_sum<3>(acc, part, count, st->red3) && !DDQ) mix_scalars3(st, seq);
+}
+
+__global__ void k_mix_scalars3(MixState *st, int seq) { mix_scalars3(st, seq); }
 
 template <int NL, int KIND, int GRP>
 __global__ void __launch_bounds__(QB)
@@ -726,12 +738,17 @@ k_mix_hop_q16a(uint4 *__restrict__ out, const uint4 *__restrict__ src, const uns
 
 // PERSIST: a grid of (SMs x MINB) blocks strides over the site blocks, so
 // no partial last wave of blocks leaves SMs idle
-// PK: packed FP32x2 arithmetic (q16_slot_pk)
-template <int NL, int KIND, int BATCH, bool RECON, int MINB = 1, bool PERSIST = false, bool PK = false>
+// PK: packed FP32x2 arithmetic (q16_slot_pk).  DDQ (with PK, decomposed
+// lattice): a neighbour outside the block comes from the halos of gh (an
+// up record multiplies the link as usual; a down record is the product
+// -U^+ psi and is added as is)
+template <int NL, int KIND, int BATCH, bool RECON, int MINB = 1, bool PERSIST = false, bool PK = false,
+          bool DDQ = false>
 __global__ void __launch_bounds__(QB, MINB)
 k_mix_hop_q16r(uint4 *__restrict__ out, const uint4 *__restrict__ src, const unsigned char *__restrict__ lk,
                const uint4 *__restrict__ same, Geom g, NbrGeom ng, int p, MixState *st, double *part,
-               unsigned *count, float c_long, const uint4 *__restrict__ rres = nullptr, int seq = 0) {
+               unsigned *count, float c_long, const uint4 *__restrict__ rres = nullptr, int seq = 0,
+               DdQ16Ghost gh = DdQ16Ghost()) {
   if (st->flag) return;
   const int tid = threadIdx.x;
   const i64 Vh = g.Vh;
@@ -753,9 +770,11 @@ k_mix_hop_q16r(uint4 *__restrict__ out, const uint4 *__restrict__ src, const uns
     for (int k0 = 0; k0 < NL; k0 += BATCH) {
       uint4 ua[BATCH], ub[BATCH], nb[BATCH];
       uint2 uc[BATCH];
+      bool prd[BATCH];
 #pragma unroll
       for (int s = 0; s < BATCH; s++) {
         const int k = k0 + s;
+        prd[s] = false;
         const unsigned char *ls = gl + q16_slot_off(k, RECON);
         ua[s] = __ldcs(reinterpret_cast<const uint4 *>(ls) + tid);
         if (RECON && (k & 1)) {
@@ -766,10 +785,28 @@ k_mix_hop_q16r(uint4 *__restrict__ out, const uint4 *__restrict__ src, const uns
           ub[s] = __ldcs(reinterpret_cast<const uint4 *>(ls + 16 * QB) + tid);
           uc[s] = __ldcs(reinterpret_cast<const uint2 *>(ls + 32 * QB) + tid);
         }
-        nb[s] = src[nbr_fast(ng, x, lex, slot_mu<NL>(k), slot_disp<NL>(k))];
+        const int mu = slot_mu<NL>(k), dsp = slot_disp<NL>(k);
+        if (DDQ && (gh.mask >> mu & 1) && (unsigned)(x[mu] + dsp) >= (unsigned)g.L[mu]) {
+          const int y = x[mu] + dsp, fh = gh.fh[mu], fi = dd_face_index(g, x, mu);
+          if (y < 0) {
+            nb[s] = gh.dn[mu][(i64)(dsp == -1 ? 0 : -y) * fh + fi];
+            prd[s] = true;
+          } else {
+            nb[s] = gh.up[mu][(i64)(y - g.L[mu]) * fh + fi];
+          }
+        } else {
+          nb[s] = src[nbr_fast(ng, x, lex, mu, dsp)];
+        }
       }
 #pragma unroll
       for (int s = 0; s < BATCH; s++) {
+        if (DDQ && prd[s]) {   // a = (t.x - s.y, t.y + s.x): the product enters t
+          float2 z[3];
+          SpQ16::load(&nb[s], 0, 0, z);
+#pragma unroll
+          for (int r = 0; r < 3; r++) { pt[r].x += z[r].x; pt[r].y += z[r].y; }
+          continue;
+        }
         if (PK) {
           if (RECON && ((k0 + s) & 1))
             q16_slot_recon_pk(ua[s], make_uint2(ub[s].x, ub[s].y), __uint_as_float(uc[s].x), nb[s], c_long, pt, ps);
@@ -787,7 +824,7 @@ k_mix_hop_q16r(uint4 *__restrict__ out, const uint4 *__restrict__ src, const uns
     else acc1[0] += q16_epilogue<KIND>(out, same, i, Vh, (float)st->m2, a);
   }
   } while (PERSIST && (sb += gridDim.x) < nsb);
-  if constexpr (KIND == 3) q16_finish3(acc1, part, count, st, seq);
+  if constexpr (KIND == 3) q16_finish3<DDQ>(acc1, part, count, st, seq);
   else q16_finish<KIND>(acc1, part, count, st);
 }
 
@@ -892,6 +929,26 @@ LinksSloppy links_parity(SloppyLinks *s, int lkfmt, int p) {
 // default), 110.0 with 23, 111.2 with 20 / 21, 112-113 with 22, 24, 26,
 // against 117.3 for the scalar variant 15 (a third fewer instructions per
 // slot; the kernel was issue-bound at 62 % issue-active).
+// decomposed lattice: the hop of variant 25 (4 slots, 5 blocks per SM,
+// persistent, packed) reading the halos of gh; KIND 1 or 3
+static void launch_q16_dd(int kind, int nl, bool recon, float c_long, int grid, uint4 *out, const uint4 *src,
+                          const unsigned char *lk, const uint4 *same, const Geom &g, const NbrGeom &ng, int par,
+                          MixState *st, const uint4 *rres, int seq, const DdQ16Ghost &gh) {
+  Context &c = ctx();
+  const int gp = std::min(grid, (c.red_blocks / 8) * 5);
+#define QDD_ARGS out, src, lk, same, g, ng, par, st, c.d_part, c.d_count, c_long, rres, seq, gh
+#define QDD(K)                                                                                              \
+  do {                                                                                                      \
+    if (nl != 16) k_mix_hop_q16r<8, K, 4, false, 5, true, true, true><<<gp, QB, 0, c.s>>>(QDD_ARGS);        \
+    else if (recon) k_mix_hop_q16r<16, K, 4, true, 5, true, true, true><<<gp, QB, 0, c.s>>>(QDD_ARGS);      \
+    else k_mix_hop_q16r<16, K, 4, false, 5, true, true, true><<<gp, QB, 0, c.s>>>(QDD_ARGS);                \
+  } while (0)
+  if (kind == 1) QDD(1);
+  else QDD(3);
+#undef QDD
+#undef QDD_ARGS
+}
+
 // KIND 3 hops (fused update) exist for the persistent packed variants 20-26
 static void launch_q16_fused(int variant, int nl, bool recon, float c_long, int grid, uint4 *out, const uint4 *src,
                              const unsigned char *lk, const uint4 *same, const Geom &g, const NbrGeom &ng, int par,
@@ -1106,11 +1163,42 @@ static void run_mixed(LinOp<double> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t *r
   constexpr bool q16v = std::is_same<Lk, LkQ16B>::value && std::is_same<Sp, SpQ16>::value;
   const bool fuse = q16v && ns == 1 && c.opt.fuse_update && c.opt.hop_kernel >= 20;
   int seq = 0;
+  // a decomposed lattice: halos before each hop, the reductions summed over
+  // the processes before the scalars (the fused int16 iteration only)
+  const bool ddq = dd_active();
+  if (ddq && !fuse) {
+    release();
+    fail(QOP_FAIL, "mixed solver on a decomposed lattice: needs int16 storage, one mass, fuse_update and a "
+                   "packed hop variant (20-26)");
+  }
   while (true) {
     const int it0 = h.iter;
     int prof0 = -1;
     std::vector<int> recs;
     for (int k = 0; k < chunk; k++) {
+      if constexpr (q16v) {
+        if (ddq) {
+          const unsigned char *lq = (const unsigned char *)lk_q.a, *lp = (const unsigned char *)lk_p.a;
+          {
+            ProfScope ps1(hname, hop_bytes);
+            const DdQ16Ghost g1 = dd_halo_q16(L.f, ps, p);
+            launch_q16_dd(1, nl, recon, c_long, gridq, ts, ps, lq, nullptr, g, ng, q, dst, nullptr, 0, g1);
+            recs.push_back(ps1.idx);
+          }
+          dd_allreduce(&dst->dp2, 1);
+          {
+            ProfScope ps2(hname3, hop_bytes + (double)Vh * Sp::site_bytes * 2);
+            const DdQ16Ghost g2 = dd_halo_q16(L.f, ts, q);
+            launch_q16_dd(3, nl, recon, c_long, gridq, Aps, ts, lp, ps, g, ng, p, dst, rs, ++seq, g2);
+            recs.push_back(ps2.idx);
+          }
+          dd_allreduce(dst->red3, 3);
+          k_mix_scalars3<<<1, 1, 0, c.s>>>(dst, seq);
+          k_mix_update_p<Sp><<<gridv, 256, 0, c.s>>>(xs, rs, ps, Aps, Vh, dst, seq);
+          QLAUNCHN(4);
+          continue;
+        }
+      }
       {
         ProfScope ps1(hname, hop_bytes);
         if constexpr (std::is_same<Lk, LkQ16B>::value) {

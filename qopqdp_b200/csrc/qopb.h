@@ -166,8 +166,8 @@ int dd_node_number(const int x[4]);
 long dd_node_index(const int x[4]);
 // entry points without a decomposed form refuse with QOP_FAIL
 void dd_refuse(const char *what);
-// the sloppy precision the solvers use (64 on a decomposed lattice: the
-// 16- and 32-bit sloppy kernels are single-domain)
+// the sloppy precision the solvers use (on a decomposed lattice 16 only for
+// the fused int16 single-mass iteration, whose kernels read halos; else 64)
 int sloppy_prec();
 
 // every handle remembers the lattice it was created on; entry points refuse

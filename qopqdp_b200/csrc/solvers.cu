@@ -310,7 +310,7 @@ void solve_multi(QOP_info_t *info, FlaT<T> *f, QOP_invert_arg_t *ia, QOP_resid_a
     return;
   }
   if constexpr (std::is_same<T, double>::value) {
-    if (sloppy_prec() < 64 && nsolve > 1) {
+    if (sloppy_prec() < 64 && nsolve > 1 && !ctx().dd) {   // batched solver: single block only
       solve_multi_mixed(info, f, ia, ra, masses, out, in, nsolve);
       return;
     }

@@ -15,7 +15,7 @@ import pytest
 import conftest
 import oracle as O
 from conftest import gpu_lattice
-from helpers import asqtad_links, full_residual, rel_norm_err, site_rel_err
+from helpers import asqtad_links, eo_residual, full_residual, half, rel_norm_err, site_rel_err
 from qopqdp_b200 import lattice as LT
 from qopqdp_b200.qop import QOP_EVEN, QOP_EVENODD, QOP_ODD, QOP_invert_arg_t, QOP_resid_arg_t, Qop
 
@@ -148,5 +148,64 @@ def test_decomposed_lattice_refuses_single_domain_entry_points():
         assert q.lib.QOPB_lattice_create((q.lib.QOPB_lattice_create.argtypes[0]._type_ * 4)(*L)) == -1
         assert q.lib.QOPB_serve_start() == -1
         q.destroy_G(G)
+    finally:
+        restore(q)
+
+
+class _KStat(__import__("ctypes").Structure):
+    _fields_ = [("name", __import__("ctypes").c_char * 32), ("launches", __import__("ctypes").c_int),
+                ("total_ms", __import__("ctypes").c_double), ("bytes_per_launch", __import__("ctypes").c_double)]
+
+
+def _prof_classes(q):
+    import ctypes as C
+    q.lib.QOPB_prof_end.argtypes = [C.POINTER(_KStat), C.c_int]
+    buf = (_KStat * 32)()
+    n = q.lib.QOPB_prof_end(buf, 32)
+    return {buf[i].name.decode(): buf[i].launches for i in range(min(n, 32))}
+
+
+@pytest.mark.parametrize("mask,comm", [(15, False), (9, True)])
+def test_int16_mixed_solver_on_decomposed_lattice(mask, comm):
+    """The int16 reliable-update solver (fused iteration, packed hop) on a
+    decomposed lattice: int16 halo records, down-halo products formed with
+    the FP64 links, and the step scalars computed after the all-reduce.  Each
+    solve reaches the FP64 target with the iteration count and solution of
+    the same solve on the undecomposed lattice, and runs the decomposed int16
+    kernels (not an FP64 fallback)."""
+    q = gpu_lattice(L, "D")
+    fat, lng = asqtad_links(L, 0.4, 11)
+    fo = O.Fla(O.Lattice(L), fat, lng)
+
+    def solves():
+        fla = q.create_L_from_raw(fat, lng)
+        assert q.set_opts(prec_sloppy=16, cg=0) == 0
+        out = {}
+        q.lib.QOPB_prof_begin()
+        for eo, m, seed in ((QOP_EVEN, 0.03, 41), (QOP_ODD, 0.01, 42)):
+            src = LT.gaussian_vector(L, seed)
+            hin, hout = q.create_V(src), q.create_V(np.zeros_like(src))
+            ra = QOP_resid_arg_t(1e-20, 0, 0, 0, 0, 0)
+            info = q.invert(fla, m, hout, hin, QOP_invert_arg_t(1e9, 20000, 20000, 5, eo), ra)
+            assert info.status == 0
+            out[eo] = (q.extract_V(hout, V), ra.final_iter, src, m)
+            q.destroy_V(hin)
+            q.destroy_V(hout)
+        out["prof"] = _prof_classes(q)
+        assert q.set_opts(prec_sloppy=64) == 0
+        q.destroy_L(fla)
+        return out
+
+    base = solves()
+    try:
+        reinit(q, mask, comm)
+        split = solves()
+        assert split["prof"].get("hop_q16_upd_linkq16", 0) > 0, split["prof"]
+        for eo in (QOP_EVEN, QOP_ODD):
+            got, it, src, m = split[eo]
+            want, it0, _, _ = base[eo]
+            assert eo_residual(fo, m, got, src, L, eo) <= 1.05e-20, eo
+            assert abs(it - it0) <= 0.05 * it0 + 3, (eo, it, it0)
+            assert rel_norm_err(half(got, L, eo), half(want, L, eo)) <= 1e-8, eo
     finally:
         restore(q)
