@@ -786,17 +786,18 @@ k_mix_hop_q16r(uint4 *__restrict__ out, const uint4 *__restrict__ src, const uns
           uc[s] = __ldcs(reinterpret_cast<const uint2 *>(ls + 32 * QB) + tid);
         }
         const int mu = slot_mu<NL>(k), dsp = slot_disp<NL>(k);
-        if (DDQ && (gh.mask >> mu & 1) && (unsigned)(x[mu] + dsp) >= (unsigned)g.L[mu]) {
+        const uint4 *np = src + nbr_fast(ng, x, lex, mu, dsp);
+        if (DDQ && (gh.mask >> mu & 1)) {   // uniform over the launch: no divergence here
+          // the halo address is selected, not branched to: every lane issues
+          // one load per slot (each warp of a split x3 row has boundary lanes)
           const int y = x[mu] + dsp, fh = gh.fh[mu], fi = dd_face_index(g, x, mu);
-          if (y < 0) {
-            nb[s] = gh.dn[mu][(i64)(dsp == -1 ? 0 : -y) * fh + fi];
-            prd[s] = true;
-          } else {
-            nb[s] = gh.up[mu][(i64)(y - g.L[mu]) * fh + fi];
-          }
-        } else {
-          nb[s] = src[nbr_fast(ng, x, lex, mu, dsp)];
+          const bool cross = (unsigned)y >= (unsigned)g.L[mu];
+          const uint4 *hp = y < 0 ? gh.dn[mu] + (i64)(dsp == -1 ? 0 : -y) * fh + fi
+                                  : gh.up[mu] + (i64)max(y - g.L[mu], 0) * fh + fi;   // in range when unused
+          np = cross ? hp : np;
+          prd[s] = cross && y < 0;
         }
+        nb[s] = *np;
       }
 #pragma unroll
       for (int s = 0; s < BATCH; s++) {
