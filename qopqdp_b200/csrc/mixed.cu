@@ -766,6 +766,14 @@ k_mix_hop_q16r(uint4 *__restrict__ out, const uint4 *__restrict__ src, const uns
     const int lex = ((x[0] * g.L[1] + x[1]) * g.L[2] + x[2]) * g.L[3] + x[3];
     float2 a[3] = {make_float2(0, 0), make_float2(0, 0), make_float2(0, 0)};
     float2 pt[3] = {make_float2(0, 0), make_float2(0, 0), make_float2(0, 0)}, ps[3] = {pt[0], pt[1], pt[2]};
+    // halo face index per decomposed direction: one per site, shared by the
+    // four slots of that direction
+    int hfi[4] = {0, 0, 0, 0};
+    if constexpr (DDQ) {
+#pragma unroll
+      for (int mu = 0; mu < 4; mu++)
+        if (gh.mask >> mu & 1) hfi[mu] = dd_face_index(g, x, mu);
+    }
 #pragma unroll
     for (int k0 = 0; k0 < NL; k0 += BATCH) {
       uint4 ua[BATCH], ub[BATCH], nb[BATCH];
@@ -790,7 +798,7 @@ k_mix_hop_q16r(uint4 *__restrict__ out, const uint4 *__restrict__ src, const uns
         if (DDQ && (gh.mask >> mu & 1)) {   // uniform over the launch: no divergence here
           // the halo address is selected, not branched to: every lane issues
           // one load per slot (each warp of a split x3 row has boundary lanes)
-          const int y = x[mu] + dsp, fh = gh.fh[mu], fi = dd_face_index(g, x, mu);
+          const int y = x[mu] + dsp, fh = gh.fh[mu], fi = hfi[mu];
           const bool cross = (unsigned)y >= (unsigned)g.L[mu];
           const uint4 *hp = y < 0 ? gh.dn[mu] + (i64)(dsp == -1 ? 0 : -y) * fh + fi
                                   : gh.up[mu] + (i64)max(y - g.L[mu], 0) * fh + fi;   // in range when unused
