@@ -209,3 +209,43 @@ def test_int16_mixed_solver_on_decomposed_lattice(mask, comm):
             assert rel_norm_err(half(got, L, eo), half(want, L, eo)) <= 1e-8, eo
     finally:
         restore(q)
+
+
+def test_eigcg_on_decomposed_lattice():
+    """eigCG (option cg = 1) on a lattice decomposed in all four directions:
+    its operator applications read halos and its inner products are summed
+    over the decomposition, so it accumulates the same low modes as on the
+    undecomposed lattice."""
+    q = gpu_lattice(L, "D")
+    fat, lng = asqtad_links(L, 0.4, 11)
+    fo = O.Fla(O.Lattice(L), fat, lng)
+
+    def run():
+        fla = q.create_L_from_raw(fat, lng)
+        assert q.set_opts(prec_sloppy=64, cg=1, eigcg_nev=6, eigcg_m=30, eigcg_l=120) == 0
+        its = []
+        for s in range(4):
+            src = LT.gaussian_vector(L, 500 + s)
+            src[V // 2:] = 0
+            hin, hout = q.create_V(src), q.create_V(np.zeros_like(src))
+            ra = QOP_resid_arg_t(1e-16, 0, 0, 0, 0, 0)
+            assert q.invert(fla, 0.02, hout, hin, QOP_invert_arg_t(1e9, 5000, 5000, 5, QOP_EVENODD), ra).status == 0
+            got = q.extract_V(hout, V)
+            assert full_residual(fo, 0.02, got, src) <= 1.05e-16
+            its.append(ra.final_iter)
+            q.destroy_V(hin)
+            q.destroy_V(hout)
+        lam = q.eigcg_values(fla, QOP_EVEN)
+        assert q.set_opts(cg=0) == 0
+        q.destroy_L(fla)
+        return its, lam
+
+    its0, lam0 = run()
+    try:
+        reinit(q, 15, False)
+        its1, lam1 = run()
+        assert len(lam1) == len(lam0)
+        assert np.allclose(lam1[:4], lam0[:4], rtol=1e-6, atol=0), (lam0[:4], lam1[:4])
+        assert all(abs(a - b) <= 0.05 * b + 3 for a, b in zip(its1, its0)), (its0, its1)
+    finally:
+        restore(q)
