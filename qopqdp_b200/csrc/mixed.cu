@@ -932,8 +932,10 @@ LinksSloppy links_parity(SloppyLinks *s, int lkfmt, int p) {
 // 17-19 = persistent with a per-thread cp.async ring 3 / 2 / 4 slots ahead
 // (6 / 8 / 5 blocks per SM): 157-170 us, the 4-5 small asynchronous copies
 // per slot and thread cost more issue slots than the latency they hide.
-// 20-26 = persistent with packed FP32x2 arithmetic (q16_slot_pk): 2 slots
-// and 6 / 7 / 8 blocks per SM, 4 slots and 6 / 7 / 5, 8 slots and 6.  At
+// 20-28 = persistent with packed FP32x2 arithmetic (q16_slot_pk): 2 slots
+// and 6 / 7 / 8 blocks per SM, 4 slots and 6 / 7 / 5, 8 slots and 6, 4 and
+// 8 slots with 4 blocks (128 registers; with the fused update the solve
+// takes 1525 / 1536 ms against 1489 ms for 25 on one box).  At
 // 32^3x64: 109.1-109.4 us with 25 (4 slots, 5 blocks, 96 registers; the
 // default), 110.0 with 23, 111.2 with 20 / 21, 112-113 with 22, 24, 26,
 // against 117.3 for the scalar variant 15 (a third fewer instructions per
@@ -978,6 +980,8 @@ static void launch_q16_fused(int variant, int nl, bool recon, float c_long, int 
     case 23: Q16RPK3(4, 6); break;
     case 24: Q16RPK3(4, 7); break;
     case 26: Q16RPK3(8, 6); break;
+    case 27: Q16RPK3(4, 4); break;
+    case 28: Q16RPK3(8, 4); break;
     default: Q16RPK3(4, 5); break;
   }
 #undef Q16RPK3
@@ -1045,6 +1049,8 @@ static void launch_q16(int variant, int nl, bool recon, float c_long, int grid, 
     case 24: Q16RPK(4, 7); break;
     case 25: Q16RPK(4, 5); break;
     case 26: Q16RPK(8, 6); break;
+    case 27: Q16RPK(4, 4); break;
+    case 28: Q16RPK(8, 4); break;
     case 1:
       if (nl == 16) k_mix_hop_q16<16, KIND, 2><<<grid, QB, 4 * QSLOT, c.s>>>(Q16_ARGS);
       else k_mix_hop_q16<8, KIND, 2><<<grid, QB, 4 * QSLOT, c.s>>>(Q16_ARGS);

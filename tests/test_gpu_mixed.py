@@ -236,7 +236,7 @@ def _single_iters(q, fla, src, m, L, eo=0):
 
 
 def test_every_hop_kernel_variant():
-    """Each selectable int16 hop kernel (option hop_kernel 0-26: plain,
+    """Each selectable int16 hop kernel (option hop_kernel 0-28: plain,
     TMA-staged, register-capped, persistent, cp.async-ring and packed
     FP32x2 forms) solves to the FP64 target; the scalar forms share the
     decode and arithmetic order and the packed forms round the scaled site
@@ -248,13 +248,13 @@ def test_every_hop_kernel_variant():
     fla = q.create_L_from_raw(fat, lng)
     src = LT.gaussian_vector(L, 330)
     its = {}
-    for v in range(27):
+    for v in range(29):
         assert q.set_opts(prec_sloppy=16, hop_kernel=v) == 0
         st, it, got = _single_iters(q, fla, src, 0.03, L)
         assert st == 0
         assert eo_residual(fo, 0.03, got, src, L, 0) <= 1.05e-20, v
         its[v] = it
-    assert q.set_opts(hop_kernel=27) != 0                  # out of range
+    assert q.set_opts(hop_kernel=29) != 0                  # out of range
     assert q.set_opts(prec_sloppy=64, hop_kernel=25) == 0
     ref = its[25]
     assert all(abs(i - ref) <= 0.03 * ref + 3 for i in its.values()), its
