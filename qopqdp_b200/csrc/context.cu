@@ -183,7 +183,11 @@ QOP_status_t QOP_init(QOP_layout_t *layout) {
     return QOP_FAIL;
   }
   ensure_partials(g);
-  OPT_CATCH(QOP_FAIL)
+  } catch (Fail &e) {
+    log0(0, "QOP error: %s\n", e.msg.c_str());
+    dd_free();   // a decomposition set up before the failure
+    return QOP_FAIL;
+  }
   c.g = g;
   c.lats.assign(1, g);
   c.lat = 0;

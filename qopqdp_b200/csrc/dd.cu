@@ -209,18 +209,23 @@ bool dd_setup(const QOP_layout_t *layout, Geom &g) {
   }
   g.V = (i64)g.L[0] * g.L[1] * g.L[2] * g.L[3];
   g.Vh = g.V / 2;
-  for (int i = 0; i < 4; i++) {
-    d->fh[i] = (int)(g.V / g.L[i] / 2);
-    if (!(d->mask >> i & 1)) continue;
-    // sized for FP64 and 16 links; one set serves both precisions
-    d->raw_cap[i] = (size_t)dd_depth(16) * 3 * d->fh[i] * sizeof(double2);
-    d->prod_cap[i] = (size_t)dd_nprod(16) * 3 * d->fh[i] * sizeof(double2);
-    QCHECK(cudaMalloc(&d->sraw[i], d->raw_cap[i]));
-    QCHECK(cudaMalloc(&d->gup[i], d->raw_cap[i]));
-    QCHECK(cudaMalloc(&d->sprod[i], d->prod_cap[i]));
-    QCHECK(cudaMalloc(&d->gdn[i], d->prod_cap[i]));
+  c.dd = d;   // owned by the context from here: dd_free releases what was allocated
+  try {
+    for (int i = 0; i < 4; i++) {
+      d->fh[i] = (int)(g.V / g.L[i] / 2);
+      if (!(d->mask >> i & 1)) continue;
+      // sized for FP64 and 16 links; one set serves both precisions
+      d->raw_cap[i] = (size_t)dd_depth(16) * 3 * d->fh[i] * sizeof(double2);
+      d->prod_cap[i] = (size_t)dd_nprod(16) * 3 * d->fh[i] * sizeof(double2);
+      QCHECK(cudaMalloc(&d->sraw[i], d->raw_cap[i]));
+      QCHECK(cudaMalloc(&d->gup[i], d->raw_cap[i]));
+      QCHECK(cudaMalloc(&d->sprod[i], d->prod_cap[i]));
+      QCHECK(cudaMalloc(&d->gdn[i], d->prod_cap[i]));
+    }
+  } catch (...) {
+    dd_free();
+    throw;
   }
-  c.dd = d;
   return true;
 }
 
