@@ -260,13 +260,49 @@ long dd_node_index(const int x[4]) {
 // input at x_mu = s (for the -mu neighbour's up halo); product slab 0 holds
 // -F_mu^+ psi at x_mu = L-1 and slab 1 + j holds -N_mu^+ psi at x_mu = L-1-j
 // (for the +mu neighbour's down halo)
+// one pack launch for every decomposed direction: entry j covers the
+// threads [start[j], start[j+1]) of direction mu[j]
+struct DdPackPlan {
+  int n;
+  int mu[4], fh[4];
+  i64 start[5];
+  void *sraw[4], *sprod[4];
+};
+
+static DdPackPlan dd_plan(const Dd &d, int nl) {
+  DdPackPlan pl{};
+  const int per = dd_depth(nl) + dd_nprod(nl);
+  for (int mu = 0; mu < 4; mu++) {
+    if (!(d.mask >> mu & 1)) continue;
+    pl.mu[pl.n] = mu;
+    pl.fh[pl.n] = d.fh[mu];
+    pl.sraw[pl.n] = d.sraw[mu];
+    pl.sprod[pl.n] = d.sprod[mu];
+    pl.start[pl.n + 1] = pl.start[pl.n] + (i64)per * d.fh[mu];
+    pl.n++;
+  }
+  return pl;
+}
+
+// the plan entry and slab coordinates of thread t (false past the end)
+__device__ __forceinline__ bool dd_plan_entry(const DdPackPlan &pl, i64 t, int &j, int &s, int &fi) {
+  if (t >= pl.start[pl.n]) return false;
+  j = 0;
+  while (j + 1 < pl.n && t >= pl.start[j + 1]) j++;
+  const i64 l = t - pl.start[j];
+  s = (int)(l / pl.fh[j]);
+  fi = (int)(l % pl.fh[j]);
+  return true;
+}
+
 template <typename T>
-__global__ void k_dd_pack(const c2<T> *__restrict__ in, const c2<T> *__restrict__ lk, Geom g, int mu, int q, int nl,
-                          int fh, c2<T> *__restrict__ sraw, c2<T> *__restrict__ sprod) {
-  const int depth = dd_depth(nl), np = dd_nprod(nl);
-  const i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x;
-  if (t >= (i64)(depth + np) * fh) return;
-  const int s = (int)(t / fh), fi = (int)(t % fh);
+__global__ void k_dd_pack(const c2<T> *__restrict__ in, const c2<T> *__restrict__ lk, Geom g, int q, int nl,
+                          DdPackPlan pl) {
+  const int depth = dd_depth(nl);
+  int j, s, fi;
+  if (!dd_plan_entry(pl, blockIdx.x * (i64)blockDim.x + threadIdx.x, j, s, fi)) return;
+  const int mu = pl.mu[j], fh = pl.fh[j];
+  c2<T> *sraw = (c2<T> *)pl.sraw[j], *sprod = (c2<T> *)pl.sprod[j];
   int xm, slot = -1;
   if (s < depth) {
     xm = s;
@@ -334,30 +370,29 @@ template <typename T> DdGhost<T> dd_halo(FlaT<T> *f, const c2<T> *in, int q) {
   const Geom &g = c.g;
   DdGhost<T> h{};
   h.mask = d.mask;
-  const int nl = f->nlinks, depth = dd_depth(nl), np = dd_nprod(nl);
+  const int nl = f->nlinks;
   const c2<T> *lk = f->d + (i64)q * nl * 9 * g.Vh;
   for (int mu = 0; mu < 4; mu++) {
     h.fh[mu] = d.fh[mu];
-    if (!(d.mask >> mu & 1)) continue;
-    const i64 n = (i64)(depth + np) * d.fh[mu];
-    k_dd_pack<T><<<grid_for(n, 128), 128, 0, c.s>>>(in, lk, g, mu, q, nl, d.fh[mu], (c2<T> *)d.sraw[mu],
-                                                     (c2<T> *)d.sprod[mu]);
-    QLAUNCH();
     h.up[mu] = (const c2<T> *)d.gup[mu];
     h.dn[mu] = (const c2<T> *)d.gdn[mu];
   }
+  const DdPackPlan pl = dd_plan(d, nl);
+  k_dd_pack<T><<<grid_for(pl.start[pl.n], 128), 128, 0, c.s>>>(in, lk, g, q, nl, pl);
+  QLAUNCH();
   dd_exchange(d, nl, sizeof(c2<T>) * 3, sizeof(c2<T>) * 3);
   return h;
 }
 
 // int16 records: raw slabs copy the records; product slabs decode the
 // record, apply -U^+ with the FP64 forward link and store a new record
-__global__ void k_dd_pack_q16(const uint4 *__restrict__ in, const double2 *__restrict__ lk, Geom g, int mu, int q,
-                              int nl, int fh, uint4 *__restrict__ sraw, uint4 *__restrict__ sprod) {
-  const int depth = dd_depth(nl), np = dd_nprod(nl);
-  const i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x;
-  if (t >= (i64)(depth + np) * fh) return;
-  const int s = (int)(t / fh), fi = (int)(t % fh);
+__global__ void k_dd_pack_q16(const uint4 *__restrict__ in, const double2 *__restrict__ lk, Geom g, int q, int nl,
+                              DdPackPlan pl) {
+  const int depth = dd_depth(nl);
+  int j, s, fi;
+  if (!dd_plan_entry(pl, blockIdx.x * (i64)blockDim.x + threadIdx.x, j, s, fi)) return;
+  const int mu = pl.mu[j], fh = pl.fh[j];
+  uint4 *sraw = (uint4 *)pl.sraw[j], *sprod = (uint4 *)pl.sprod[j];
   int xm, slot = -1;
   if (s < depth) {
     xm = s;
@@ -402,18 +437,16 @@ DdQ16Ghost dd_halo_q16(FlaT<double> *f, const uint4 *in, int q) {
   const Geom &g = c.g;
   DdQ16Ghost h{};
   h.mask = d.mask;
-  const int nl = f->nlinks, depth = dd_depth(nl), np = dd_nprod(nl);
+  const int nl = f->nlinks;
   const double2 *lk = f->d + (i64)q * nl * 9 * g.Vh;
   for (int mu = 0; mu < 4; mu++) {
     h.fh[mu] = d.fh[mu];
-    if (!(d.mask >> mu & 1)) continue;
-    const i64 n = (i64)(depth + np) * d.fh[mu];
-    k_dd_pack_q16<<<grid_for(n, 128), 128, 0, c.s>>>(in, lk, g, mu, q, nl, d.fh[mu], (uint4 *)d.sraw[mu],
-                                                      (uint4 *)d.sprod[mu]);
-    QLAUNCH();
     h.up[mu] = (const uint4 *)d.gup[mu];
     h.dn[mu] = (const uint4 *)d.gdn[mu];
   }
+  const DdPackPlan pl = dd_plan(d, nl);
+  k_dd_pack_q16<<<grid_for(pl.start[pl.n], 128), 128, 0, c.s>>>(in, lk, g, q, nl, pl);
+  QLAUNCH();
   dd_exchange(d, nl, sizeof(uint4), sizeof(uint4));
   return h;
 }
