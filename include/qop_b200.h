@@ -29,6 +29,11 @@ typedef struct {
 } QOPB_kstat_t;
 int QOPB_prof_begin(void);
 int QOPB_prof_end(QOPB_kstat_t *out, int max);
+/* Bracket only launches 0, n, 2n, ... of each kernel class (n >= 1; 1, the
+   default, brackets every launch).  Each pair of event records costs the
+   stream a few microseconds, so sampling keeps long timed regions close to
+   their unprofiled speed.  Returns 0, or -1 for n < 1. */
+int QOPB_prof_every(int n);
 
 /* Number of kernels the library has launched since it was loaded. */
 unsigned long long QOPB_launch_count(void);

@@ -8,7 +8,7 @@
 namespace qopb {
 
 namespace {
-struct Cls { std::string name; double bytes = 0; int launches = 0; double ms = 0; };
+struct Cls { std::string name; double bytes = 0; int launches = 0; double ms = 0; long seen = 0; };
 struct Rec { int cls; cudaEvent_t a, b; double bytes; };
 struct Prof {
   bool active = false;
@@ -16,6 +16,7 @@ struct Prof {
   std::vector<cudaEvent_t> pool;   // free events
   std::vector<Rec> recs;
   size_t cap = 1 << 16;            // at most this many recorded launches
+  int every = 1;                   // bracket every `every`-th launch of a class
 };
 Prof g_prof;
 
@@ -43,6 +44,7 @@ int prof_start(const char *name, double bytes) {
     g_prof.cls.push_back(Cls{name});
     c = (int)g_prof.cls.size() - 1;
   }
+  if (g_prof.cls[c].seen++ % g_prof.every != 0) return -1;
   cudaEvent_t a = take_event(), b = take_event();
   if (!a || !b) return -1;
   cudaEventRecord(a, ctx().s);
@@ -81,6 +83,12 @@ extern "C" int QOPB_prof_begin(void) {
   g_prof.recs.clear();
   g_prof.cls.clear();
   g_prof.active = true;
+  return 0;
+}
+
+extern "C" int QOPB_prof_every(int n) {
+  if (n < 1) return -1;
+  g_prof.every = n;
   return 0;
 }
 
