@@ -144,3 +144,43 @@ def test_raw_roundtrip_keeps_other_parity():
     q.extract_V(h, V, 1, into=out)             # only the odd half is written
     assert np.array_equal(out[: V // 2], b[: V // 2])
     q.destroy_V(h)
+
+
+def test_profiler_samples_every_nth_launch():
+    """QOPB_prof_every(n) brackets launches 0, n, 2n, ... of each kernel
+    class with CUDA events (1, the default, brackets every launch; n < 1 is
+    refused); the per-class counts follow, and every sampled class has a
+    positive device time."""
+    import ctypes as C
+
+    class KStat(C.Structure):
+        _fields_ = [("name", C.c_char * 32), ("launches", C.c_int), ("total_ms", C.c_double),
+                    ("bytes_per_launch", C.c_double)]
+
+    L = (4, 4, 4, 4)
+    q, fla, _ = setup(L, "D")
+    src = LT.gaussian_vector(L, 3)
+    hin, hout = q.create_V(src), q.create_V(np.zeros_like(src))
+    q.lib.QOPB_prof_end.argtypes = [C.POINTER(KStat), C.c_int]
+
+    def classes(every, calls):
+        assert q.lib.QOPB_prof_every(every) == 0
+        q.lib.QOPB_prof_begin()
+        for _ in range(calls):
+            q.dslash(fla, 0.1, hout, hin, 1, 0)
+        buf = (KStat * 32)()
+        n = q.lib.QOPB_prof_end(buf, 32)
+        return {buf[i].name.decode(): (buf[i].launches, buf[i].total_ms) for i in range(min(n, 32))}
+
+    try:
+        assert q.lib.QOPB_prof_every(0) == -1
+        full, samp = classes(1, 10), classes(4, 10)
+    finally:
+        q.lib.QOPB_prof_every(1)
+        q.destroy_V(hin)
+        q.destroy_V(hout)
+        q.destroy_L(fla)
+    assert full and set(full) == set(samp)
+    for name, (n, ms) in full.items():
+        assert n >= 10 and n % 10 == 0 and ms > 0, (name, n, ms)
+        assert samp[name][0] == -(-n // 4) and samp[name][1] > 0, (name, n, samp[name])
