@@ -348,156 +348,284 @@ static void launch_bhop(int variant, int nl, bool recon, int ngrp, int nsb, uint
 #undef BH_CALL
 }
 
-void run_batch(FlaT<double> *f, int eo, int n, const double *mass, c2<double> **x, c2<double> *const *b,
-               const double *rsqmin, int max_iter, int *iters, double *final_rsq) {
+struct BatchEngine::Impl {
+  FlaT<double> *f;
+  int lat, eo, cap;
+  i64 Vh;
+  Range is;
+  NbrGeom ng;
+  int nsb, gridv;
+  uint4 *rs = nullptr, *ps = nullptr, *Aps = nullptr, *ts = nullptr;
+  float2 *xs = nullptr;
+  c2<double> *r = nullptr, *Ax = nullptr, *tmp = nullptr;
+  double *part = nullptr;
+  unsigned *count = nullptr;
+  MixState *dst = nullptr;
+  std::vector<MixState> h;   // host copy of the per-slot solver state
+  struct Sys {
+    bool busy = false;
+    c2<double> *x = nullptr;
+    const c2<double> *b = nullptr;
+    double mass = 0, b2 = 0, r2 = 0;
+    int nru = 0, stalls = 0, last_iter = 0;
+  };
+  std::vector<Sys> sys;
+  std::vector<int> done_now;   // started at their target: reported by the next step
+  static size_t npart(int cap, int nsb, int gridv) {
+    // k_bhop: (groups x BG <= cap + 15) x site blocks; k_bupdate: cap x gridv
+    return std::max<size_t>((size_t)(cap + 15) * nsb, (size_t)cap * gridv);
+  }
+  void release_all() {
+    dfree(rs); dfree(ps); dfree(Aps); dfree(ts); dfree(xs); dfree(r); dfree(Ax); dfree(tmp);
+    dfree(part); dfree(count); dfree(dst);
+  }
+  void check_current() const {
+    if (ctx().lat != lat) fail(QOP_FAIL, "batched solver: its lattice %d is not the current one", lat);
+  }
+  // FP64 true residual b_j - A_j x_j into r; returns its norm^2
+  double true_resid(int j) {
+    LinOp<double> L{f, sys[j].mass, eo, tmp};
+    L.d2(Ax, sys[j].x);
+    Blas<double>::axpby(r, 1.0, sys[j].b, -1.0, Ax, is);
+    return Blas<double>::norm2(r, is);
+  }
+};
+
+size_t BatchEngine::bytes(const Geom &g, int cap) {
+  const int nsb = (int)((g.Vh + QB - 1) / QB), gridv = grid_for(g.Vh, 256);
+  return (size_t)cap * g.Vh * (4 * sizeof(uint4) + 3 * sizeof(float2)) + 3 * sizeof(c2<double>) * vec_elems(g) +
+         sizeof(double) * Impl::npart(cap, nsb, gridv) + (sizeof(unsigned) + sizeof(MixState)) * cap;
+}
+
+BatchEngine::BatchEngine(FlaT<double> *f, int eo, int cap) : d(new Impl()) {
+  Impl &e = *d;
   Context &c = ctx();
   const Geom &g = c.g;
-  const i64 Vh = g.Vh;
-  const int p = eo, q = 1 - eo;
-  const Range is = vrange(g, eo);
-  if (n < 1) return;
-  if (n > BATCH_MAX) fail(QOP_FAIL, "run_batch: %d systems exceed the batch limit %d", n, BATCH_MAX);
-  SloppyLinks *sl = sloppy_get(f, LK_Q16);
+  if (cap < 1 || cap > BATCH_MAX) {
+    delete d;
+    fail(QOP_FAIL, "batched solver: %d slots (1..%d)", cap, BATCH_MAX);
+  }
+  e.f = f;
+  e.lat = c.lat;
+  e.eo = eo;
+  e.cap = cap;
+  e.Vh = g.Vh;
+  e.is = vrange(g, eo);
+  for (int k = 0; k < 4; k++) e.ng.L[k] = g.L[k];
+  e.ng.str[3] = 1; e.ng.str[2] = g.L[3]; e.ng.str[1] = g.L[2] * g.L[3]; e.ng.str[0] = g.L[1] * g.L[2] * g.L[3];
+  e.nsb = (int)((e.Vh + QB - 1) / QB);
+  e.gridv = grid_for(e.Vh, 256);
+  e.h.assign(cap, MixState{});
+  for (auto &s : e.h) s.flag = MIX_DONE;   // free slots are skipped by every kernel
+  e.sys.assign(cap, Impl::Sys{});
+  try {
+    sloppy_get(f, LK_Q16);   // the int16 link copy, built on first use
+    const i64 Vh = e.Vh;
+    e.rs = dalloc<uint4>(cap * Vh);
+    e.ps = dalloc<uint4>(cap * Vh);
+    e.Aps = dalloc<uint4>(cap * Vh);
+    e.ts = dalloc<uint4>(cap * Vh);
+    e.xs = dalloc<float2>(3 * cap * Vh);
+    dzero(e.xs, sizeof(float2) * 3 * cap * Vh);
+    e.r = dalloc<c2<double>>(vec_elems(g));
+    e.Ax = dalloc<c2<double>>(vec_elems(g));
+    e.tmp = dalloc<c2<double>>(vec_elems(g));
+    e.part = dalloc<double>(Impl::npart(cap, e.nsb, e.gridv));
+    e.count = dalloc<unsigned>(cap);
+    dzero(e.count, sizeof(unsigned) * cap);
+    e.dst = dalloc<MixState>(cap);
+  } catch (...) {
+    e.release_all();
+    delete d;
+    throw;
+  }
+}
+
+BatchEngine::~BatchEngine() {
+  d->release_all();
+  delete d;
+}
+
+int BatchEngine::cap() const { return d->cap; }
+int BatchEngine::busy() const {
+  int n = 0;
+  for (const auto &y : d->sys) n += y.busy;
+  return n;
+}
+int BatchEngine::running() const {
+  int n = 0;
+  for (int j = 0; j < d->cap; j++) n += d->sys[j].busy && d->h[j].flag != MIX_DONE;
+  return n;
+}
+int BatchEngine::free_slot() const {
+  for (int j = 0; j < d->cap; j++)
+    if (!d->sys[j].busy) return j;
+  return -1;
+}
+int BatchEngine::iters(int s) const { return d->h[s].iter + d->sys[s].nru; }
+double BatchEngine::final_rsq(int s) const { return d->sys[s].b2 > 0 ? d->sys[s].r2 / d->sys[s].b2 : 0.0; }
+
+void BatchEngine::release(int s) {
+  if (s < 0 || s >= d->cap) return;
+  d->sys[s] = Impl::Sys{};
+  d->h[s] = MixState{};
+  d->h[s].flag = MIX_DONE;
+}
+
+void BatchEngine::start(int s, c2<double> *x, const c2<double> *b, double mass, double rsqmin, int max_iter,
+                        bool x_zero) {
+  Impl &e = *d;
+  Context &c = ctx();
+  e.check_current();
+  if (s < 0 || s >= e.cap || e.sys[s].busy) fail(QOP_FAIL, "batched solver: slot %d is not free", s);
+  const i64 Vh = e.Vh;
+  Impl::Sys &y = e.sys[s];
+  y = Impl::Sys{};
+  y.busy = true;
+  y.x = x;
+  y.b = b;
+  y.mass = mass;
+  MixState &st = e.h[s];
+  st = MixState{};
+  y.b2 = Blas<double>::norm2(b, e.is);
+  st.stop = rsqmin * y.b2;
+  st.delta2 = c.opt.ru_delta * c.opt.ru_delta;
+  st.m2 = mass * mass;
+  st.max_iter = max_iter;
+  if (y.b2 == 0.0 || x_zero) Blas<double>::zero(x, e.is);
+  y.r2 = y.b2 == 0.0 ? 0.0 : x_zero ? y.b2 : e.true_resid(s);
+  if (y.b2 == 0.0 || y.r2 <= st.stop) {
+    st.flag = MIX_DONE;
+    e.done_now.push_back(s);
+    return;
+  }
+  k_to_sloppy<SpQ16><<<e.gridv, 256, 0, c.s>>>(e.rs + s * Vh, (x_zero ? b : e.r) + e.is.off, Vh);
+  k_copy_elems<uint4><<<grid_for(Vh, 256), 256, 0, c.s>>>(e.ps + s * Vh, e.rs + s * Vh, Vh);
+  QLAUNCHN(2);
+  dzero(e.xs + 3 * s * Vh, sizeof(float2) * 3 * Vh);
+  st.rsq = st.rsq_old = st.maxr2 = y.r2;
+  st.flag = MIX_RUN;
+}
+
+std::vector<int> BatchEngine::step() {
+  Impl &e = *d;
+  Context &c = ctx();
+  e.check_current();
+  const Geom &g = c.g;
+  const i64 Vh = e.Vh;
+  const int eo = e.eo, p = eo, q = 1 - eo;
+  std::vector<int> fin;
+  fin.swap(e.done_now);
+  int n = 0, active = 0;   // launches cover slots 0 .. n-1
+  for (int j = 0; j < e.cap; j++)
+    if (e.sys[j].busy) {
+      n = j + 1;
+      active += e.h[j].flag != MIX_DONE;
+    }
+  if (active == 0) return fin;
+  SloppyLinks *sl = sloppy_get(e.f, LK_Q16);
   const LinksSloppy lk_p = links_parity(sl, LK_Q16, p), lk_q = links_parity(sl, LK_Q16, q);
   // by default 8 systems per thread when they fill whole groups of 8 (16
   // sources at 32^4: 531 us per hop against 574 with 4), else 4 (12 masses
   // at 24^3x48: 1696 ms per call against 1989 ms with groups of 8 and 4)
   const int variant = c.opt.batch_kernel < 0 ? (n % 8 == 0 ? 7 : 1) : std::min(c.opt.batch_kernel, N_BHOP - 1);
   const int BG = kBhop[variant].bg;
-  const int ngrp = (n + BG - 1) / BG, nsb = (int)((Vh + QB - 1) / QB), gridv = grid_for(Vh, 256);
+  const int ngrp = (n + BG - 1) / BG, nsb = e.nsb, gridv = e.gridv;
   const int nl = sl->nl;
   const bool recon = sl->recon != 0;
   const float c_long = (float)sl->c_long;
-  NbrGeom ng;
-  for (int d = 0; d < 4; d++) ng.L[d] = g.L[d];
-  ng.str[3] = 1; ng.str[2] = g.L[3]; ng.str[1] = g.L[2] * g.L[3]; ng.str[0] = g.L[1] * g.L[2] * g.L[3];
-
-  uint4 *rs = dalloc<uint4>(n * Vh), *ps = dalloc<uint4>(n * Vh), *Aps = dalloc<uint4>(n * Vh),
-        *ts = dalloc<uint4>(n * Vh);
-  float2 *xs = dalloc<float2>(3 * n * Vh);
-  dzero(xs, sizeof(float2) * 3 * n * Vh);
-  c2<double> *r = dalloc<c2<double>>(vec_elems(g)), *Ax = dalloc<c2<double>>(vec_elems(g));
-  c2<double> *tmp = dalloc<c2<double>>(vec_elems(g));
-  const size_t npart = std::max<size_t>((size_t)ngrp * nsb * BG, (size_t)n * gridv);
-  double *part = dalloc<double>(npart);
-  const int ncount = std::max(ngrp, n);
-  unsigned *count = dalloc<unsigned>(ncount);
-  dzero(count, sizeof(unsigned) * ncount);
-  MixState *dst = dalloc<MixState>(n);
-  std::vector<MixState> h(n);
-  std::vector<double> b2(n), r2(n);
-  std::vector<int> nru(n, 0), stalls(n, 0), last_iter(n, 0);
-  auto release = [&]() {
-    dfree(rs); dfree(ps); dfree(Aps); dfree(ts); dfree(xs); dfree(r); dfree(Ax); dfree(tmp);
-    dfree(part); dfree(count); dfree(dst);
-  };
-  // FP64 true residual b_j - A_j x_j into r; returns its norm^2
-  auto true_resid = [&](int j) {
-    LinOp<double> L{f, mass[j], eo, tmp};
-    L.d2(Ax, x[j]);
-    Blas<double>::axpby(r, 1.0, b[j], -1.0, Ax, is);
-    return Blas<double>::norm2(r, is);
-  };
-  const double delta2 = c.opt.ru_delta * c.opt.ru_delta;
-  int active = 0;
-  for (int j = 0; j < n; j++) {
-    b2[j] = Blas<double>::norm2(b[j], is);
-    MixState &s = h[j];
-    s = MixState{};
-    s.stop = rsqmin[j] * b2[j];
-    s.delta2 = delta2;
-    s.m2 = mass[j] * mass[j];
-    s.max_iter = max_iter;
-    if (b2[j] == 0.0) Blas<double>::zero(x[j], is);
-    r2[j] = b2[j] == 0.0 ? 0.0 : true_resid(j);
-    if (b2[j] == 0.0 || r2[j] <= s.stop) {
-      s.flag = MIX_DONE;
-      continue;
-    }
-    k_to_sloppy<SpQ16><<<gridv, 256, 0, c.s>>>(rs + j * Vh, r + is.off, Vh);
-    k_copy_elems<uint4><<<grid_for(Vh, 256), 256, 0, c.s>>>(ps + j * Vh, rs + j * Vh, Vh);
-    QLAUNCHN(2);
-    s.rsq = s.rsq_old = s.maxr2 = r2[j];
-    s.flag = MIX_RUN;
-    active++;
-  }
-  QCHECK(cudaMemcpyAsync(dst, h.data(), sizeof(MixState) * n, cudaMemcpyHostToDevice, c.s));
   const int chunk = c.opt.chunk;
   char hname[32];
   snprintf(hname, sizeof hname, "bhop_q16_x%d", n);
   const double link_site = recon ? (nl / 2) * (40.0 + 28.0) : nl * 40.0;
-  while (active > 0) {
-    // compulsory bytes of one hop for the systems running in this chunk
-    const double hop_bytes = (double)Vh * (link_site + 2.0 * 16 * active);
-    std::vector<int> recs;
-    for (int k = 0; k < chunk; k++) {
-      {
-        ProfScope s1(hname, hop_bytes);
-        launch_bhop<1>(variant, nl, recon, ngrp, nsb, ts, ps, (const unsigned char *)lk_q.a, nullptr, g, ng, q, dst, n, part,
-                       count, c_long);
-        recs.push_back(s1.idx);
-      }
-      {
-        ProfScope s2(hname, hop_bytes + (double)Vh * 16 * active);
-        launch_bhop<2>(variant, nl, recon, ngrp, nsb, Aps, ts, (const unsigned char *)lk_p.a, ps, g, ng, p, dst, n, part,
-                       count, c_long);
-        recs.push_back(s2.idx);
-      }
-      k_bupdate<<<dim3(gridv, n), 256, 0, c.s>>>(xs, rs, ps, Aps, Vh, dst, part, count);
-      k_bp<<<dim3(gridv, n), 256, 0, c.s>>>(ps, rs, Vh, dst);
-      QLAUNCHN(4);
+  // compulsory bytes of one hop for the systems running in this chunk
+  const double hop_bytes = (double)Vh * (link_site + 2.0 * 16 * active);
+  QCHECK(cudaMemcpyAsync(e.dst, e.h.data(), sizeof(MixState) * n, cudaMemcpyHostToDevice, c.s));
+  std::vector<int> recs;
+  for (int k = 0; k < chunk; k++) {
+    {
+      ProfScope s1(hname, hop_bytes);
+      launch_bhop<1>(variant, nl, recon, ngrp, nsb, e.ts, e.ps, (const unsigned char *)lk_q.a, nullptr, g, e.ng, q,
+                     e.dst, n, e.part, e.count, c_long);
+      recs.push_back(s1.idx);
     }
-    QCHECK(cudaMemcpyAsync(h.data(), dst, sizeof(MixState) * n, cudaMemcpyDeviceToHost, c.s));
-    sync();
-    // drop timing records of hops that found every system idle
-    int most = 0;
-    for (int j = 0; j < n; j++) most = std::max(most, h[j].iter - last_iter[j] + (h[j].flag == MIX_BREAK ? 1 : 0));
-    for (size_t k = 2 * (size_t)most; k < recs.size(); k++) prof_discard(recs[k]);
-    std::vector<int> pupd;
-    for (int j = 0; j < n; j++) {
-      MixState &s = h[j];
-      const int ran = s.iter - last_iter[j];
-      last_iter[j] = s.iter;
-      if (s.flag != MIX_UPDATE && s.flag != MIX_BREAK) continue;
-      stalls[j] = ran == 0 ? stalls[j] + 1 : 0;   // repeated breakdown without progress
-      // reliable update: fold the sloppy solution into FP64, true residual
-      k_fold_x<<<grid_for(3 * Vh, 256), 256, 0, c.s>>>(x[j] + is.off, xs + 3 * j * Vh, 3 * Vh);
-      QLAUNCH();
-      r2[j] = true_resid(j);
-      nru[j]++;
-      log0(QOP_VERB_MED, "BATCHCG[%d/%d]: iter %d sloppy rsq %g true rsq %g (stop %g)\n", j, n, s.iter, s.rsq, r2[j],
-           s.stop);
-      if (r2[j] <= s.stop || s.iter + nru[j] >= s.max_iter || stalls[j] > 2) {
-        s.flag = MIX_DONE;
-        active--;
-        continue;
-      }
-      const bool broke = s.flag == MIX_BREAK || !(s.rsq_old > 0);
-      const double rsq_prev = s.rsq_old;
-      k_to_sloppy<SpQ16><<<gridv, 256, 0, c.s>>>(rs + j * Vh, r + is.off, Vh);
-      QLAUNCH();
-      s.rsq = r2[j];
-      s.maxr2 = r2[j];
-      s.flag = MIX_RUN;
-      if (broke) {   // restart the recursion from the true residual
-        k_copy_elems<uint4><<<grid_for(Vh, 256), 256, 0, c.s>>>(ps + j * Vh, rs + j * Vh, Vh);
-        QLAUNCH();
-      } else {
-        s.beta = r2[j] / rsq_prev;
-        pupd.push_back(j);
-      }
+    {
+      ProfScope s2(hname, hop_bytes + (double)Vh * 16 * active);
+      launch_bhop<2>(variant, nl, recon, ngrp, nsb, e.Aps, e.ts, (const unsigned char *)lk_p.a, e.ps, g, e.ng, p,
+                     e.dst, n, e.part, e.count, c_long);
+      recs.push_back(s2.idx);
     }
-    QCHECK(cudaMemcpyAsync(dst, h.data(), sizeof(MixState) * n, cudaMemcpyHostToDevice, c.s));
-    for (int j : pupd) {
-      k_bp<<<dim3(gridv, 1), 256, 0, c.s>>>(ps + j * Vh, rs + j * Vh, Vh, dst + j);
-      QLAUNCH();
+    k_bupdate<<<dim3(gridv, n), 256, 0, c.s>>>(e.xs, e.rs, e.ps, e.Aps, Vh, e.dst, e.part, e.count);
+    k_bp<<<dim3(gridv, n), 256, 0, c.s>>>(e.ps, e.rs, Vh, e.dst);
+    QLAUNCHN(4);
+  }
+  std::vector<MixState> &h = e.h;
+  QCHECK(cudaMemcpyAsync(h.data(), e.dst, sizeof(MixState) * n, cudaMemcpyDeviceToHost, c.s));
+  sync();
+  // drop timing records of hops that found every system idle
+  int most = 0;
+  for (int j = 0; j < n; j++)
+    if (e.sys[j].busy) most = std::max(most, h[j].iter - e.sys[j].last_iter + (h[j].flag == MIX_BREAK ? 1 : 0));
+  for (size_t k = 2 * (size_t)most; k < recs.size(); k++) prof_discard(recs[k]);
+  std::vector<int> pupd;
+  for (int j = 0; j < n; j++) {
+    Impl::Sys &y = e.sys[j];
+    MixState &s = h[j];
+    if (!y.busy) continue;
+    const int ran = s.iter - y.last_iter;
+    y.last_iter = s.iter;
+    if (s.flag != MIX_UPDATE && s.flag != MIX_BREAK) continue;
+    y.stalls = ran == 0 ? y.stalls + 1 : 0;   // repeated breakdown without progress
+    // reliable update: fold the sloppy solution into FP64, true residual
+    k_fold_x<<<grid_for(3 * Vh, 256), 256, 0, c.s>>>(y.x + e.is.off, e.xs + 3 * j * Vh, 3 * Vh);
+    QLAUNCH();
+    y.r2 = e.true_resid(j);
+    y.nru++;
+    log0(QOP_VERB_MED, "BATCHCG[%d/%d]: iter %d sloppy rsq %g true rsq %g (stop %g)\n", j, n, s.iter, s.rsq, y.r2,
+         s.stop);
+    if (y.r2 <= s.stop || s.iter + y.nru >= s.max_iter || y.stalls > 2) {
+      s.flag = MIX_DONE;
+      fin.push_back(j);
+      continue;
     }
+    const bool broke = s.flag == MIX_BREAK || !(s.rsq_old > 0);
+    const double rsq_prev = s.rsq_old;
+    k_to_sloppy<SpQ16><<<gridv, 256, 0, c.s>>>(e.rs + j * Vh, e.r + e.is.off, Vh);
+    QLAUNCH();
+    s.rsq = y.r2;
+    s.maxr2 = y.r2;
+    s.flag = MIX_RUN;
+    if (broke) {   // restart the recursion from the true residual
+      k_copy_elems<uint4><<<grid_for(Vh, 256), 256, 0, c.s>>>(e.ps + j * Vh, e.rs + j * Vh, Vh);
+      QLAUNCH();
+    } else {
+      s.beta = y.r2 / rsq_prev;
+      pupd.push_back(j);
+    }
+  }
+  QCHECK(cudaMemcpyAsync(e.dst, h.data(), sizeof(MixState) * n, cudaMemcpyHostToDevice, c.s));
+  for (int j : pupd) {
+    k_bp<<<dim3(gridv, 1), 256, 0, c.s>>>(e.ps + j * Vh, e.rs + j * Vh, Vh, e.dst + j);
+    QLAUNCH();
+  }
+  return fin;
+}
+
+void run_batch(FlaT<double> *f, int eo, int n, const double *mass, c2<double> **x, c2<double> *const *b,
+               const double *rsqmin, int max_iter, int *iters, double *final_rsq) {
+  if (n < 1) return;
+  if (n > BATCH_MAX) fail(QOP_FAIL, "run_batch: %d systems exceed the batch limit %d", n, BATCH_MAX);
+  BatchEngine e(f, eo, n);
+  for (int j = 0; j < n; j++) e.start(j, x[j], b[j], mass[j], rsqmin[j], max_iter, false);
+  for (int left = n; left > 0;) {
+    const int k = (int)e.step().size();
+    if (k == 0 && e.running() == 0) break;
+    left -= k;
   }
   for (int j = 0; j < n; j++) {
-    iters[j] = h[j].iter + nru[j];
-    final_rsq[j] = b2[j] > 0 ? r2[j] / b2[j] : 0.0;
+    iters[j] = e.iters(j);
+    final_rsq[j] = e.final_rsq(j);
   }
-  release();
   sync();
 }
 

@@ -1,22 +1,35 @@
 // serve.cu -- solve service (B200 addition, no counterpart in the
-// reference): callers queue requests, one worker thread groups the systems
-// of requests on the same link handle and parity into batched
-// mixed-precision solves (batch.cu, up to BATCH_MAX systems) and writes the
-// results back in the QOP raw layout with the QOP_asqtad_invert
-// normalisation (m A^-1 b).
+// reference) with continuous batching: callers queue requests; one worker
+// thread keeps a batched mixed-precision solver (BatchEngine, batch.cu: 16
+// slots) per link handle and parity in flight and admits the systems of a
+// queued request into free slots between solver steps, so a request that
+// arrives while others are on the GPU joins their hop launches at once
+// instead of waiting for their batch to finish.  A step advances every
+// running system of one engine by a chunk of iterations plus its reliable
+// updates; the worker steps the engines in turn, so requests on different
+// lattices or handles share the device chunk by chunk.  Results are written
+// back in the QOP raw layout with the QOP_asqtad_invert normalisation
+// (m A^-1 b) as each system finishes.
 //
-// Requests of one group are taken in arrival order from the front of the
-// queue; a request is never split across batches.  Timing per request:
-// queue (submit -> batch start), solve (batch start -> results copied) and
-// total.  While the service runs the worker owns the library (its global
-// stream, current lattice and option state); callers only submit and wait.
+// Admission: requests in arrival order; a request is never split (all of
+// its sources enter one engine together) and a request that does not fit
+// holds back the later requests of its engine.  A new engine is created
+// only if its device memory fits in the free HBM (less a reserve) while
+// other engines run; an engine whose slots are all free is destroyed.
+// Timing per request: queue (submit -> admission), solve (admission ->
+// last source finished) and total.  While the service runs the worker owns
+// the library (its global stream, current lattice and option state);
+// callers only submit and wait.
 #include "solvers.cuh"
 #include "fields.cuh"
+#include <algorithm>
 #include <chrono>
 #include <condition_variable>
 #include <deque>
+#include <memory>
 #include <mutex>
 #include <thread>
+#include <tuple>
 #include <unordered_map>
 #include <vector>
 
@@ -34,7 +47,7 @@ struct Job {
   std::vector<const double *> src;
   std::vector<double *> dst;
   double t_submit = 0, t_start = 0, t_done = 0;
-  int status = QOP_SUCCESS, iters_max = 0, batch = 0;
+  int status = QOP_SUCCESS, iters_max = 0, batch = 0, left = 0;
   double rsq_max = 0;
   bool done = false;
 };
@@ -50,98 +63,212 @@ struct Service {
 };
 Service g_srv;
 
-// one batched solve for a group of requests sharing links, lattice, parity
-void run_group(std::vector<Job *> &grp) {
-  const QOPB_request_t &r0 = grp[0]->rq;
-  if (QOPB_lattice_use(r0.lattice) != 0) fail(QOP_FAIL, "serve: unknown lattice %d", r0.lattice);
-  handle_check(r0.links, "FermionLinksAsqtad");
-  FlaT<double> *f = reinterpret_cast<FlaT<double> *>(r0.links);
-  const int eo = r0.evenodd;
-  const Geom &g = ctx().g;
-  std::vector<double> m, rq;
+// one engine with its FP64 solution and source vectors per slot
+struct Lane {
+  int lattice = 0, eo = 0;
+  const void *links = nullptr;
+  std::unique_ptr<BatchEngine> eng;
   std::vector<c2<double> *> x, b;
-  std::vector<std::pair<Job *, int>> who;
-  int max_iter = 1;
-  for (Job *j : grp) {
-    max_iter = std::max(max_iter, j->rq.max_iter > 0 ? j->rq.max_iter : 100000);
-    for (int k = 0; k < j->rq.nrhs; k++) {
-      m.push_back(j->rq.mass);
-      rq.push_back(j->rq.rsqmin);
-      who.push_back({j, k});
-    }
-  }
-  const int n = (int)m.size();
-  try {
-    for (int s = 0; s < n; s++) {
-      c2<double> *xs = dalloc<c2<double>>(vec_elems(g)), *bs = dalloc<c2<double>>(vec_elems(g));
-      x.push_back(xs);
-      b.push_back(bs);
-      dzero(xs, sizeof(c2<double>) * vec_elems(g));
-      dzero(bs, sizeof(c2<double>) * vec_elems(g));
-      raw_to_dev<double, double>(bs, who[s].first->src[who[s].second], 3, eo);
-    }
-    std::vector<int> its(n);
-    std::vector<double> frs(n);
-    run_batch(f, eo, n, m.data(), x.data(), b.data(), rq.data(), max_iter, its.data(), frs.data());
-    for (int s = 0; s < n; s++) {
-      Job *j = who[s].first;
-      dev_to_raw<double, double>(j->dst[who[s].second], x[s], 3, eo, m[s]);   // m A^-1 b
-      j->iters_max = std::max(j->iters_max, its[s]);
-      j->rsq_max = std::max(j->rsq_max, frs[s]);
-      j->batch = n;
-    }
-  } catch (...) {
+  struct Occ { Job *job = nullptr; int k = 0; };
+  std::vector<Occ> occ;
+  ~Lane() {
+    eng.reset();
     for (auto *p : x) dfree(p);
     for (auto *p : b) dfree(p);
-    throw;
   }
-  for (auto *p : x) dfree(p);
-  for (auto *p : b) dfree(p);
-  sync();
+};
+
+constexpr size_t HBM_RESERVE = size_t(2) << 30;   // left free when other engines run
+
+void finish(Job *j, int status) {
+  Service &S = g_srv;
+  {
+    std::lock_guard<std::mutex> lk(S.mu);
+    j->t_done = now_ms();
+    if (status != QOP_SUCCESS) j->status = status;
+    j->done = true;
+  }
+  S.cv_done.notify_all();
 }
+
+struct Worker {
+  std::vector<std::unique_ptr<Lane>> lanes;
+  std::deque<Job *> pending;   // taken from the queue, not yet admitted
+
+  Lane *find(const QOPB_request_t &r) {
+    for (auto &l : lanes)
+      if (l->links == r.links && l->lattice == r.lattice && l->eo == r.evenodd) return l.get();
+    return nullptr;
+  }
+  bool any_running() const {
+    for (auto &l : lanes)
+      if (l->eng->busy() > 0) return true;
+    return false;
+  }
+
+  // a new engine for the request's handle and parity on the current lattice;
+  // nullptr (nothing allocated) when it does not fit while others run
+  Lane *create(const QOPB_request_t &r) {
+    const Geom &g = ctx().g;
+    const size_t need = BatchEngine::bytes(g, BATCH_MAX) + 2 * sizeof(c2<double>) * vec_elems(g) * BATCH_MAX;
+    size_t fr = 0, tot = 0;
+    if (any_running() && cudaMemGetInfo(&fr, &tot) == cudaSuccess && fr < need + HBM_RESERVE) return nullptr;
+    cudaGetLastError();
+    auto l = std::make_unique<Lane>();
+    l->lattice = r.lattice;
+    l->eo = r.evenodd;
+    l->links = r.links;
+    l->eng = std::make_unique<BatchEngine>(reinterpret_cast<FlaT<double> *>(r.links), r.evenodd, BATCH_MAX);
+    for (int s = 0; s < BATCH_MAX; s++) {
+      l->x.push_back(dalloc<c2<double>>(vec_elems(g)));
+      l->b.push_back(dalloc<c2<double>>(vec_elems(g)));
+    }
+    l->occ.assign(BATCH_MAX, Lane::Occ{});
+    lanes.push_back(std::move(l));
+    return lanes.back().get();
+  }
+
+  // admit pending requests in arrival order while slots and memory allow
+  void admit() {
+    std::vector<const Lane *> held;   // engines whose earlier request did not fit
+    std::vector<std::tuple<const void *, int, int>> held_new;
+    for (auto it = pending.begin(); it != pending.end();) {
+      Job *j = *it;
+      const QOPB_request_t &r = j->rq;
+      const auto key = std::make_tuple((const void *)r.links, r.lattice, (int)r.evenodd);
+      bool later = false;
+      for (auto &k : held_new) later = later || k == key;
+      Lane *l = find(r);
+      if (later || (l && std::find(held.begin(), held.end(), l) != held.end())) { ++it; continue; }
+      bool starting = false;   // slots of l are being filled
+      try {
+        if (QOPB_lattice_use(r.lattice) != 0) fail(QOP_FAIL, "serve: unknown lattice %d", r.lattice);
+        handle_check(r.links, "FermionLinksAsqtad");
+        if (!l) {
+          try {
+            l = create(r);
+          } catch (Fail &e) {
+            if (e.status != QOP_MEM_ERROR || !any_running()) throw;
+            l = nullptr;
+          }
+          if (!l) {   // waits for memory
+            held_new.push_back(key);
+            ++it;
+            continue;
+          }
+        }
+        if (BATCH_MAX - l->eng->busy() < r.nrhs) {
+          held.push_back(l);
+          ++it;
+          continue;
+        }
+        const Geom &g = ctx().g;
+        j->t_start = now_ms();
+        j->left = r.nrhs;
+        starting = true;
+        for (int k = 0; k < r.nrhs; k++) {
+          const int s = l->eng->free_slot();
+          dzero(l->b[s], sizeof(c2<double>) * vec_elems(g));
+          raw_to_dev<double, double>(l->b[s], j->src[k], 3, r.evenodd);
+          l->occ[s] = Lane::Occ{j, k};
+          l->eng->start(s, l->x[s], l->b[s], r.mass, r.rsqmin, r.max_iter > 0 ? r.max_iter : 100000, true);
+        }
+        j->batch = std::max(j->batch, l->eng->busy());
+      } catch (Fail &e) {
+        fprintf(stderr, "QOPB serve: %s\n", e.msg.c_str());
+        bool in_lane = false;
+        if (starting) {
+          // the engine's state is unknown after a failed start: every request
+          // in it fails (this one too, if it holds a slot)
+          for (auto &o : l->occ) in_lane = in_lane || o.job == j;
+          drop(l, e.status);
+        }
+        if (!in_lane) {
+          j->t_start = now_ms();
+          finish(j, e.status);
+        }
+      }
+      it = pending.erase(it);
+    }
+  }
+
+  // fail every request with a source in lane l and destroy it
+  void drop(Lane *l, int status) {
+    std::vector<Job *> js;
+    for (auto &o : l->occ)
+      if (o.job && std::find(js.begin(), js.end(), o.job) == js.end()) js.push_back(o.job);
+    for (auto &p : lanes)
+      if (p.get() == l) { p.reset(); break; }
+    lanes.erase(std::remove(lanes.begin(), lanes.end(), nullptr), lanes.end());
+    for (Job *j : js) finish(j, status);
+  }
+
+  // one step of every engine with work; results of finished systems
+  void step_all() {
+    for (size_t li = 0; li < lanes.size(); li++) {
+      Lane *l = lanes[li].get();
+      if (l->eng->busy() == 0) continue;
+      std::vector<Job *> ended;
+      try {
+        if (QOPB_lattice_use(l->lattice) != 0) fail(QOP_FAIL, "serve: unknown lattice %d", l->lattice);
+        const std::vector<int> fin = l->eng->step();
+        const int nb = l->eng->busy();
+        for (auto &o : l->occ)
+          if (o.job) o.job->batch = std::max(o.job->batch, nb);
+        for (int s : fin) {
+          Lane::Occ &o = l->occ[s];
+          Job *j = o.job;
+          const QOPB_request_t &r = j->rq;
+          dev_to_raw<double, double>(j->dst[o.k], l->x[s], 3, r.evenodd, r.mass);   // m A^-1 b
+          j->iters_max = std::max(j->iters_max, l->eng->iters(s));
+          j->rsq_max = std::max(j->rsq_max, l->eng->final_rsq(s));
+          l->eng->release(s);
+          o = Lane::Occ{};
+          if (--j->left == 0) ended.push_back(j);
+        }
+        if (!ended.empty()) sync();
+      } catch (Fail &e) {
+        fprintf(stderr, "QOPB serve: %s\n", e.msg.c_str());
+        for (Job *j : ended) finish(j, QOP_SUCCESS);
+        drop(l, e.status);
+        li--;
+        continue;
+      }
+      for (Job *j : ended) finish(j, QOP_SUCCESS);
+    }
+    // engines with no system left are freed (their memory goes to new ones)
+    lanes.erase(std::remove_if(lanes.begin(), lanes.end(), [](const std::unique_ptr<Lane> &l) {
+                  return l->eng->busy() == 0;
+                }),
+                lanes.end());
+  }
+};
 
 void worker_loop(int device) {
   cudaSetDevice(device);
   Service &S = g_srv;
+  Worker w;
   while (true) {
-    std::vector<Job *> grp;
     {
       std::unique_lock<std::mutex> lk(S.mu);
-      S.cv.wait(lk, [&] { return S.stopping || !S.queue.empty(); });
-      if (S.queue.empty()) return;   // stopping and drained
-      const Job *first = S.queue.front();
-      int nsys = 0;
-      for (auto it = S.queue.begin(); it != S.queue.end();) {
-        const QOPB_request_t &r = (*it)->rq;
-        if (r.links == first->rq.links && r.lattice == first->rq.lattice && r.evenodd == first->rq.evenodd &&
-            nsys + r.nrhs <= BATCH_MAX) {
-          nsys += r.nrhs;
-          grp.push_back(*it);
-          it = S.queue.erase(it);
-        } else {
-          ++it;
-        }
+      const bool work = w.any_running() || !w.pending.empty();
+      if (!work) S.cv.wait(lk, [&] { return S.stopping || !S.queue.empty(); });
+      while (!S.queue.empty()) {
+        w.pending.push_back(S.queue.front());
+        S.queue.pop_front();
       }
+      if (S.stopping && w.pending.empty() && !w.any_running()) return;
     }
-    const double t0 = now_ms();
-    for (Job *j : grp) j->t_start = t0;
-    int status = QOP_SUCCESS;
-    try {
-      run_group(grp);
-    } catch (Fail &e) {
-      fprintf(stderr, "QOPB serve: %s\n", e.msg.c_str());
-      status = e.status;
-    }
-    {
-      std::lock_guard<std::mutex> lk(S.mu);
-      const double t1 = now_ms();
-      for (Job *j : grp) {
-        j->t_done = t1;
-        j->status = status;
-        j->done = true;
+    w.admit();
+    if (!w.any_running() && !w.pending.empty()) {
+      // nothing runs and the front requests still do not fit: they cannot
+      for (Job *j : w.pending) {
+        j->t_start = now_ms();
+        finish(j, QOP_MEM_ERROR);
       }
+      w.pending.clear();
     }
-    S.cv_done.notify_all();
+    w.step_all();
   }
 }
 

@@ -55,6 +55,40 @@ bool mixed_cgms(LinOp<double> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t **ra, co
 constexpr int BATCH_MAX = 16;
 void run_batch(FlaT<double> *f, int eo, int n, const double *mass, c2<double> **x, c2<double> *const *b,
                const double *rsqmin, int max_iter, int *iters, double *final_rsq);
+
+// The solver of run_batch as a set of `cap` slots on one link handle and
+// parity of the current lattice that systems enter and leave between steps
+// (continuous batching): a system started while others are in flight joins
+// their next hop launches; a finished slot can take a new system at once.
+// Each system's iteration is independent of the others', so a system takes
+// the same iterations and reaches the same solution alone or in a mix.
+class BatchEngine {
+ public:
+  BatchEngine(FlaT<double> *f, int eo, int cap);
+  ~BatchEngine();
+  BatchEngine(const BatchEngine &) = delete;
+  BatchEngine &operator=(const BatchEngine &) = delete;
+  // device bytes of an engine with cap slots on geometry g
+  static size_t bytes(const Geom &g, int cap);
+  int cap() const;
+  int busy() const;       // slots holding a system (running or finished)
+  int running() const;    // slots still iterating
+  int free_slot() const;  // lowest free slot, or -1
+  // start (m^2 - D D) x = b in free slot s; x (the starting guess, or zero
+  // with x_zero) and b are FP64 device vectors the caller keeps until the
+  // slot is released; rsqmin is the target on |b - A x|^2 / |b|^2
+  void start(int s, c2<double> *x, const c2<double> *b, double mass, double rsqmin, int max_iter, bool x_zero);
+  // one chunk of iterations of every running system, then their reliable
+  // updates; returns the slots whose systems finished (x holds the solution)
+  std::vector<int> step();
+  int iters(int s) const;         // hop pairs plus reliable updates
+  double final_rsq(int s) const;  // FP64 |r|^2 / |b|^2
+  void release(int s);
+
+ private:
+  struct Impl;
+  Impl *d;
+};
 // several masses on one parity with prec_sloppy < 64: reduced-precision
 // multi-shift CG per shared source, then per-solve refinement
 void solve_multi_mixed(QOP_info_t *info, FlaT<double> *f, QOP_invert_arg_t *ia, QOP_resid_arg_t **ra,

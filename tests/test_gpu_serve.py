@@ -100,3 +100,74 @@ def test_serve_two_lattices():
     q.destroy_L(hb)
     assert q.lattice_use(0) == 0
     q.destroy_L(ha)
+
+
+def test_serve_continuous_batching_same_alone_and_in_the_mix():
+    """Continuous batching: a request that arrives while a long request on
+    the same links is in flight joins its batch at once (it shares A's hop
+    launches and finishes long before A), a request on another lattice runs
+    beside them, and each result is the same alone and in the mix (both meet
+    the FP64 target; their difference is within the solve tolerance)."""
+    import time
+    q = gpu_lattice(LA, "D")
+    lb = q.lattice_create(LB)
+    fa, la_, _, _ = hisq_links(LA, 0.5, 9)
+    fb, lb_ = asqtad_links(LB, 0.3, 7)
+    foa, fob = O.Fla(O.Lattice(LA), fa, la_), O.Fla(O.Lattice(LB), fb, lb_)
+    assert q.lattice_use(0) == 0
+    ha = q.create_L_from_raw(fa, la_)
+    assert q.lattice_use(lb) == 0
+    hb = q.create_L_from_raw(fb, lb_)
+    assert q.lattice_use(0) == 0
+    rsq = 1e-20
+    # A: 4 sources at m = 0.002 on LB (~16k iterations); R: LB, same links
+    # and parity, m = 0.05; C: LA, m = 0.1
+    a_src = [LT.gaussian_vector(LB, 700 + k) for k in range(4)]
+    r_src, c_src = LT.gaussian_vector(LB, 710), LT.gaussian_vector(LA, 711)
+    R = (hb, lb, 0, 0.05)
+    Cq = (ha, 0, 1, 0.1)
+    assert q.serve_start() == 0
+    try:
+        alone = {}
+        for name, (h, lat, eo, m), s in (("R", R, r_src), ("C", Cq, c_src)):
+            d = [np.zeros_like(s)]
+            rc, res = q.serve_wait(q.serve_submit(h, lat, eo, m, rsq, [s], d), 120.0)
+            assert rc == 0 and res.status == 0 and res.batch_systems == 1
+            alone[name] = (d[0], res.iters_max)
+        a_dst = [np.zeros_like(s) for s in a_src]
+        r_dst, c_dst = [np.zeros_like(r_src)], [np.zeros_like(c_src)]
+        t_a = time.perf_counter()
+        ta = q.serve_submit(hb, lb, 0, 0.002, rsq, a_src, a_dst)
+        assert ta >= 0
+        assert q.serve_wait(ta, 0.05)[0] == 1          # A is in flight
+        t_r = time.perf_counter()
+        tr = q.serve_submit(*R[:3], R[3], rsq, [r_src], r_dst)
+        tc = q.serve_submit(*Cq[:3], Cq[3], rsq, [c_src], c_dst)
+        rc_r, res_r = q.serve_wait(tr, 120.0)
+        rc_c, res_c = q.serve_wait(tc, 120.0)
+        rc_a, res_a = q.serve_wait(ta, 300.0)
+    finally:
+        assert q.serve_stop() == 0
+    assert rc_r == rc_c == rc_a == 0
+    assert res_r.status == res_c.status == res_a.status == 0
+    # R shared A's batch and did not wait for it
+    assert res_r.batch_systems >= 5, res_r.batch_systems
+    assert res_r.queue_ms < 0.25 * res_a.solve_ms, (res_r.queue_ms, res_a.solve_ms)
+    assert 1e3 * (t_r - t_a) + res_r.total_ms < res_a.total_ms, (res_r.total_ms, res_a.total_ms)
+    assert 1e3 * (t_r - t_a) + res_c.total_ms < res_a.total_ms, (res_c.total_ms, res_a.total_ms)
+    # every result meets its FP64 target
+    for fo, L, eo, m, srcs, dsts in ((fob, LB, 0, 0.002, a_src, a_dst), (fob, LB, 0, 0.05, [r_src], r_dst),
+                                     (foa, LA, 1, 0.1, [c_src], c_dst)):
+        for s, d in zip(srcs, dsts):
+            assert eo_residual(fo, m, d, s, L, eo) <= rsq * 1.05, (L, m)
+    # the same alone and in the mix
+    for name, L, eo, m, d in (("R", LB, 0, 0.05, r_dst[0]), ("C", LA, 1, 0.1, c_dst[0])):
+        d0, it0 = alone[name]
+        err = rel_norm_err(half(d, L, eo), half(d0, L, eo))
+        assert err <= max(1e-8, 30 * np.sqrt(rsq) / m ** 2), (name, err)
+    assert abs(res_r.iters_max - alone["R"][1]) <= 2
+    assert abs(res_c.iters_max - alone["C"][1]) <= 2
+    assert q.lattice_use(lb) == 0
+    q.destroy_L(hb)
+    assert q.lattice_use(0) == 0
+    q.destroy_L(ha)
