@@ -80,6 +80,8 @@ def parse():
                          "serve: the solve service under Poisson load")
     ap.add_argument("--serve-burst", type=int, default=12, help="requests of the peak-throughput burst")
     ap.add_argument("--serve-seconds", type=float, default=20.0, help="arrival window per load level")
+    ap.add_argument("--serve-policy", type=int, default=0, choices=[0, 1],
+                    help="0: step every engine in turn; 1: only the engine holding the oldest request")
     return ap.parse_args()
 
 
@@ -1022,6 +1024,7 @@ def run_serve(a):
             out.append((rc, res.status, res.total_ms, res.final_rsq_max / rsq, nrhs, res.batch_systems))
         return out
 
+    assert q.set_opts(serve_policy=a.serve_policy) == 0
     assert q.serve_start() == 0
     # warm-up: one request per lattice (builds the int16 link copies)
     collect([(submit(k, 0.05, 1e-16, 1), 1, 1e-16) for k in range(len(SERVE_LATTICES))])
@@ -1072,7 +1075,8 @@ def run_serve(a):
                 "data": "synthetic",
                 "config": {"workload": "serve", "lattices": SERVE_LATTICES, "mass": "log-uniform [0.005, 0.1]",
                            "tol": [1e-8, 1e-10], "sources_per_request": "1-8", "burst": a.serve_burst,
-                           "seconds_per_load": a.serve_seconds, "parallelism": "replicas x%d" % world},
+                           "seconds_per_load": a.serve_seconds, "policy": a.serve_policy,
+                           "parallelism": "replicas x%d" % world},
                 "peak_solves_per_s": peak, "loads": loads, "p99_ms_max_over_ranks": p99}
         print(json.dumps(line), flush=True)
     for lat, (H, _) in zip(lats, links):

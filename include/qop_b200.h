@@ -107,11 +107,14 @@ int QOPB_lattice_create(const int latsize[4]);
 int QOPB_lattice_use(int id);
 int QOPB_lattice_current(void);
 
-/* Solve service (no counterpart in the reference).  A worker thread
-   takes queued requests, groups the systems of requests on the same link
-   handle (up to 16) into one batched mixed-precision solve (int16 storage,
-   FP64 reliable updates: every solution meets its FP64 target) and copies
-   the results to the caller's buffers.  A request solves, for each of its
+/* Solve service (no counterpart in the reference).  A worker thread keeps
+   a batched mixed-precision solver (16 slots; int16 storage, FP64 reliable
+   updates: every solution meets its FP64 target) per link handle and
+   parity in flight and admits the systems of queued requests into free
+   slots between solver steps (continuous batching); each finished system's
+   result is copied to the caller's buffer.  Option tag serve_policy: 0
+   steps every solver in turn (default), 1 only the one holding the oldest
+   request.  A request solves, for each of its
    nrhs sources, A x = b with A = m^2 - D D on parity `evenodd` (QOP_EVEN or
    QOP_ODD) and writes m A^-1 b on that parity (the QOP_asqtad_invert
    convention) into dst[k]; src[k] / dst[k] are raw full-volume arrays

@@ -11,6 +11,11 @@
 // back in the QOP raw layout with the QOP_asqtad_invert normalisation
 // (m A^-1 b) as each system finishes.
 //
+// Option serve_policy 1 steps only the engine holding the oldest request
+// (requests still join any engine's free slots): first-come first-served
+// across engines, which shortens the longest latencies of a heavy-tailed
+// mix at the cost of the median.
+//
 // Admission: requests in arrival order; a request is never split (all of
 // its sources enter one engine together) and a request that does not fit
 // holds back the later requests of its engine.  A new engine is created
@@ -203,11 +208,26 @@ struct Worker {
     for (Job *j : js) finish(j, status);
   }
 
-  // one step of every engine with work; results of finished systems
+  // submission time of the oldest request holding a slot of l
+  static double oldest(const Lane *l) {
+    double t = 1e300;
+    for (auto &o : l->occ)
+      if (o.job) t = std::min(t, o.job->t_submit);
+    return t;
+  }
+
+  // one step of every engine with work (policy 1: of the engine holding the
+  // oldest request, and of engines with nothing left to iterate); results
+  // of finished systems
   void step_all() {
+    const Lane *first = nullptr;
+    if (ctx().opt.serve_policy == 1)
+      for (auto &l : lanes)
+        if (l->eng->running() > 0 && (!first || oldest(l.get()) < oldest(first))) first = l.get();
     for (size_t li = 0; li < lanes.size(); li++) {
       Lane *l = lanes[li].get();
       if (l->eng->busy() == 0) continue;
+      if (first && l != first && l->eng->running() > 0) continue;
       std::vector<Job *> ended;
       try {
         if (QOPB_lattice_use(l->lattice) != 0) fail(QOP_FAIL, "serve: unknown lattice %d", l->lattice);

@@ -46,8 +46,13 @@ def test_handles_belong_to_their_lattice():
     assert q.lattice_use(0) == 0
 
 
-def test_serve_two_lattices():
+@pytest.mark.parametrize("policy", [0, 1])
+def test_serve_two_lattices(policy):
+    """Queued requests on two lattices, both service policies (0: every
+    engine steps in turn; 1: the engine holding the oldest request)."""
     q = gpu_lattice(LA, "D")
+    assert q.set_opts(serve_policy=2) != 0
+    assert q.set_opts(serve_policy=policy) == 0
     lb = q.lattice_create(LB)
     fa, la_, _, _ = hisq_links(LA, 0.5, 9)
     fb, lb_ = asqtad_links(LB, 0.3, 7)
@@ -83,6 +88,7 @@ def test_serve_two_lattices():
         results.append(res)
     assert q.serve_wait(tickets[0], 1.0)[0] == -1      # released
     assert q.serve_stop() == 0
+    assert q.set_opts(serve_policy=0) == 0
     for (on_b, L, srcs, dsts, mass, rsq, eo), res in zip(reqs, results):
         fo = fob if on_b else foa
         assert res.status == 0
