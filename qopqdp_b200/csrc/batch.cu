@@ -29,6 +29,8 @@
 #include "fields.cuh"
 #include "mixed.cuh"
 #include <algorithm>
+#include <array>
+#include <map>
 #include <vector>
 #include <cmath>
 
@@ -348,6 +350,10 @@ static void launch_bhop(int variant, int nl, bool recon, int ngrp, int nsb, uint
 #undef BH_CALL
 }
 
+// autotuned batched hop variant per (lattice extents, links per site,
+// long-link reconstruction, systems)
+static std::map<std::array<int, 7>, int> g_bhop_tuned;
+
 struct BatchEngine::Impl {
   FlaT<double> *f;
   int lat, eo, cap;
@@ -525,22 +531,42 @@ std::vector<int> BatchEngine::step() {
   if (active == 0) return fin;
   SloppyLinks *sl = sloppy_get(e.f, LK_Q16);
   const LinksSloppy lk_p = links_parity(sl, LK_Q16, p), lk_q = links_parity(sl, LK_Q16, q);
-  // by default 8 systems per thread when they fill whole groups of 8 (16
-  // sources at 32^4: 531 us per hop against 574 with 4), else 4 (12 masses
-  // at 24^3x48: 1696 ms per call against 1989 ms with groups of 8 and 4)
-  const int variant = c.opt.batch_kernel < 0 ? (n % 8 == 0 ? 7 : 1) : std::min(c.opt.batch_kernel, N_BHOP - 1);
-  const int BG = kBhop[variant].bg;
-  const int ngrp = (n + BG - 1) / BG, nsb = e.nsb, gridv = e.gridv;
   const int nl = sl->nl;
   const bool recon = sl->recon != 0;
   const float c_long = (float)sl->c_long;
+  const int nsb = e.nsb, gridv = e.gridv;
+  QCHECK(cudaMemcpyAsync(e.dst, e.h.data(), sizeof(MixState) * n, cudaMemcpyHostToDevice, c.s));
+  // by default 8 systems per thread when they fill whole groups of 8 (16
+  // sources at 32^4: 531 us per hop against 574 with 4), else 4 (12 masses
+  // at 24^3x48: 1696 ms per call against 1989 ms with groups of 8 and 4);
+  // batch_kernel -2: the fastest of 1, 6, 7, 9, 12 timed on the first step
+  // with this lattice and number of systems
+  int variant = c.opt.batch_kernel == -1 ? (n % 8 == 0 ? 7 : 1) : std::min(c.opt.batch_kernel, N_BHOP - 1);
+  if (c.opt.batch_kernel == -2) {
+    const std::array<int, 7> key{g.L[0], g.L[1], g.L[2], g.L[3], nl, recon ? 1 : 0, n};
+    auto it = g_bhop_tuned.find(key);
+    if (it != g_bhop_tuned.end()) {
+      variant = it->second;
+    } else {
+      const unsigned char *lq = (const unsigned char *)lk_q.a;
+      variant = tune_pick({1, 6, 7, 9, 12}, [&](int v) {   // t = D p: recomputed by the first iteration
+        launch_bhop<1>(v, nl, recon, (n + kBhop[v].bg - 1) / kBhop[v].bg, nsb, e.ts, e.ps, lq, nullptr, g, e.ng, q,
+                       e.dst, n, e.part, e.count, c_long);
+        QLAUNCH();
+      });
+      g_bhop_tuned[key] = variant;
+      log0(QOP_VERB_LOW, "autotune: batched hop variant %d for %d systems on %dx%dx%dx%d\n", variant, n, g.L[0],
+           g.L[1], g.L[2], g.L[3]);
+    }
+  }
+  const int BG = kBhop[variant].bg;
+  const int ngrp = (n + BG - 1) / BG;
   const int chunk = c.opt.chunk;
   char hname[32];
   snprintf(hname, sizeof hname, "bhop_q16_x%d", n);
   const double link_site = recon ? (nl / 2) * (40.0 + 28.0) : nl * 40.0;
   // compulsory bytes of one hop for the systems running in this chunk
   const double hop_bytes = (double)Vh * (link_site + 2.0 * 16 * active);
-  QCHECK(cudaMemcpyAsync(e.dst, e.h.data(), sizeof(MixState) * n, cudaMemcpyHostToDevice, c.s));
   std::vector<int> recs;
   for (int k = 0; k < chunk; k++) {
     {

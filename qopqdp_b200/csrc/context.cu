@@ -292,7 +292,7 @@ QOP_status_t QOP_asqtad_invert_set_opts(QOP_opt_t opts[], int nopts) {
       if (p != 16 && p != 32 && p != 64) return QOP_FAIL;
       n.sloppy_prec = p;
     } else if (!strcmp(t, "batch_kernel")) {
-      if (v < -1 || v > 15) return QOP_FAIL;
+      if (v < -2 || v > 15) return QOP_FAIL;
       n.batch_kernel = (int)v;
     } else if (!strcmp(t, "multi_shift")) {
       n.multi_shift = v != 0;
@@ -304,7 +304,7 @@ QOP_status_t QOP_asqtad_invert_set_opts(QOP_opt_t opts[], int nopts) {
     } else if (!strcmp(t, "recon_long")) {
       n.recon_long = v != 0;
     } else if (!strcmp(t, "hop_kernel")) {
-      if (v < 0 || v > 28) return QOP_FAIL;
+      if (v < -1 || v > 28) return QOP_FAIL;
       n.hop_kernel = (int)v;
     } else if (!strcmp(t, "half_format")) {
       if (v < 0 || v > 2) return QOP_FAIL;

@@ -155,7 +155,7 @@ int sloppy_prec() {
   const Context &c = ctx();
   if (!c.dd) return c.opt.sloppy_prec;
   const Options &o = c.opt;
-  return (o.sloppy_prec == 16 && o.half_format == 0 && o.fuse_update && o.hop_kernel >= 20) ? 16 : 64;
+  return (o.sloppy_prec == 16 && o.half_format == 0 && o.fuse_update && (o.hop_kernel >= 20 || o.hop_kernel == -1)) ? 16 : 64;
 }
 
 void dd_allreduce(double *d, int n) {

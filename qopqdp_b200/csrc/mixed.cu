@@ -29,6 +29,7 @@
 #include "mixed.cuh"
 #include "dd.cuh"
 #include <algorithm>
+#include <array>
 #include <map>
 #include <vector>
 #include <cmath>
@@ -1089,6 +1090,10 @@ struct MsArgs {
   c2<double> **x;
 };
 
+// autotuned int16 hop variant per (lattice extents, links per site, long-link
+// reconstruction)
+static std::map<std::array<int, 6>, int> g_hop_tuned;
+
 template <class Sp, class Lk>
 static void run_mixed(LinOp<double> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t *ra, c2<double> *x,
                       const c2<double> *b, int eo, SloppyLinks *sl, int lkfmt, const MsArgs *ms = nullptr) {
@@ -1176,7 +1181,29 @@ static void run_mixed(LinOp<double> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t *r
   // fused update (option fuse_update): the second hop reduces what the
   // update needs and one kernel updates x, r and p
   constexpr bool q16v = std::is_same<Lk, LkQ16B>::value && std::is_same<Sp, SpQ16>::value;
-  const bool fuse = q16v && ns == 1 && c.opt.fuse_update && c.opt.hop_kernel >= 20;
+  // int16 hop variant: the option, or (hop_kernel -1) the fastest of the
+  // packed persistent variants 20-26 timed on this lattice's first solve
+  int hk = c.opt.hop_kernel;
+  if constexpr (std::is_same<Lk, LkQ16B>::value) {
+    if (hk < 0) {
+      const std::array<int, 6> key{g.L[0], g.L[1], g.L[2], g.L[3], nl, recon ? 1 : 0};
+      auto it = g_hop_tuned.find(key);
+      if (dd_active()) {
+        hk = 25;   // the decomposed hop has the shape of variant 25
+      } else if (it != g_hop_tuned.end()) {
+        hk = it->second;
+      } else {
+        const unsigned char *lq = (const unsigned char *)lk_q.a;
+        hk = tune_pick({20, 21, 22, 23, 24, 25, 26}, [&](int v) {   // t = D p: recomputed by the first iteration
+          launch_q16<1>(v, nl, recon, c_long, gridq, ts, ps, lq, nullptr, g, ng, q, dst);
+          QLAUNCH();
+        });
+        g_hop_tuned[key] = hk;
+        log0(QOP_VERB_LOW, "autotune: int16 hop variant %d on %dx%dx%dx%d\n", hk, g.L[0], g.L[1], g.L[2], g.L[3]);
+      }
+    }
+  }
+  const bool fuse = q16v && ns == 1 && c.opt.fuse_update && hk >= 20;
   int seq = 0;
   // a decomposed lattice: halos before each hop, the reductions summed over
   // the processes before the scalars (the fused int16 iteration only)
@@ -1218,7 +1245,7 @@ static void run_mixed(LinOp<double> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t *r
         ProfScope ps1(hname, hop_bytes);
         if constexpr (std::is_same<Lk, LkQ16B>::value) {
           const unsigned char *lq = (const unsigned char *)lk_q.a;
-          launch_q16<1>(c.opt.hop_kernel, nl, recon, c_long, gridq, ts, ps, lq, nullptr, g, ng, q, dst);
+          launch_q16<1>(hk, nl, recon, c_long, gridq, ts, ps, lq, nullptr, g, ng, q, dst);
         } else {
           if (nl == 16) k_mix_hop<Sp, Lk, 16, 1><<<gridh, 128, 0, c.s>>>(ts, ps, lk_q, nullptr, g, q, dst, c.d_part, c.d_count);
           else k_mix_hop<Sp, Lk, 8, 1><<<gridh, 128, 0, c.s>>>(ts, ps, lk_q, nullptr, g, q, dst, c.d_part, c.d_count);
@@ -1229,11 +1256,11 @@ static void run_mixed(LinOp<double> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t *r
         ProfScope ps2(fuse ? hname3 : hname, hop_bytes + (double)Vh * Sp::site_bytes * (fuse ? 2 : 1));
         if constexpr (q16v) {
           const unsigned char *lp = (const unsigned char *)lk_p.a;
-          if (fuse) launch_q16_fused(c.opt.hop_kernel, nl, recon, c_long, gridq, Aps, ts, lp, ps, g, ng, p, dst, rs, ++seq);
-          else launch_q16<2>(c.opt.hop_kernel, nl, recon, c_long, gridq, Aps, ts, lp, ps, g, ng, p, dst);
+          if (fuse) launch_q16_fused(hk, nl, recon, c_long, gridq, Aps, ts, lp, ps, g, ng, p, dst, rs, ++seq);
+          else launch_q16<2>(hk, nl, recon, c_long, gridq, Aps, ts, lp, ps, g, ng, p, dst);
         } else if constexpr (std::is_same<Lk, LkQ16B>::value) {
           const unsigned char *lp = (const unsigned char *)lk_p.a;
-          launch_q16<2>(c.opt.hop_kernel, nl, recon, c_long, gridq, Aps, ts, lp, ps, g, ng, p, dst);
+          launch_q16<2>(hk, nl, recon, c_long, gridq, Aps, ts, lp, ps, g, ng, p, dst);
         } else {
           if (nl == 16) k_mix_hop<Sp, Lk, 16, 2><<<gridh, 128, 0, c.s>>>(Aps, ts, lk_p, ps, g, p, dst, c.d_part, c.d_count);
           else k_mix_hop<Sp, Lk, 8, 2><<<gridh, 128, 0, c.s>>>(Aps, ts, lk_p, ps, g, p, dst, c.d_part, c.d_count);

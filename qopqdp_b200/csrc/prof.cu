@@ -66,6 +66,34 @@ void prof_discard(int idx) {
 
 bool prof_active() { return g_prof.active; }
 
+int tune_pick(const std::vector<int> &cand, const std::function<void(int)> &launch, int reps) {
+  Context &c = ctx();
+  cudaEvent_t a = nullptr, b = nullptr;
+  int best = cand.empty() ? -1 : cand[0];
+  float best_ms = 3.0e38f;
+  try {
+    QCHECK(cudaEventCreate(&a));
+    QCHECK(cudaEventCreate(&b));
+    for (int v : cand) {
+      launch(v);   // warm-up
+      QCHECK(cudaEventRecord(a, c.s));
+      for (int r = 0; r < reps; r++) launch(v);
+      QCHECK(cudaEventRecord(b, c.s));
+      QCHECK(cudaEventSynchronize(b));
+      float ms = 0;
+      QCHECK(cudaEventElapsedTime(&ms, a, b));
+      if (ms < best_ms) { best_ms = ms; best = v; }
+    }
+  } catch (...) {
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+    throw;
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return best;
+}
+
 }  // namespace qopb
 
 using namespace qopb;

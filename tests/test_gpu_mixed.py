@@ -314,6 +314,44 @@ def test_every_batch_kernel_variant():
     q.destroy_L(fla)
 
 
+def test_autotuned_hop_variants():
+    """Options hop_kernel -1 and batch_kernel -2: the first solve on a
+    lattice times the candidate variants (one-system hops 20-26; batched
+    hops 1, 6, 7, 9, 12) and keeps the fastest; the solves reach the FP64
+    target with the iteration counts of the fixed defaults, and a second
+    solve (cached choice) repeats the first."""
+    L = (8, 8, 8, 8)
+    q = gpu_lattice(L, "D")
+    fat, lng, _, _ = hisq_links(L, 0.5, 9)
+    fo = O.Fla(O.Lattice(L), fat, lng)
+    fla = q.create_L_from_raw(fat, lng)
+    src = LT.gaussian_vector(L, 330)
+    srcs = [LT.gaussian_vector(L, 340 + s) for s in range(4)]
+    ms = [[0.03], [0.05], [0.03], [0.1]]
+    assert q.set_opts(hop_kernel=-2) != 0 and q.set_opts(batch_kernel=-3) != 0
+    try:
+        assert q.set_opts(prec_sloppy=16, hop_kernel=25, batch_kernel=-1) == 0
+        ref_it = _single_iters(q, fla, src, 0.03, L)[1]
+        info, ras, _ = _run_multi(q, fla, ms, srcs, 1e-20)
+        ref_b = [r[0].final_iter for r in ras]
+        assert q.set_opts(hop_kernel=-1, batch_kernel=-2) == 0
+        runs = []
+        for _ in range(2):
+            st, it, got = _single_iters(q, fla, src, 0.03, L)
+            assert st == 0 and eo_residual(fo, 0.03, got, src, L, 0) <= 1.05e-20
+            info, ras, outs = _run_multi(q, fla, ms, srcs, 1e-20)
+            assert info.status == 0
+            for s in range(4):
+                assert eo_residual(fo, ms[s][0], outs[s][0], srcs[s], L, 0) <= 1.05e-20, s
+            runs.append((it, [r[0].final_iter for r in ras]))
+        assert runs[0] == runs[1]
+        assert abs(runs[0][0] - ref_it) <= 0.03 * ref_it + 3, (runs, ref_it)
+        assert all(abs(a - b) <= 0.03 * b + 3 for a, b in zip(runs[0][1], ref_b)), (runs, ref_b)
+    finally:
+        assert q.set_opts(prec_sloppy=64, hop_kernel=25, batch_kernel=-1) == 0
+        q.destroy_L(fla)
+
+
 @pytest.mark.parametrize("L", [(6, 6, 6, 6), (4, 6, 4, 10)])
 def test_mixed_ragged_site_blocks(L):
     """Lattices whose sites per parity are not a multiple of the 128-site
