@@ -367,7 +367,12 @@ struct BatchEngine::Impl {
   double *part = nullptr;
   unsigned *count = nullptr;
   MixState *dst = nullptr;
-  std::vector<MixState> h;   // host copy of the per-slot solver state
+  MixState *h = nullptr;     // host copy of the per-slot solver state (pinned: source of the uploads)
+  MixState *hd = nullptr;    // pinned landing buffer of the download after a chunk
+  cudaStream_t own = nullptr;
+  bool inflight = false;     // a chunk was launched and not yet collected
+  int launched_n = 0;
+  std::vector<int> recs;
   struct Sys {
     bool busy = false;
     c2<double> *x = nullptr;
@@ -382,8 +387,14 @@ struct BatchEngine::Impl {
     return std::max<size_t>((size_t)(cap + 15) * nsb, (size_t)cap * gridv);
   }
   void release_all() {
+    if (own) cudaStreamSynchronize(own);   // nothing of ours in flight when the memory goes back
     dfree(rs); dfree(ps); dfree(Aps); dfree(ts); dfree(xs); dfree(r); dfree(Ax); dfree(tmp);
     dfree(part); dfree(count); dfree(dst);
+    if (h) cudaFreeHost(h);
+    if (hd) cudaFreeHost(hd);
+    if (own) cudaStreamDestroy(own);
+    h = hd = nullptr;
+    own = nullptr;
   }
   void check_current() const {
     if (ctx().lat != lat) fail(QOP_FAIL, "batched solver: its lattice %d is not the current one", lat);
@@ -403,7 +414,7 @@ size_t BatchEngine::bytes(const Geom &g, int cap) {
          sizeof(double) * Impl::npart(cap, nsb, gridv) + (sizeof(unsigned) + sizeof(MixState)) * cap;
 }
 
-BatchEngine::BatchEngine(FlaT<double> *f, int eo, int cap) : d(new Impl()) {
+BatchEngine::BatchEngine(FlaT<double> *f, int eo, int cap, bool own_stream) : d(new Impl()) {
   Impl &e = *d;
   Context &c = ctx();
   const Geom &g = c.g;
@@ -421,10 +432,14 @@ BatchEngine::BatchEngine(FlaT<double> *f, int eo, int cap) : d(new Impl()) {
   e.ng.str[3] = 1; e.ng.str[2] = g.L[3]; e.ng.str[1] = g.L[2] * g.L[3]; e.ng.str[0] = g.L[1] * g.L[2] * g.L[3];
   e.nsb = (int)((e.Vh + QB - 1) / QB);
   e.gridv = grid_for(e.Vh, 256);
-  e.h.assign(cap, MixState{});
-  for (auto &s : e.h) s.flag = MIX_DONE;   // free slots are skipped by every kernel
   e.sys.assign(cap, Impl::Sys{});
   try {
+    QCHECK(cudaMallocHost(&e.h, sizeof(MixState) * cap));
+    QCHECK(cudaMallocHost(&e.hd, sizeof(MixState) * cap));
+    for (int j = 0; j < cap; j++) {
+      e.h[j] = MixState{};
+      e.h[j].flag = MIX_DONE;   // free slots are skipped by every kernel
+    }
     sloppy_get(f, LK_Q16);   // the int16 link copy, built on first use
     const i64 Vh = e.Vh;
     e.rs = dalloc<uint4>(cap * Vh);
@@ -440,6 +455,10 @@ BatchEngine::BatchEngine(FlaT<double> *f, int eo, int cap) : d(new Impl()) {
     e.count = dalloc<unsigned>(cap);
     dzero(e.count, sizeof(unsigned) * cap);
     e.dst = dalloc<MixState>(cap);
+    // the allocations and the link copy are complete before any other
+    // stream uses them
+    sync();
+    if (own_stream) QCHECK(cudaStreamCreateWithFlags(&e.own, cudaStreamNonBlocking));
   } catch (...) {
     e.release_all();
     delete d;
@@ -453,6 +472,7 @@ BatchEngine::~BatchEngine() {
 }
 
 int BatchEngine::cap() const { return d->cap; }
+cudaStream_t BatchEngine::stream() const { return d->own ? d->own : ctx().s; }
 int BatchEngine::busy() const {
   int n = 0;
   for (const auto &y : d->sys) n += y.busy;
@@ -481,9 +501,12 @@ void BatchEngine::release(int s) {
 void BatchEngine::start(int s, c2<double> *x, const c2<double> *b, double mass, double rsqmin, int max_iter,
                         bool x_zero) {
   Impl &e = *d;
+  StreamScope ss(e.own);
   Context &c = ctx();
   e.check_current();
   if (s < 0 || s >= e.cap || e.sys[s].busy) fail(QOP_FAIL, "batched solver: slot %d is not free", s);
+  if (e.inflight) fail(QOP_FAIL, "batched solver: a chunk is in flight");
+  sync();   // the last upload of the slot states has read them
   const i64 Vh = e.Vh;
   Impl::Sys &y = e.sys[s];
   y = Impl::Sys{};
@@ -514,28 +537,33 @@ void BatchEngine::start(int s, c2<double> *x, const c2<double> *b, double mass, 
 }
 
 std::vector<int> BatchEngine::step() {
+  launch();
+  return collect();
+}
+
+void BatchEngine::launch() {
   Impl &e = *d;
+  StreamScope ss(e.own);
   Context &c = ctx();
   e.check_current();
+  if (e.inflight) fail(QOP_FAIL, "batched solver: a chunk is in flight");
   const Geom &g = c.g;
   const i64 Vh = e.Vh;
   const int eo = e.eo, p = eo, q = 1 - eo;
-  std::vector<int> fin;
-  fin.swap(e.done_now);
   int n = 0, active = 0;   // launches cover slots 0 .. n-1
   for (int j = 0; j < e.cap; j++)
     if (e.sys[j].busy) {
       n = j + 1;
       active += e.h[j].flag != MIX_DONE;
     }
-  if (active == 0) return fin;
+  if (active == 0) return;
   SloppyLinks *sl = sloppy_get(e.f, LK_Q16);
   const LinksSloppy lk_p = links_parity(sl, LK_Q16, p), lk_q = links_parity(sl, LK_Q16, q);
   const int nl = sl->nl;
   const bool recon = sl->recon != 0;
   const float c_long = (float)sl->c_long;
   const int nsb = e.nsb, gridv = e.gridv;
-  QCHECK(cudaMemcpyAsync(e.dst, e.h.data(), sizeof(MixState) * n, cudaMemcpyHostToDevice, c.s));
+  QCHECK(cudaMemcpyAsync(e.dst, e.h, sizeof(MixState) * n, cudaMemcpyHostToDevice, c.s));
   // by default 8 systems per thread when they fill whole groups of 8 (16
   // sources at 32^4: 531 us per hop against 574 with 4), else 4 (12 masses
   // at 24^3x48: 1696 ms per call against 1989 ms with groups of 8 and 4);
@@ -585,9 +613,28 @@ std::vector<int> BatchEngine::step() {
     k_bp<<<dim3(gridv, n), 256, 0, c.s>>>(e.ps, e.rs, Vh, e.dst);
     QLAUNCHN(4);
   }
-  std::vector<MixState> &h = e.h;
-  QCHECK(cudaMemcpyAsync(h.data(), e.dst, sizeof(MixState) * n, cudaMemcpyDeviceToHost, c.s));
+  QCHECK(cudaMemcpyAsync(e.hd, e.dst, sizeof(MixState) * n, cudaMemcpyDeviceToHost, c.s));
+  e.recs.swap(recs);
+  e.launched_n = n;
+  e.inflight = true;
+}
+
+std::vector<int> BatchEngine::collect() {
+  Impl &e = *d;
+  StreamScope ss(e.own);
+  Context &c = ctx();
+  e.check_current();
+  std::vector<int> fin;
+  fin.swap(e.done_now);
+  if (!e.inflight) return fin;
+  e.inflight = false;
+  const i64 Vh = e.Vh;
+  const int n = e.launched_n, gridv = e.gridv;
+  std::vector<int> recs;
+  recs.swap(e.recs);
   sync();
+  memcpy(e.h, e.hd, sizeof(MixState) * n);   // the states after the chunk
+  MixState *h = e.h;
   // drop timing records of hops that found every system idle
   int most = 0;
   for (int j = 0; j < n; j++)
@@ -629,7 +676,7 @@ std::vector<int> BatchEngine::step() {
       pupd.push_back(j);
     }
   }
-  QCHECK(cudaMemcpyAsync(e.dst, h.data(), sizeof(MixState) * n, cudaMemcpyHostToDevice, c.s));
+  QCHECK(cudaMemcpyAsync(e.dst, h, sizeof(MixState) * n, cudaMemcpyHostToDevice, c.s));
   for (int j : pupd) {
     k_bp<<<dim3(gridv, 1), 256, 0, c.s>>>(e.ps + j * Vh, e.rs + j * Vh, Vh, e.dst + j);
     QLAUNCH();

@@ -6,10 +6,12 @@
 // arrives while others are on the GPU joins their hop launches at once
 // instead of waiting for their batch to finish.  A step advances every
 // running system of one engine by a chunk of iterations plus its reliable
-// updates; the worker steps the engines in turn, so requests on different
-// lattices or handles share the device chunk by chunk.  Results are written
-// back in the QOP raw layout with the QOP_asqtad_invert normalisation
-// (m A^-1 b) as each system finishes.
+// updates.  Each engine runs on a stream of its own and the worker launches
+// the chunks of all engines with work before it collects any, so requests
+// on different lattices or handles run on the device side by side.  Results
+// are written
+// back in the QOP raw layout with the QOP_asqtad_invert normalisation (m
+// A^-1 b) as each system finishes.
 //
 // Option serve_policy 1 steps only the engine holding the oldest request
 // (requests still join any engine's free slots): first-come first-served
@@ -85,6 +87,20 @@ struct Lane {
 
 constexpr size_t HBM_RESERVE = size_t(2) << 30;   // left free when other engines run
 
+// free device memory, counting what the stream-ordered pool holds unused
+size_t free_hbm() {
+  size_t fr = 0, tot = 0;
+  if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) { cudaGetLastError(); return 0; }
+  cudaMemPool_t pool;
+  uint64_t reserved = 0, used = 0;
+  if (cudaDeviceGetDefaultMemPool(&pool, ctx().device) == cudaSuccess &&
+      cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) == cudaSuccess &&
+      cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess && reserved > used)
+    fr += (size_t)(reserved - used);
+  cudaGetLastError();
+  return fr;
+}
+
 void finish(Job *j, int status) {
   Service &S = g_srv;
   {
@@ -116,18 +132,17 @@ struct Worker {
   Lane *create(const QOPB_request_t &r) {
     const Geom &g = ctx().g;
     const size_t need = BatchEngine::bytes(g, BATCH_MAX) + 2 * sizeof(c2<double>) * vec_elems(g) * BATCH_MAX;
-    size_t fr = 0, tot = 0;
-    if (any_running() && cudaMemGetInfo(&fr, &tot) == cudaSuccess && fr < need + HBM_RESERVE) return nullptr;
-    cudaGetLastError();
+    if (any_running() && free_hbm() < need + HBM_RESERVE) return nullptr;
     auto l = std::make_unique<Lane>();
     l->lattice = r.lattice;
     l->eo = r.evenodd;
     l->links = r.links;
-    l->eng = std::make_unique<BatchEngine>(reinterpret_cast<FlaT<double> *>(r.links), r.evenodd, BATCH_MAX);
+    l->eng = std::make_unique<BatchEngine>(reinterpret_cast<FlaT<double> *>(r.links), r.evenodd, BATCH_MAX, true);
     for (int s = 0; s < BATCH_MAX; s++) {
       l->x.push_back(dalloc<c2<double>>(vec_elems(g)));
       l->b.push_back(dalloc<c2<double>>(vec_elems(g)));
     }
+    sync();   // allocated before the engine's stream uses them
     l->occ.assign(BATCH_MAX, Lane::Occ{});
     lanes.push_back(std::move(l));
     return lanes.back().get();
@@ -171,6 +186,7 @@ struct Worker {
         j->t_start = now_ms();
         j->left = r.nrhs;
         starting = true;
+        StreamScope ss(l->eng->stream());
         for (int k = 0; k < r.nrhs; k++) {
           const int s = l->eng->free_slot();
           dzero(l->b[s], sizeof(c2<double>) * vec_elems(g));
@@ -217,24 +233,38 @@ struct Worker {
   }
 
   // one step of every engine with work (policy 1: of the engine holding the
-  // oldest request, and of engines with nothing left to iterate); results
-  // of finished systems
+  // oldest request, and of engines with nothing left to iterate): every
+  // engine's chunk is launched on its own stream before any is collected,
+  // so the chunks of different lattices run side by side; then results of
+  // finished systems
   void step_all() {
     const Lane *first = nullptr;
     if (ctx().opt.serve_policy == 1)
       for (auto &l : lanes)
         if (l->eng->running() > 0 && (!first || oldest(l.get()) < oldest(first))) first = l.get();
-    for (size_t li = 0; li < lanes.size(); li++) {
-      Lane *l = lanes[li].get();
-      if (l->eng->busy() == 0) continue;
-      if (first && l != first && l->eng->running() > 0) continue;
+    std::vector<Lane *> go;
+    for (auto &l : lanes)
+      if (l->eng->busy() > 0 && !(first && l.get() != first && l->eng->running() > 0)) go.push_back(l.get());
+    std::vector<Lane *> launched;
+    for (Lane *l : go) {
+      try {
+        if (QOPB_lattice_use(l->lattice) != 0) fail(QOP_FAIL, "serve: unknown lattice %d", l->lattice);
+        l->eng->launch();
+        launched.push_back(l);
+      } catch (Fail &e) {
+        fprintf(stderr, "QOPB serve: %s\n", e.msg.c_str());
+        drop(l, e.status);
+      }
+    }
+    for (Lane *l : launched) {
       std::vector<Job *> ended;
       try {
         if (QOPB_lattice_use(l->lattice) != 0) fail(QOP_FAIL, "serve: unknown lattice %d", l->lattice);
-        const std::vector<int> fin = l->eng->step();
+        const std::vector<int> fin = l->eng->collect();
         const int nb = l->eng->busy();
         for (auto &o : l->occ)
           if (o.job) o.job->batch = std::max(o.job->batch, nb);
+        StreamScope ss(l->eng->stream());
         for (int s : fin) {
           Lane::Occ &o = l->occ[s];
           Job *j = o.job;
@@ -251,7 +281,6 @@ struct Worker {
         fprintf(stderr, "QOPB serve: %s\n", e.msg.c_str());
         for (Job *j : ended) finish(j, QOP_SUCCESS);
         drop(l, e.status);
-        li--;
         continue;
       }
       for (Job *j : ended) finish(j, QOP_SUCCESS);

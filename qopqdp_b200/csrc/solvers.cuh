@@ -56,6 +56,17 @@ constexpr int BATCH_MAX = 16;
 void run_batch(FlaT<double> *f, int eo, int n, const double *mass, c2<double> **x, c2<double> *const *b,
                const double *rsqmin, int max_iter, int *iters, double *final_rsq);
 
+// makes s the library stream while in scope (nullptr: no change)
+struct StreamScope {
+  cudaStream_t old;
+  explicit StreamScope(cudaStream_t s) : old(ctx().s) {
+    if (s) ctx().s = s;
+  }
+  ~StreamScope() { ctx().s = old; }
+  StreamScope(const StreamScope &) = delete;
+  StreamScope &operator=(const StreamScope &) = delete;
+};
+
 // The solver of run_batch as a set of `cap` slots on one link handle and
 // parity of the current lattice that systems enter and leave between steps
 // (continuous batching): a system started while others are in flight joins
@@ -64,7 +75,9 @@ void run_batch(FlaT<double> *f, int eo, int n, const double *mass, c2<double> **
 // the same iterations and reaches the same solution alone or in a mix.
 class BatchEngine {
  public:
-  BatchEngine(FlaT<double> *f, int eo, int cap);
+  // own_stream: the engine's work runs on a stream of its own, so that the
+  // chunks of several engines launched before any is collected overlap
+  BatchEngine(FlaT<double> *f, int eo, int cap, bool own_stream = false);
   ~BatchEngine();
   BatchEngine(const BatchEngine &) = delete;
   BatchEngine &operator=(const BatchEngine &) = delete;
@@ -81,6 +94,12 @@ class BatchEngine {
   // one chunk of iterations of every running system, then their reliable
   // updates; returns the slots whose systems finished (x holds the solution)
   std::vector<int> step();
+  // step() in two halves: launch() enqueues the chunk and returns at once;
+  // collect() waits for it and serves the reliable updates.  Between the two
+  // no slot may be started or released.
+  void launch();
+  std::vector<int> collect();
+  cudaStream_t stream() const;   // the engine's stream (the library stream without own_stream)
   int iters(int s) const;         // hop pairs plus reliable updates
   double final_rsq(int s) const;  // FP64 |r|^2 / |b|^2
   void release(int s);
