@@ -298,6 +298,8 @@ QOP_status_t QOP_asqtad_invert_set_opts(QOP_opt_t opts[], int nopts) {
       n.multi_shift = v != 0;
     } else if (!strcmp(t, "fuse_update")) {
       n.fuse_update = v != 0;
+    } else if (!strcmp(t, "pdl")) {
+      n.pdl = v != 0;
     } else if (!strcmp(t, "serve_policy")) {
       if (v != 0 && v != 1) return QOP_FAIL;
       n.serve_policy = (int)v;

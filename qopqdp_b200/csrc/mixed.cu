@@ -140,6 +140,31 @@ k_mix_p(typename Sp::elem *__restrict__ p, const typename Sp::elem *__restrict__
   Sp::store(p, i, Vh, pv);
 }
 
+// Programmatic dependent launch (option pdl): a kernel launched with the
+// attribute may be scheduled while the kernel ahead of it in the stream
+// drains; griddepcontrol.wait holds it until that kernel has completed and
+// its memory is visible.  Without the attribute the wait returns at once.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+static void launch_k(bool pdl, void (*k)(KArgs...), dim3 grid, dim3 block, cudaStream_t s, Args... args) {
+  if (!pdl) {
+    k<<<grid, block, 0, s>>>(args...);
+    return;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  QCHECK(cudaLaunchKernelEx(&cfg, k, args...));
+}
+
 // x += alpha p, r -= alpha Ap and p = r + beta p in one pass (fused update:
 // the scalars come from the KIND 3 hop).  Runs only for the iteration whose
 // hop recorded `seq` in tok; when that hop set MIX_UPDATE, p is left to the
@@ -148,6 +173,7 @@ template <class Sp>
 __global__ void __launch_bounds__(256)
 k_mix_update_p(float2 *__restrict__ xs, typename Sp::elem *__restrict__ r, typename Sp::elem *__restrict__ p,
                const typename Sp::elem *__restrict__ Ap, i64 Vh, const MixState *st, int seq) {
+  pdl_wait();
   if (st->tok != seq) return;
   const int fl = st->flag;
   if (fl != MIX_RUN && fl != MIX_UPDATE) return;
@@ -750,6 +776,7 @@ k_mix_hop_q16r(uint4 *__restrict__ out, const uint4 *__restrict__ src, const uns
                const uint4 *__restrict__ same, Geom g, NbrGeom ng, int p, MixState *st, double *part,
                unsigned *count, float c_long, const uint4 *__restrict__ rres = nullptr, int seq = 0,
                DdQ16Ghost gh = DdQ16Ghost()) {
+  if constexpr (PK) pdl_wait();   // the packed variants may be launched as dependents
   if (st->flag) return;
   const int tid = threadIdx.x;
   const i64 Vh = g.Vh;
@@ -964,15 +991,15 @@ static void launch_q16_dd(int kind, int nl, bool recon, float c_long, int grid, 
 // KIND 3 hops (fused update) exist for the persistent packed variants 20-26
 static void launch_q16_fused(int variant, int nl, bool recon, float c_long, int grid, uint4 *out, const uint4 *src,
                              const unsigned char *lk, const uint4 *same, const Geom &g, const NbrGeom &ng, int par,
-                             MixState *st, const uint4 *rres, int seq) {
+                             MixState *st, const uint4 *rres, int seq, bool pdl = false) {
   Context &c = ctx();
-#define Q16_ARGS3 out, src, lk, same, g, ng, par, st, c.d_part, c.d_count, c_long, rres, seq
+#define Q16_ARGS3 out, src, lk, same, g, ng, par, st, c.d_part, c.d_count, c_long, rres, seq, DdQ16Ghost()
 #define Q16RPK3(B, M)                                                                                          \
   do {                                                                                                         \
     const int gp = std::min(grid, (c.red_blocks / 8) * M);                                                     \
-    if (nl != 16) k_mix_hop_q16r<8, 3, B, false, M, true, true><<<gp, QB, 0, c.s>>>(Q16_ARGS3);               \
-    else if (recon) k_mix_hop_q16r<16, 3, B, true, M, true, true><<<gp, QB, 0, c.s>>>(Q16_ARGS3);             \
-    else k_mix_hop_q16r<16, 3, B, false, M, true, true><<<gp, QB, 0, c.s>>>(Q16_ARGS3);                       \
+    if (nl != 16) launch_k(pdl, k_mix_hop_q16r<8, 3, B, false, M, true, true>, gp, QB, c.s, Q16_ARGS3);       \
+    else if (recon) launch_k(pdl, k_mix_hop_q16r<16, 3, B, true, M, true, true>, gp, QB, c.s, Q16_ARGS3);     \
+    else launch_k(pdl, k_mix_hop_q16r<16, 3, B, false, M, true, true>, gp, QB, c.s, Q16_ARGS3);               \
   } while (0)
   switch (variant) {
     case 20: Q16RPK3(2, 6); break;
@@ -992,7 +1019,7 @@ static void launch_q16_fused(int variant, int nl, bool recon, float c_long, int 
 template <int KIND>
 static void launch_q16(int variant, int nl, bool recon, float c_long, int grid, uint4 *out, const uint4 *src,
                        const unsigned char *lk, const uint4 *same, const Geom &g, const NbrGeom &ng, int par,
-                       MixState *st) {
+                       MixState *st, bool pdl = false) {
   Context &c = ctx();
 #define Q16_ARGS out, src, lk, same, g, ng, par, st, c.d_part, c.d_count
 #define Q16R(NLV, B)                                                                        \
@@ -1013,12 +1040,13 @@ static void launch_q16(int variant, int nl, bool recon, float c_long, int grid, 
     else if (recon) k_mix_hop_q16r<16, KIND, B, true, M, true><<<gp, QB, 0, c.s>>>(Q16_ARGS, c_long);    \
     else k_mix_hop_q16r<16, KIND, B, false, M, true><<<gp, QB, 0, c.s>>>(Q16_ARGS, c_long);              \
   } while (0)
+#define Q16PK_TAIL c_long, (const uint4 *)nullptr, 0, DdQ16Ghost()
 #define Q16RPK(B, M)                                                                                           \
   do {                                                                                                         \
     const int gp = std::min(grid, (c.red_blocks / 8) * M);                                                     \
-    if (nl != 16) k_mix_hop_q16r<8, KIND, B, false, M, true, true><<<gp, QB, 0, c.s>>>(Q16_ARGS, c_long);     \
-    else if (recon) k_mix_hop_q16r<16, KIND, B, true, M, true, true><<<gp, QB, 0, c.s>>>(Q16_ARGS, c_long);   \
-    else k_mix_hop_q16r<16, KIND, B, false, M, true, true><<<gp, QB, 0, c.s>>>(Q16_ARGS, c_long);             \
+    if (nl != 16) launch_k(pdl, k_mix_hop_q16r<8, KIND, B, false, M, true, true>, gp, QB, c.s, Q16_ARGS, Q16PK_TAIL);   \
+    else if (recon) launch_k(pdl, k_mix_hop_q16r<16, KIND, B, true, M, true, true>, gp, QB, c.s, Q16_ARGS, Q16PK_TAIL); \
+    else launch_k(pdl, k_mix_hop_q16r<16, KIND, B, false, M, true, true>, gp, QB, c.s, Q16_ARGS, Q16PK_TAIL);           \
   } while (0)
 #define Q16A(RR, M)                                                                                       \
   do {                                                                                                    \
@@ -1074,6 +1102,8 @@ static void launch_q16(int variant, int nl, bool recon, float c_long, int grid, 
       break;
   }
 #undef Q16A
+#undef Q16RPK
+#undef Q16PK_TAIL
 #undef Q16RP
 #undef Q16RM
 #undef Q16R
@@ -1204,6 +1234,8 @@ static void run_mixed(LinOp<double> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t *r
     }
   }
   const bool fuse = q16v && ns == 1 && c.opt.fuse_update && hk >= 20;
+  // the three kernels of the fused iteration as programmatic dependents
+  const bool pdl = fuse && c.opt.pdl;
   int seq = 0;
   // a decomposed lattice: halos before each hop, the reductions summed over
   // the processes before the scalars (the fused int16 iteration only)
@@ -1245,7 +1277,7 @@ static void run_mixed(LinOp<double> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t *r
         ProfScope ps1(hname, hop_bytes);
         if constexpr (std::is_same<Lk, LkQ16B>::value) {
           const unsigned char *lq = (const unsigned char *)lk_q.a;
-          launch_q16<1>(hk, nl, recon, c_long, gridq, ts, ps, lq, nullptr, g, ng, q, dst);
+          launch_q16<1>(hk, nl, recon, c_long, gridq, ts, ps, lq, nullptr, g, ng, q, dst, pdl);
         } else {
           if (nl == 16) k_mix_hop<Sp, Lk, 16, 1><<<gridh, 128, 0, c.s>>>(ts, ps, lk_q, nullptr, g, q, dst, c.d_part, c.d_count);
           else k_mix_hop<Sp, Lk, 8, 1><<<gridh, 128, 0, c.s>>>(ts, ps, lk_q, nullptr, g, q, dst, c.d_part, c.d_count);
@@ -1256,7 +1288,7 @@ static void run_mixed(LinOp<double> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t *r
         ProfScope ps2(fuse ? hname3 : hname, hop_bytes + (double)Vh * Sp::site_bytes * (fuse ? 2 : 1));
         if constexpr (q16v) {
           const unsigned char *lp = (const unsigned char *)lk_p.a;
-          if (fuse) launch_q16_fused(hk, nl, recon, c_long, gridq, Aps, ts, lp, ps, g, ng, p, dst, rs, ++seq);
+          if (fuse) launch_q16_fused(hk, nl, recon, c_long, gridq, Aps, ts, lp, ps, g, ng, p, dst, rs, ++seq, pdl);
           else launch_q16<2>(hk, nl, recon, c_long, gridq, Aps, ts, lp, ps, g, ng, p, dst);
         } else if constexpr (std::is_same<Lk, LkQ16B>::value) {
           const unsigned char *lp = (const unsigned char *)lk_p.a;
@@ -1272,7 +1304,7 @@ static void run_mixed(LinOp<double> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t *r
         k_ms_p<Sp><<<gridv, 256, 0, c.s>>>(ps, rs, Vh, dst, dsh, ns, mv);
         QLAUNCHN(4);
       } else if (fuse) {
-        k_mix_update_p<Sp><<<gridv, 256, 0, c.s>>>(xs, rs, ps, Aps, Vh, dst, seq);
+        launch_k(pdl, k_mix_update_p<Sp>, gridv, 256, c.s, xs, rs, ps, (const E *)Aps, Vh, (const MixState *)dst, seq);
         QLAUNCHN(3);
       } else {
         k_mix_update<Sp><<<gridv, 256, 0, c.s>>>(xs, rs, ps, Aps, Vh, dst, c.d_part, c.d_count);

@@ -288,6 +288,32 @@ def test_fused_update_solves_like_the_four_kernel_iteration():
         q.destroy_L(fla)
 
 
+def test_programmatic_dependent_launch_solves_like_the_default():
+    """Option pdl: the three kernels of the fused int16 iteration launched
+    as programmatic dependents (each waits in griddepcontrol.wait for the one
+    ahead of it) compute exactly what the ordinary launches compute: the
+    same iteration count and the same solution, bit for bit."""
+    L = (8, 8, 8, 8)
+    q = gpu_lattice(L, "D")
+    fat, lng, _, _ = hisq_links(L, 0.5, 9)
+    fo = O.Fla(O.Lattice(L), fat, lng)
+    fla = q.create_L_from_raw(fat, lng)
+    src = LT.gaussian_vector(L, 331)
+    try:
+        out = {}
+        for pdl in (0, 1, 0, 1):
+            assert q.set_opts(prec_sloppy=16, hop_kernel=25, fuse_update=1, pdl=pdl) == 0
+            st, it, got = _single_iters(q, fla, src, 0.03, L)
+            assert st == 0 and eo_residual(fo, 0.03, got, src, L, 0) <= 1.05e-20
+            if pdl in out:
+                assert it == out[pdl][0] and np.array_equal(got, out[pdl][1])
+            out[pdl] = (it, got)
+        assert out[1][0] == out[0][0] and np.array_equal(out[1][1], out[0][1])
+    finally:
+        assert q.set_opts(prec_sloppy=64, pdl=1) == 0
+        q.destroy_L(fla)
+
+
 def test_every_batch_kernel_variant():
     """Each selectable batched hop (option batch_kernel 0-15) solves a
     four-source batch to the FP64 target with the iteration counts of the
