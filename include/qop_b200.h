@@ -40,18 +40,19 @@ unsigned long long QOPB_launch_count(void);
 
 /* QOP_D3_asqtad_ddagd_norm2 without any device allocation (no counterpart
    in the reference).  For callers that cannot allocate device memory where
-   they apply the operator: code recorded into a CUDA graph (allocation is
-   not allowed during stream capture), programs whose own allocator has
-   reserved the device memory, and loops that must not wait on an
-   allocator.  It computes out = m^2 in - D_eo,oe D_oe,eo in on parity eo
-   (QOP_EVEN or QOP_ODD) and returns |D_oe in|^2 + m^2 |in|^2, like the
-   regular entry point.  Its scratch is a fixed array inside the library
-   (about 3.2 MB, held on every GPU that loads the library until exit), so
-   lattices with more than 65536 sites per parity are rejected with
-   info->status = QOP_FAIL and a return value of -1.  The first call on a
-   device looks up that array's device address; make that first call before
-   any stream capture.  All calls share the array: calls that overlap on the
-   GPU race and must be serialised by the caller. */
+   they apply the operator: applications whose own caching allocator has
+   reserved nearly all of the GPU's memory (a cudaMalloc from this library
+   would fail there), and loops that must not wait on an allocator.  It
+   computes out = m^2 in - D_eo,oe D_oe,eo in on parity eo (QOP_EVEN or
+   QOP_ODD) and returns |D_oe in|^2 + m^2 |in|^2, like the regular entry
+   point; the handles must be live handles of the current lattice.  Its
+   scratch is a fixed array inside the library (about 3.2 MB, held on every
+   GPU that loads the library until exit), so lattices with more than 65536
+   sites per parity are rejected with info->status = QOP_FAIL and a return
+   value of -1.  The call is synchronous (it returns the norm to the host).
+   The first call on a device looks up that array's device address under a
+   lock.  All calls share the array: calls that overlap on the GPU race and
+   must be serialised by the caller. */
 double QOPB_D3_asqtad_ddagd_norm2_noalloc(QOP_info_t *info, QOP_D3_FermionLinksAsqtad *asqtad, double mass,
                                           QOP_D3_ColorVector *out, QOP_D3_ColorVector *in, QOP_evenodd_t eo);
 

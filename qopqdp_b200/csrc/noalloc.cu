@@ -1,13 +1,16 @@
 // noalloc.cu -- QOPB_D3_asqtad_ddagd_norm2_noalloc: the normal-equation
 // operator A = m^2 - D_eo D_oe with |D_oe in|^2 + m^2 |in|^2, computed
-// without any device allocation.
+// without any device allocation.  It has no counterpart in the reference.
 //
 // Who needs it: callers that cannot allocate device memory at the point
-// where they apply the operator -- code recording the call into a CUDA graph
-// (an allocation inside a stream capture is not allowed), applications whose
-// own caching allocator has reserved the device memory up front, and
-// latency-critical loops that must not wait on the allocator.  The regular
-// QOP_D3_asqtad_ddagd_norm2 allocates a temporary vector per call.
+// where they apply the operator.  Applications with their own caching
+// allocator (a lattice code's memory manager, a framework's pool) often
+// reserve nearly all of the GPU's memory up front, so a cudaMalloc from this
+// library fails there even though the application has room; and inner loops
+// that must not stall on the allocator (cudaMalloc and a first-fit pool
+// growth can synchronise the device) want the operator with no allocation at
+// all.  The regular QOP_D3_asqtad_ddagd_norm2 allocates a temporary parity
+// vector per call.
 //
 // Scratch: one file-scope __device__ array of NOALLOC_MAX_VH * 48 bytes plus
 // the reduction partials, the completion ticket and two result doubles
@@ -16,7 +19,14 @@
 // Every call shares the array and leaves its contents behind; the ticket is
 // cleared at the start of each call.  Calls that overlap on the GPU (for
 // example from several host threads or streams) race on the array.
+//
+// The first call on a device looks up the array's device address (the host
+// symbol is only a stand-in) with that device current; the lookup is
+// guarded by a lock, so first calls from several host threads are safe.  The
+// call is synchronous: it waits on the library stream and returns the norm
+// to the host.
 #include "qopb.h"
+#include <mutex>
 
 namespace qopb {
 
@@ -30,11 +40,13 @@ static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_DOUBLES];
 // device address of the scratch array, looked up once per device with that
 // device current (the host-side symbol is only a stand-in, not an address)
 static double *g_scratch_dev[64];
+static std::mutex g_scratch_mu;
 
 static double *scratch_for_current_device() {
   int dev = 0;
   QCHECK(cudaGetDevice(&dev));
   if (dev < 0 || dev >= 64) fail(QOP_FAIL, "noalloc: device ordinal %d out of range", dev);
+  std::lock_guard<std::mutex> lk(g_scratch_mu);
   if (!g_scratch_dev[dev]) {
     void *p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
@@ -57,9 +69,13 @@ extern "C" double QOPB_D3_asqtad_ddagd_norm2_noalloc(QOP_info_t *info, QOP_D3_Fe
   try {
     require_init("QOPB_D3_asqtad_ddagd_norm2_noalloc");
     dd_refuse("QOPB_D3_asqtad_ddagd_norm2_noalloc");
+    // live handles of the current lattice only: their arrays are indexed
+    // with the current lattice's Vh below
+    handle_check(asqtad, "FermionLinksAsqtad");
+    handle_check(out, "ColorVector");
+    handle_check(in, "ColorVector");
     FlaT<double> *f = reinterpret_cast<FlaT<double> *>(asqtad);
     VecT<double> *o = reinterpret_cast<VecT<double> *>(out), *i = reinterpret_cast<VecT<double> *>(in);
-    if (!f || !o || !i) fail(QOP_FAIL, "QOPB_D3_asqtad_ddagd_norm2_noalloc: NULL handle");
     if (eo != QOP_EVEN && eo != QOP_ODD) fail(QOP_FAIL, "QOPB_D3_asqtad_ddagd_norm2_noalloc: eo must be EVEN or ODD");
     const Geom &g = ctx().g;
     if (g.Vh > NOALLOC_MAX_VH)

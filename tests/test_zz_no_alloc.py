@@ -1,12 +1,15 @@
 """QOPB_D3_asqtad_ddagd_norm2_noalloc through the C ABI.
 
 This entry point serves callers that cannot allocate device memory where
-they apply the operator (a CUDA-graph capture, an application allocator
-owning the device memory, allocation-free inner loops).  Its result must
+they apply the operator: applications whose own caching allocator has
+reserved the GPU's memory up front (a cudaMalloc from this library fails
+there), and loops that must not wait on an allocator.  Its result must
 equal the allocating QOP_D3_asqtad_ddagd_norm2 on two calls in a row (the
-scratch it reuses keeps the previous call's contents), and lattices beyond
-its fixed scratch must be rejected.  Collected last so a failure here cannot
-hide other tests; it also passes when run alone in a fresh process.
+scratch it reuses keeps the previous call's contents), it must allocate
+nothing, it must refuse handles that are dead or belong to another lattice,
+and lattices beyond its fixed scratch must be rejected.  Collected last so
+a failure here cannot hide other tests; it also passes when run alone in a
+fresh process.
 """
 import ctypes as C
 
@@ -20,6 +23,8 @@ from qopqdp_b200.qop import QOP_info_t
 
 pytestmark = pytest.mark.gpu
 
+NOALLOC_MAX_VH = 65536
+
 
 def _fn(q):
     f = q.lib.QOPB_D3_asqtad_ddagd_norm2_noalloc
@@ -28,21 +33,59 @@ def _fn(q):
     return f
 
 
-def test_noalloc_ddagd_norm2_matches_allocating_entry_point():
-    L = (8, 8, 8, 8)
+def _launches(q):
+    q.lib.QOPB_launch_count.restype = C.c_ulonglong
+    return int(q.lib.QOPB_launch_count())
+
+
+class _Memory:
+    """Device memory seen by the driver: the stream-ordered pool's used bytes
+    and their high-water mark (the library allocates its temporaries from
+    that pool), and the device's free memory (plain cudaMalloc)."""
+
+    def __init__(self):
+        from cuda.bindings import driver as d
+        self.d = d
+        assert d.cuInit(0)[0] == d.CUresult.CUDA_SUCCESS
+        err, dev = d.cuCtxGetDevice()
+        assert err == d.CUresult.CUDA_SUCCESS
+        err, self.pool = d.cuDeviceGetDefaultMemPool(dev)
+        assert err == d.CUresult.CUDA_SUCCESS
+
+    def _attr(self, a):
+        err, v = self.d.cuMemPoolGetAttribute(self.pool, a)
+        assert err == self.d.CUresult.CUDA_SUCCESS
+        return int(v)
+
+    def reset_high(self):
+        a = self.d.CUmemPool_attribute.CU_MEMPOOL_ATTR_USED_MEM_HIGH
+        err, = self.d.cuMemPoolSetAttribute(self.pool, a, self.d.cuuint64_t(0))
+        assert err == self.d.CUresult.CUDA_SUCCESS
+
+    def used(self):
+        return self._attr(self.d.CUmemPool_attribute.CU_MEMPOOL_ATTR_USED_MEM_CURRENT)
+
+    def high(self):
+        return self._attr(self.d.CUmemPool_attribute.CU_MEMPOOL_ATTR_USED_MEM_HIGH)
+
+    def free(self):
+        err, free, _ = self.d.cuMemGetInfo()
+        assert err == self.d.CUresult.CUDA_SUCCESS
+        return int(free)
+
+
+def _check_against_allocating(q, L, mass, seed, calls=2):
     V = int(np.prod(L))
-    q = gpu_lattice(L, "D")
     fn = _fn(q)
-    fat, lng = asqtad_links(L, 0.3, 7)
+    fat, lng = asqtad_links(L, 0.3, seed)
     fla = q.create_L_from_raw(fat, lng)
-    mass = 0.05
     for eo in (0, 1):
         src = LT.gaussian_vector(L, 200 + eo)
         hin = q.create_V(src)
         href = q.create_V(np.zeros_like(src))
         n_ref = q.ddagd_norm2(fla, mass, href, hin, eo)
         ref = q.extract_V(href, V)
-        for call in range(2):                       # scratch reused between calls
+        for call in range(calls):                   # scratch reused between calls
             hout = q.create_V(np.zeros_like(src))
             info = QOP_info_t()
             n = fn(C.byref(info), fla, mass, hout, hin, eo)
@@ -53,6 +96,85 @@ def test_noalloc_ddagd_norm2_matches_allocating_entry_point():
             q.destroy_V(hout)
         q.destroy_V(hin)
         q.destroy_V(href)
+    q.destroy_L(fla)
+
+
+def test_noalloc_ddagd_norm2_matches_allocating_entry_point():
+    L = (8, 8, 8, 8)
+    q = gpu_lattice(L, "D")
+    _check_against_allocating(q, L, 0.05, 7)
+
+
+def test_noalloc_at_its_maximum_lattice():
+    L = (16, 16, 16, 32)                             # exactly 65536 sites per parity
+    assert int(np.prod(L)) // 2 == NOALLOC_MAX_VH
+    q = gpu_lattice(L, "D")
+    _check_against_allocating(q, L, 0.1, 11)
+
+
+def test_noalloc_allocates_nothing():
+    L = (8, 8, 8, 8)
+    V = int(np.prod(L))
+    q = gpu_lattice(L, "D")
+    fn = _fn(q)
+    fat, lng = asqtad_links(L, 0.3, 7)
+    fla = q.create_L_from_raw(fat, lng)
+    src = LT.gaussian_vector(L, 300)
+    hin, hout = q.create_V(src), q.create_V(np.zeros_like(src))
+    info = QOP_info_t()
+    assert fn(C.byref(info), fla, 0.05, hout, hin, 0) > 0      # first call: scratch address lookup
+    mem = _Memory()
+    # the measurement sees the allocating entry point's temporary
+    used0 = mem.used()
+    mem.reset_high()
+    q.ddagd_norm2(fla, 0.05, hout, hin, 0)
+    assert mem.high() >= used0 + 3 * 16 * (V // 2), "pool high-water mark missed a temporary vector"
+    # and the no-alloc entry point leaves both the pool and free memory alone
+    used1, free1 = mem.used(), mem.free()
+    mem.reset_high()
+    for _ in range(4):
+        assert fn(C.byref(info), fla, 0.05, hout, hin, 0) > 0 and info.status == 0
+    assert mem.high() == used1 and mem.used() == used1
+    assert mem.free() == free1
+    for h in (hin, hout):
+        q.destroy_V(h)
+    q.destroy_L(fla)
+
+
+def test_noalloc_refuses_foreign_and_dead_handles():
+    L = (8, 8, 8, 8)
+    LB = (4, 4, 4, 8)
+    q = gpu_lattice(L, "D")
+    fn = _fn(q)
+    fat, lng = asqtad_links(L, 0.3, 7)
+    fla = q.create_L_from_raw(fat, lng)
+    src = LT.gaussian_vector(L, 400)
+    hin, hout = q.create_V(src), q.create_V(np.zeros_like(src))
+    # handles made on a second, smaller lattice
+    lb = q.lattice_create(LB)
+    assert lb >= 1 and q.lattice_use(lb) == 0
+    fb, lb_ = asqtad_links(LB, 0.3, 7)
+    fla_b = q.create_L_from_raw(fb, lb_)
+    vb = q.create_V(LT.gaussian_vector(LB, 401))
+    assert q.lattice_use(0) == 0
+    dead = q.create_V(src)
+    q.destroy_V(dead)
+    cases = [(fla_b, hout, hin), (fla, vb, hin), (fla, hout, vb), (fla, hout, dead), (fla, dead, hin), (None, hout, hin)]
+    for args in cases:
+        n0 = _launches(q)
+        info = QOP_info_t()
+        n = fn(C.byref(info), args[0], 0.05, args[1], args[2], 0)
+        assert info.status == 1 and n == -1.0, args
+        assert _launches(q) == n0, "a refused call launched kernels"
+    # the valid handles still work after the refusals
+    info = QOP_info_t()
+    assert fn(C.byref(info), fla, 0.05, hout, hin, 0) > 0 and info.status == 0
+    assert q.lattice_use(lb) == 0
+    q.destroy_L(fla_b)
+    q.destroy_V(vb)
+    assert q.lattice_use(0) == 0
+    for h in (hin, hout):
+        q.destroy_V(h)
     q.destroy_L(fla)
 
 
