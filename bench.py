@@ -47,7 +47,13 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 PEAK_FALLBACK_GBS = 6650.0
-BENCH_ITERS_FILE = os.path.join(ROOT, "profiles", "bench_iterations.json")
+# Iterations of the plain FP64 CG (the reference algorithm) on the headline
+# workload (HISQ 32^3x64, eps 0.5, seed 2024, m 0.01, |r|/|b| <= 1e-10),
+# measured on a B200 with QOP_D3_asqtad_invert at prec_sloppy 64: 5920.
+# The CPU reference arm times a bounded number of oracle CG iterations and
+# scales by this count (a full FP64 CPU solve takes ~6 minutes on 16 host
+# threads); the device arm reports its own FP64 iteration count beside it.
+FP64_ITERS_HEADLINE = 5920
 
 
 def parse():
@@ -65,6 +71,9 @@ def parse():
     ap.add_argument("--ru-delta", type=float, default=0.3, help="reliable-update threshold on |r|")
     ap.add_argument("--fp64-steps", type=int, default=1)
     ap.add_argument("--cpu-iters", type=int, default=12, help="CG iterations timed on the host")
+    ap.add_argument("--ref-iters", type=int, default=None,
+                    help="FP64 CG iterations of one solve, for the reference arm's solves/s (default: the "
+                         "measured count of the headline workload)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--prof-every", type=int, default=8,
                     help="headline solve: bracket every n-th launch of each kernel class with CUDA events")
@@ -102,6 +111,15 @@ def rank_info():
 
 def workload_name(a, L):
     return "hisq_%s_m%g_tol%g_eps%g_seed%d" % ("x".join(map(str, L)), a.mass, a.tol, a.eps, a.seed)
+
+
+def headline_config(a, L, world):
+    """The `config` of the headline line, identical in both arms."""
+    V = int(np.prod(L))
+    return {"workload": workload_name(a, L), "lattice": list(L), "mass": a.mass, "tol": a.tol, "eps": a.eps,
+            "parallelism": "replicas x%d" % world,
+            "l2": ("inputs larger than L2 (links %.2f GB FP64)" if V * 16 * 18 * 8 > 126e6 else
+                   "L2-resident inputs (links %.2f GB FP64)") % (V * 16 * 18 * 8 / 1e9)}
 
 
 def measured_peak():
@@ -202,6 +220,22 @@ def cpu_iteration_time(fat, lng, L, src, mass, iters, threads):
     return dt / max(ra.final_iter, 1), ra.final_iter, O.get_threads()
 
 
+def oracle_true_rsq(fat, lng, L, src, out, mass, threads):
+    """|b - A x|^2 / |b|^2 on the even sites for the solve output out = m A^-1 b
+    (A = m^2 - D_eo D_oe), computed by the oracle in FP64 as the reference's
+    check_resids does (examples/asqtad_test.c:84-130)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.set_threads(threads)
+    fo = O.Fla(O.Lattice(L), fat, lng)
+    V = int(np.prod(L))
+    t = fo.dslash(mass, out, O.EVENODD, O.EVEN)
+    chk = fo.dslash(-mass, t, O.EVEN, O.EVENODD)
+    b = src[: V // 2]
+    r = chk[: V // 2] / mass + b
+    return float((r ** 2).sum() / (b ** 2).sum())
+
+
 def run_reference(a):
     rank, _, world = rank_info()
     if rank != 0:
@@ -218,9 +252,8 @@ def run_reference(a):
     fat, lng, _, _ = lat.hisq_links(LT.hisq_coeff_vector(LT.hisq_bench_coeffs()), U)
     del U
     src = LT.gaussian_vector(L, a.seed)
-    iters_db = json.load(open(BENCH_ITERS_FILE)) if os.path.exists(BENCH_ITERS_FILE) else {}
-    key = workload_name(a, L)
-    n_solve = iters_db.get(key, {}).get("fp64_iters")
+    n_solve = a.ref_iters or (FP64_ITERS_HEADLINE if workload_name(a, L) == workload_name(a, (32, 32, 32, 64))
+                              and (a.mass, a.tol, a.eps, a.seed) == (0.01, 1e-10, 0.5, 2024) else None)
     per = []
     for k in range(a.warmup + a.steps):
         s, it, th = cpu_iteration_time(fat, lng, L, src, a.mass, a.cpu_iters, threads)
@@ -229,18 +262,20 @@ def run_reference(a):
     s_it = float(np.median(per))
     if n_solve:
         value = 1.0 / (s_it * n_solve)
-        sample = ("%d CG iterations of the FP64 reference algorithm per step on %d host threads; solves/s "
-                  "extrapolated with the full solve's %d iterations (FP64 solve of this workload)" %
-                  (a.cpu_iters, th, n_solve))
+        sample = ("%d CG iterations of the FP64 reference algorithm (oracle, C/OpenMP) per step on %d host "
+                  "threads, %.4f s per iteration (median of %d steps); solves/s extrapolated to %d iterations, the "
+                  "FP64 CG iteration count of this workload" % (it, th, s_it, a.steps, n_solve))
     else:
         value = None
-        sample = "%d CG iterations per step; full-solve iteration count not recorded" % a.cpu_iters
+        sample = "%d CG iterations per step; no FP64 iteration count for this workload (--ref-iters)" % a.cpu_iters
     line = {"metric": "mixed-prec CG solves/s @1e-10 (HISQ eo solve)", "value": value, "unit": "solves/s",
             "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
-            "ms_per_step": 1e3 / value if value else None, "higher_is_better": True, "scaling": "weak",
+            "ms_per_step": 1e3 / value if value else None, "ms_per_step_kind": "extrapolated",
+            "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": key, "lattice": L, "mass": a.mass, "tol": a.tol},
+            "config": headline_config(a, L, world),
             "impl": "reference",
+            "measured": {"sec_per_iter": s_it, "iters_per_step": it, "fp64_iters_per_solve": n_solve},
             "cpu_baseline": {"value": value, "unit": "solves/s", "cores": th, "kind": "port", "sample": sample,
                              "sec_per_iter": s_it},
             "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -401,28 +436,25 @@ def run_b200(a):
         roof = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
                 "peak_kind": peak_kind, "kernel": name, "traffic": ncu_traffic(name, L),
                 "bytes_per_launch": b, "sampled_every": a.prof_every}
-    # ---------------- CPU baseline (oracle) on rank 0, N = 1
+    # ---------------- oracle checks and CPU baseline on rank 0 (not timed)
     cpu = None
+    oracle_rsq = None
     n_fp64 = fp64.get("iters")
-    if rank == 0 and world == 1 and not a.no_cpu:
+    if rank == 0 and not a.no_cpu:
         fat, lng = q.extract_L(fla, V)
         threads = os.cpu_count() or 1
-        s_it, nit, th = cpu_iteration_time(fat, lng, L, src, a.mass, a.cpu_iters, threads)
-        n_ref = n_fp64 or int(np.median(iters))
-        cpu = {"value": 1.0 / (s_it * n_ref), "unit": "solves/s", "cores": th, "kind": "port",
-               "sample": "%d CG iterations of the oracle (FP64 reference algorithm, C/OpenMP) on %d host threads, "
-                         "%.3f s/iteration, extrapolated to the %d iterations of the FP64 solve" %
-                         (nit, th, s_it, n_ref), "sec_per_iter": s_it}
+        # the FP64 true residual |b - A x|^2 / |b|^2 of the headline solution,
+        # recomputed by the oracle from the device's links
+        oracle_rsq = oracle_true_rsq(fat, lng, L, src, sol, a.mass, threads)
+        if world == 1:
+            s_it, nit, th = cpu_iteration_time(fat, lng, L, src, a.mass, a.cpu_iters, threads)
+            n_ref = n_fp64 or FP64_ITERS_HEADLINE
+            cpu = {"value": 1.0 / (s_it * n_ref), "unit": "solves/s", "cores": th, "kind": "port",
+                   "sample": "%d CG iterations of the oracle (FP64 reference algorithm, C/OpenMP) on %d host "
+                             "threads, %.4f s/iteration, extrapolated to the %d iterations of the FP64 solve" %
+                             (nit, th, s_it, n_ref), "sec_per_iter": s_it}
         del fat, lng
     if rank == 0:
-        if n_fp64:
-            os.makedirs(os.path.dirname(BENCH_ITERS_FILE), exist_ok=True)
-            db = json.load(open(BENCH_ITERS_FILE)) if os.path.exists(BENCH_ITERS_FILE) else {}
-            db[workload_name(a, L)] = {"fp64_iters": n_fp64, "mixed_iters": int(np.median(iters))}
-            try:
-                json.dump(db, open(BENCH_ITERS_FILE, "w"), indent=1, sort_keys=True)
-            except OSError:
-                pass
         lat_sorted = np.sort(lat_ms)
         line = {
             "metric": "mixed-prec CG solves/s @1e-10 (HISQ eo solve)",
@@ -430,18 +462,22 @@ def run_b200(a):
             "ms_per_step": total_ms / a.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32" if a.prec < 64 else "f64",
             "data": "synthetic",
-            "config": {"workload": workload_name(a, L), "lattice": L, "mass": a.mass, "tol": a.tol,
-                       "eps": a.eps, "precision": ("int16 fixed-point" if a.prec == 16 else "FP%d" % a.prec) + " storage, FP32 arithmetic, FP64 reductions and reliable updates (delta %g)" % a.ru_delta,
-                       "parallelism": "replicas x%d" % world,
-                       "l2": "inputs larger than L2 (links %.1f GB FP64)" % (V * 16 * 18 * 8 / 1e9)},
+            "config": headline_config(a, L, world),
+            "precision": ("int16 fixed-point" if a.prec == 16 else "FP%d" % a.prec) + " storage, FP32 arithmetic, FP64 reductions and reliable updates (delta %g)" % a.ru_delta,
             "p50_ms": float(np.percentile(lat_sorted, 50)), "p99_ms": float(np.percentile(lat_sorted, 99)),
-            "iters": int(np.median(iters)), "final_rsq": float(max(rsqs)),
+            "iters": int(np.median(iters)), "final_rsq": float(max(rsqs)), "oracle_rsq": oracle_rsq,
             "fp64_cg": fp64,
             "speedup_vs_fp64": (value / world) / fp64["solves_per_s"] if fp64 else None,
             "roofline": roof, "kernels": kernels, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": int(n_launch),
             "clocks": clk.summary(), "setup_s": t_setup,
         }
+        # device time x SM clock of the dominant kernel: constant if the
+        # kernel is bound by instruction issue, falling with the clock if
+        # it is bound by HBM
+        mhz = line["clocks"].get("sm_mhz")
+        if roof and mhz:
+            roof["avg_us_x_sm_mhz"] = kernels[roof["kernel"]]["avg_us"] * mhz
         print(json.dumps(line), flush=True)
     q.destroy_V(hin)
     q.destroy_V(hout)

@@ -37,6 +37,10 @@ int QOPB_prof_every(int n);
 
 /* Number of kernels the library has launched since it was loaded. */
 unsigned long long QOPB_launch_count(void);
+/* Failure injection for tests: the n-th device allocation from now on
+   (n >= 1) fails as an out-of-memory would, and the call that makes it
+   reports QOP_MEM_ERROR; n = 0 cancels.  Returns 0, or -1 for n < 0. */
+int QOPB_inject_alloc_failure(int n);
 
 /* QOP_D3_asqtad_ddagd_norm2 without any device allocation (no counterpart
    in the reference).  For callers that cannot allocate device memory where
@@ -146,6 +150,28 @@ long long QOPB_serve_submit(const QOPB_request_t *req);     /* ticket >= 0, or -
 /* 0: done (result filled, ticket released); 1: timed out; -1: bad ticket */
 int QOPB_serve_wait(long long ticket, double timeout_s, QOPB_result_t *res);
 int QOPB_serve_stop(void);   /* finishes queued requests, joins the worker */
+
+/* Operator checks (no counterpart in the reference).  They apply the
+   reduced-precision normal-equation operator of the mixed solvers once, with
+   the solvers' own kernels, so that it can be compared site by site with the
+   FP64 operator QOP_D3_asqtad_ddagd_norm2 (lib/asqtad_dslash_p.c:1121-1138).
+   p = int16(in) on parity eo (QOP_EVEN or QOP_ODD), t = D_oe p (written to
+   t_out on the other parity), Ap = m^2 p - D_eo t (written to ap_out on
+   parity eo); both are the int16 values the solver would store, decoded.
+   QOPB_D3_sloppy_ddagd: one system; variant = an int16 hop variant (0..28,
+   the hop_kernel option), kind2 = 2 (plain second hop) or 3 (the
+   fused-update second hop, variants 20..28); sums = |t|^2, |p|^2, <p, Ap>,
+   |Ap|^2 as the kernels reduced them (the last two for kind 3 only).
+   QOPB_D3_sloppy_ddagd_batch: n <= 16 systems sharing the link stream;
+   variant = a batch_kernel value (0..15) or -1 for the solver's default;
+   sums[2j], sums[2j+1] = |t_j|^2 and <p_j, A_j p_j>.  Both return 0, or -1
+   with info->status = QOP_FAIL. */
+int QOPB_D3_sloppy_ddagd(QOP_info_t *info, QOP_D3_FermionLinksAsqtad *asqtad, double mass,
+                         QOP_D3_ColorVector *t_out, QOP_D3_ColorVector *ap_out, QOP_D3_ColorVector *in,
+                         QOP_evenodd_t eo, int variant, int kind2, double *sums);
+int QOPB_D3_sloppy_ddagd_batch(QOP_info_t *info, QOP_D3_FermionLinksAsqtad *asqtad, int n, const double *masses,
+                               QOP_D3_ColorVector **t_out, QOP_D3_ColorVector **ap_out, QOP_D3_ColorVector **in,
+                               QOP_evenodd_t eo, int variant, double *sums);
 
 #ifdef __cplusplus
 }

@@ -174,6 +174,23 @@ class Lattice:
         return fat, lng, W, n
 
 
+    def hisq_links_naik(self, hcoef, gauge, eps_naik):
+        """All link sets of QOP_hisq_create_L_from_G with n_naiks = len(eps_naik)
+        (lib/hisq_links_p.c:182-243): fn[0] = asqtad(acoeffs2, W) and, for
+        k >= 1, fn[k] = eps_naik[k] asqtad(acoeffs3, W) + fn[0], where
+        acoeffs3 keeps only difference_one_link and difference_naik
+        (:107-112); deps = asqtad(acoeffs3, W), the links QOP keeps for the
+        derivative with respect to epsilon (want_deps).  Returns
+        ([(fat, long)] * n_naiks, (deps_fat, deps_long))."""
+        fat, lng, W, _ = self.hisq_links(hcoef, gauge, want_W=True)
+        h = f64(hcoef)
+        dfat, dlng = self.make_imp_links([h[11], 0.0, 0.0, 0.0, 0.0, h[12]], W)
+        sets = [(fat, lng)]
+        for e in list(eps_naik)[1:]:
+            sets.append(([e * a + b for a, b in zip(dfat, fat)], [e * a + b for a, b in zip(dlng, lng)]))
+        return sets, (dfat, dlng)
+
+
 class Fla:
     """Oracle asqtad operator (links x 1/2, double stored)."""
 

@@ -508,6 +508,7 @@ void BatchEngine::start(int s, c2<double> *x, const c2<double> *b, double mass, 
   if (e.inflight) fail(QOP_FAIL, "batched solver: a chunk is in flight");
   sync();   // the last upload of the slot states has read them
   const i64 Vh = e.Vh;
+  need_finite(Blas<double>::norm2(b, e.is), "batched solver: source norm");   // before the slot is taken
   Impl::Sys &y = e.sys[s];
   y = Impl::Sys{};
   y.busy = true;
@@ -653,6 +654,7 @@ std::vector<int> BatchEngine::collect() {
     k_fold_x<<<grid_for(3 * Vh, 256), 256, 0, c.s>>>(y.x + e.is.off, e.xs + 3 * j * Vh, 3 * Vh);
     QLAUNCH();
     y.r2 = e.true_resid(j);
+    need_finite(y.r2, "batched solver: true residual norm");
     y.nru++;
     log0(QOP_VERB_MED, "BATCHCG[%d/%d]: iter %d sloppy rsq %g true rsq %g (stop %g)\n", j, n, s.iter, s.rsq, y.r2,
          s.stop);
@@ -703,3 +705,106 @@ void run_batch(FlaT<double> *f, int eo, int n, const double *mass, c2<double> **
 }
 
 }  // namespace qopb
+
+namespace qopb {
+__global__ void k_q16_to_f64(double2 *d, const uint4 *s, i64 Vh);   // mixed.cu
+}
+
+// The batched int16 operator of the batched solver, applied once with its
+// own hop kernels to n <= 16 systems: p_j = int16(in_j) on parity eo,
+// t_j = D_oe p_j, Ap_j = m_j^2 p_j - D_eo t_j; t_j and Ap_j are decoded
+// into t_out[j] / ap_out[j].  sums[2j], sums[2j+1] = |t_j|^2 and
+// <p_j, A_j p_j> = |t_j|^2 + m_j^2 |p_j|^2 as the kernels reduced them.  variant: a batch_kernel value (0..15), or
+// -1 for the solver's default choice for n systems.  Restates
+// QOP_asqtad_ddagd_norm2 (lib/asqtad_dslash_p.c:1121-1138) for several
+// vectors at once, as the reference's vectorised hop does
+// (lib/asqtad_dslash_p.c:1246-1279); it exists so that the batched sloppy
+// operator can be compared site by site with FP64.
+extern "C" int QOPB_D3_sloppy_ddagd_batch(QOP_info_t *info, QOP_D3_FermionLinksAsqtad *asqtad, int n,
+                                          const double *masses, QOP_D3_ColorVector **t_out,
+                                          QOP_D3_ColorVector **ap_out, QOP_D3_ColorVector **in, QOP_evenodd_t eo,
+                                          int variant, double *sums) {
+  using namespace qopb;
+  uint4 *ps = nullptr, *ts = nullptr, *as = nullptr;
+  MixState *dst = nullptr;
+  double *part = nullptr;
+  unsigned *count = nullptr;
+  auto release = [&]() { dfree(ps); dfree(ts); dfree(as); dfree(dst); dfree(part); dfree(count); };
+  try {
+    require_init("QOPB_D3_sloppy_ddagd_batch");
+    dd_refuse("QOPB_D3_sloppy_ddagd_batch");
+    handle_check(asqtad, "FermionLinksAsqtad");
+    if (n < 1 || n > BATCH_MAX) fail(QOP_FAIL, "QOPB_D3_sloppy_ddagd_batch: %d systems (1..%d)", n, BATCH_MAX);
+    if (!masses || !t_out || !ap_out || !in) fail(QOP_FAIL, "QOPB_D3_sloppy_ddagd_batch: NULL array");
+    for (int j = 0; j < n; j++) {
+      handle_check(t_out[j], "ColorVector");
+      handle_check(ap_out[j], "ColorVector");
+      handle_check(in[j], "ColorVector");
+    }
+    if (eo != QOP_EVEN && eo != QOP_ODD) fail(QOP_FAIL, "QOPB_D3_sloppy_ddagd_batch: eo must be EVEN or ODD");
+    if (variant < -1 || variant >= N_BHOP)
+      fail(QOP_FAIL, "QOPB_D3_sloppy_ddagd_batch: variant %d (-1..%d)", variant, N_BHOP - 1);
+    if (variant < 0) variant = n % 8 == 0 ? 7 : 1;
+    FlaT<double> *f = reinterpret_cast<FlaT<double> *>(asqtad);
+    Context &c = ctx();
+    const Geom &g = c.g;
+    const i64 Vh = g.Vh;
+    const int p = eo, q = 1 - eo;
+    SloppyLinks *sl = sloppy_get(f, LK_Q16);
+    const LinksSloppy lk_p = links_parity(sl, LK_Q16, p), lk_q = links_parity(sl, LK_Q16, q);
+    const int nsb = (int)((Vh + QB - 1) / QB), gridv = grid_for(Vh, 256);
+    const int BG = kBhop[variant].bg, ngrp = (n + BG - 1) / BG;
+    ps = dalloc<uint4>(n * Vh);
+    ts = dalloc<uint4>(n * Vh);
+    as = dalloc<uint4>(n * Vh);
+    dst = dalloc<MixState>(n);
+    part = dalloc<double>((size_t)ngrp * BG * nsb);
+    count = dalloc<unsigned>(ngrp);
+    dzero(count, sizeof(unsigned) * ngrp);
+    std::vector<MixState> h(n);
+    for (int j = 0; j < n; j++) {
+      h[j] = MixState{};
+      h[j].flag = MIX_RUN;
+      h[j].m2 = masses[j] * masses[j];
+      h[j].rsq = h[j].rsq_old = h[j].maxr2 = 1.0;
+      h[j].max_iter = 1 << 30;
+      k_to_sloppy<SpQ16><<<gridv, 256, 0, c.s>>>(ps + j * Vh, reinterpret_cast<VecT<double> *>(in[j])->d + par_off(g, p),
+                                                 Vh);
+      QLAUNCH();
+    }
+    QCHECK(cudaMemcpyAsync(dst, h.data(), sizeof(MixState) * n, cudaMemcpyHostToDevice, c.s));
+    NbrGeom ng;
+    for (int d = 0; d < 4; d++) ng.L[d] = g.L[d];
+    ng.str[3] = 1; ng.str[2] = g.L[3]; ng.str[1] = g.L[2] * g.L[3]; ng.str[0] = g.L[1] * g.L[2] * g.L[3];
+    const bool recon = sl->recon != 0;
+    const float c_long = (float)sl->c_long;
+    launch_bhop<1>(variant, sl->nl, recon, ngrp, nsb, ts, ps, (const unsigned char *)lk_q.a, nullptr, g, ng, q, dst, n,
+                   part, count, c_long);
+    QLAUNCH();
+    launch_bhop<2>(variant, sl->nl, recon, ngrp, nsb, as, ts, (const unsigned char *)lk_p.a, ps, g, ng, p, dst, n,
+                   part, count, c_long);
+    QLAUNCH();
+    for (int j = 0; j < n; j++) {
+      k_q16_to_f64<<<gridv, 256, 0, c.s>>>(reinterpret_cast<VecT<double> *>(t_out[j])->d + par_off(g, q), ts + j * Vh,
+                                          Vh);
+      k_q16_to_f64<<<gridv, 256, 0, c.s>>>(reinterpret_cast<VecT<double> *>(ap_out[j])->d + par_off(g, p),
+                                          as + j * Vh, Vh);
+      QLAUNCHN(2);
+    }
+    QCHECK(cudaMemcpyAsync(h.data(), dst, sizeof(MixState) * n, cudaMemcpyDeviceToHost, c.s));
+    sync();
+    if (sums)
+      for (int j = 0; j < n; j++) {
+        sums[2 * j] = h[j].dp2;
+        sums[2 * j + 1] = h[j].alpha > 0 ? 1.0 / h[j].alpha : 0.0;   // alpha = rsq / pAp with rsq = 1
+      }
+    release();
+    if (info) info->status = QOP_SUCCESS;
+    return 0;
+  } catch (Fail &e) {
+    release();
+    fprintf(stderr, "QOPB_D3_sloppy_ddagd_batch: %s\n", e.msg.c_str());
+    if (info) info->status = e.status;
+    return -1;
+  }
+}

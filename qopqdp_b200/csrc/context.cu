@@ -2,6 +2,7 @@
 // Reference: lib/common.c:39-191 (init, version, verbosity, raw index),
 // lib/asqtad_invert.c:9-113 (inverter options), lib/hisq_links.c:32-78.
 #include "qopb.h"
+#include <atomic>
 #include <cstdarg>
 #include <sys/time.h>
 #include <mutex>
@@ -73,10 +74,16 @@ void ensure_ready() {
   QCHECK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
 }
 
+// allocation-failure injection (QOPB_inject_alloc_failure): the n-th
+// allocation from now on fails as an out-of-memory would
+static std::atomic<int> g_alloc_fail_in{0};
+
 void *dmalloc(size_t bytes) {
   ensure_ready();
   void *p = nullptr;
   if (bytes == 0) bytes = 16;
+  if (g_alloc_fail_in.load() > 0 && g_alloc_fail_in.fetch_sub(1) == 1)
+    fail(QOP_MEM_ERROR, "device allocation of %zu bytes failed: injected failure", bytes);
   cudaError_t e = cudaMallocAsync(&p, bytes, g_ctx.s);
   if (e != cudaSuccess) {
     cudaGetLastError();
@@ -232,6 +239,12 @@ int QOP_is_initialized(void) { return ctx().inited; }
 
 unsigned long long QOPB_launch_count(void) { return launch_count(); }
 
+int QOPB_inject_alloc_failure(int n) {
+  if (n < 0) return -1;
+  g_alloc_fail_in.store(n);
+  return 0;
+}
+
 const char *QOP_version_str(void) { return "0.21.1-b200"; }
 int QOP_version_int(void) { return (0 * 1000 + 21) * 1000 + 1; }
 
@@ -303,6 +316,12 @@ QOP_status_t QOP_asqtad_invert_set_opts(QOP_opt_t opts[], int nopts) {
     } else if (!strcmp(t, "serve_policy")) {
       if (v != 0 && v != 1) return QOP_FAIL;
       n.serve_policy = (int)v;
+    } else if (!strcmp(t, "serve_hbm_mb")) {
+      if (!(v >= 0)) return QOP_FAIL;
+      n.serve_hbm_mb = v;
+    } else if (!strcmp(t, "mbar_tries")) {
+      if (v < 0 || v > (1 << 26)) return QOP_FAIL;
+      n.mbar_tries = (int)v;
     } else if (!strcmp(t, "recon_long")) {
       n.recon_long = v != 0;
     } else if (!strcmp(t, "hop_kernel")) {

@@ -503,8 +503,26 @@ __device__ __forceinline__ bool mbar_try(uint64_t *bar, unsigned phase) {
                : "=r"(ok) : "r"(smem_u32(bar)), "r"(phase) : "memory");
   return ok != 0;
 }
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned phase) {
-  for (int it = 0; it < (1 << 22); it++)
+// non-blocking probe of the phase (mbarrier.test_wait never suspends)
+__device__ __forceinline__ bool mbar_test(uint64_t *bar, unsigned phase) {
+  unsigned ok;
+  asm volatile("{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+               : "=r"(ok) : "r"(smem_u32(bar)), "r"(phase) : "memory");
+  return ok != 0;
+}
+// a bounded wait: false after `tries` polls (the caller raises MIX_ERROR).
+// The default limit polls with try_wait (which may suspend the thread for a
+// while per poll); a limit of 16 polls or fewer (option mbar_tries) polls
+// with the non-blocking test_wait, so that a short limit really is short,
+// and a limit of 0 gives up at once
+constexpr int MBAR_TRIES = 1 << 22;
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned phase, int tries = MBAR_TRIES) {
+  if (tries <= 16) {
+    for (int it = 0; it < tries; it++)
+      if (mbar_test(bar, phase)) return true;
+    return false;
+  }
+  for (int it = 0; it < tries; it++)
     if (mbar_try(bar, phase)) return true;
   return false;
 }
@@ -620,6 +638,7 @@ k_mix_hop_q16(uint4 *__restrict__ out, const uint4 *__restrict__ src, const unsi
   }
   float2 a[3] = {make_float2(0, 0), make_float2(0, 0), make_float2(0, 0)};
   bool ok = true;
+  const int tries = st->mbar_tries >= 0 ? st->mbar_tries : MBAR_TRIES;
   int issued[2] = {NG > 0 ? 1 : 0, NG > 1 ? 1 : 0}, waited[2] = {0, 0};   // thread 0 bookkeeping
 #pragma unroll
   for (int gi = 0; gi < NG; gi++) {
@@ -630,7 +649,7 @@ k_mix_hop_q16(uint4 *__restrict__ out, const uint4 *__restrict__ src, const unsi
       const int k = gi * GRP + s;
       nb[s] = live ? src[nbr_fast(ng, x, lex, slot_mu<NL>(k), slot_disp<NL>(k))] : make_uint4(0, 0, 0, 0);
     }
-    const bool arrived = mbar_wait_bounded(&bar[buf], (gi >> 1) & 1);
+    const bool arrived = mbar_wait_bounded(&bar[buf], (gi >> 1) & 1, tries);
     if (!arrived) ok = false;
     else waited[buf]++;
     if (arrived && live) {
@@ -653,7 +672,7 @@ k_mix_hop_q16(uint4 *__restrict__ out, const uint4 *__restrict__ src, const unsi
   }
   if (!ok) {
     st->flag = MIX_ERROR;
-    if (tid == 0)   // let copies still in flight land before the block exits (bounded)
+    if (tid == 0)   // let copies still in flight land before the block exits (bounded, default limit)
       for (int b2 = 0; b2 < 2; b2++)
         while (waited[b2] < issued[b2] && mbar_wait_bounded(&bar[b2], waited[b2] & 1)) waited[b2]++;
   }
@@ -1140,17 +1159,31 @@ static void run_mixed(LinOp<double> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t *r
   Blas<double>::zero(x, is);
   for (int s = 1; s < ns; s++) Blas<double>::zero(ms->x[s], is);
   if (b2 == 0.0) { ra->final_rsq = 0; ra->final_iter = 0; return; }
+  need_finite(b2, "mixed solver: source norm");
   const double stop = ra->rsqmin * b2;
   const i64 nb = Sp::block(Vh);
-  E *rs = dalloc<E>(nb), *ps = dalloc<E>(nb), *Aps = dalloc<E>(nb), *ts = dalloc<E>(nb);
-  float2 *xs = dalloc<float2>(3 * Vh);
-  dzero(xs, sizeof(float2) * 3 * Vh);
-  c2<double> *r = dalloc<c2<double>>(vec_elems(g)), *Ax = dalloc<c2<double>>(vec_elems(g));
-  Blas<double>::copy(r, b, is);
-  MixState *dst = dalloc<MixState>(1);
+  E *rs = nullptr, *ps = nullptr, *Aps = nullptr, *ts = nullptr;
+  float2 *xs = nullptr;
+  c2<double> *r = nullptr, *Ax = nullptr;
+  MixState *dst = nullptr;
   MixState h{};
   MsShift *dsh = nullptr;
   MsVecs mv{};
+  // frees every buffer of the solve (idempotent; on every exit, normal or
+  // thrown, so that a failed allocation or a failed check leaks nothing)
+  auto release = [&]() {
+    dfree(rs); dfree(ps); dfree(Aps); dfree(ts); dfree(xs); dfree(r); dfree(Ax); dfree(dst);
+    for (int s = 1; s < ns; s++) { dfree(mv.p[s]); dfree(mv.x[s]); mv.p[s] = nullptr; mv.x[s] = nullptr; }
+    dfree(dsh);
+    rs = ps = Aps = ts = nullptr; xs = nullptr; r = Ax = nullptr; dst = nullptr; dsh = nullptr;
+  };
+  try {
+  rs = dalloc<E>(nb); ps = dalloc<E>(nb); Aps = dalloc<E>(nb); ts = dalloc<E>(nb);
+  xs = dalloc<float2>(3 * Vh);
+  dzero(xs, sizeof(float2) * 3 * Vh);
+  r = dalloc<c2<double>>(vec_elems(g)); Ax = dalloc<c2<double>>(vec_elems(g));
+  Blas<double>::copy(r, b, is);
+  dst = dalloc<MixState>(1);
   if (ns > 1) {
     std::vector<MsShift> hs(ns);
     for (int s = 0; s < ns; s++) hs[s] = MsShift{ms->sigma[s], 1.0, 1.0, -1.0, ms->stop[s], 1, 0};
@@ -1162,11 +1195,6 @@ static void run_mixed(LinOp<double> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t *r
       dzero(mv.x[s], sizeof(float2) * 3 * Vh);
     }
   }
-  auto release = [&]() {
-    dfree(rs); dfree(ps); dfree(Aps); dfree(ts); dfree(xs); dfree(r); dfree(Ax); dfree(dst);
-    for (int s = 1; s < ns; s++) { dfree(mv.p[s]); dfree(mv.x[s]); }
-    dfree(dsh);
-  };
   const LinksSloppy lk_p = links_parity(sl, lkfmt, p), lk_q = links_parity(sl, lkfmt, q);
   const int gridh = grid_for(Vh, 128), gridv = grid_for(Vh, 256), gridq = (int)((Vh + QB - 1) / QB);
   NbrGeom ng;
@@ -1191,6 +1219,7 @@ static void run_mixed(LinOp<double> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t *r
     h.maxr2 = r2;
   };
   h.stop = stop;
+  h.mbar_tries = c.opt.mbar_tries;
   h.delta2 = c.opt.ru_delta * c.opt.ru_delta;
   h.m2 = L.mass * L.mass;
   h.max_iter = ia->max_iter;
@@ -1335,6 +1364,7 @@ static void run_mixed(LinOp<double> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t *r
     L.d2(Ax, x);
     Blas<double>::axpby(r, 1.0, b, -1.0, Ax, is);
     r2 = Blas<double>::norm2(r, is);
+    need_finite(r2, "mixed solver: true residual norm");
     nru++;
     log0(QOP_VERB_MED, "MIXCG[%d]: iter %d sloppy rsq %g true rsq %g (stop %g)\n", lkfmt, h.iter, h.rsq, r2, stop);
     if (r2 <= stop || h.iter + nru >= h.max_iter || stalls > 2) break;
@@ -1361,6 +1391,10 @@ static void run_mixed(LinOp<double> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t *r
   ra->final_iter = h.iter + nru;
   release();
   sync();
+  } catch (...) {
+    release();
+    throw;
+  }
 }
 
 static void run_sloppy(LinOp<double> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t *ra, c2<double> *x,
@@ -1515,3 +1549,101 @@ void solve_multi_mixed(QOP_info_t *info, FlaT<double> *f, QOP_invert_arg_t *ia, 
 }
 
 }  // namespace qopb
+
+// ---------------------------------------------------------------- test entry point
+namespace qopb {
+// int16 parity block -> FP64 [3][Vh] parity block (the stored values)
+__global__ void k_q16_to_f64(double2 *d, const uint4 *s, i64 Vh) {
+  const i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x;
+  if (i >= Vh) return;
+  float2 v[3];
+  SpQ16::load(s, (int)i, Vh, v);
+#pragma unroll
+  for (int c = 0; c < 3; c++) d[c * Vh + i] = make_double2(v[c].x, v[c].y);
+}
+}  // namespace qopb
+
+// The int16 normal-equation operator of the mixed solver, applied once with
+// the solver's own kernels: p = int16(in) on parity eo, t = D_oe p (the
+// first hop, stored as int16 on the other parity) and Ap = m^2 p - D_eo t
+// (the second hop: kind 2, or kind 3 = the fused-update hop that also
+// reduces <p, Ap> and |Ap|^2).  t and Ap are decoded into t_out / ap_out.
+// sums[0..3] = |t|^2, |p|^2, <p, Ap>, |Ap|^2 as the kernels reduced them
+// (the last two only for kind 3).  Restates QOP_asqtad_ddagd_norm2
+// (lib/asqtad_dslash_p.c:1121-1138) in the solver's storage; it exists so
+// that the sloppy operator can be compared site by site with FP64.
+extern "C" int QOPB_D3_sloppy_ddagd(QOP_info_t *info, QOP_D3_FermionLinksAsqtad *asqtad, double mass,
+                                    QOP_D3_ColorVector *t_out, QOP_D3_ColorVector *ap_out, QOP_D3_ColorVector *in,
+                                    QOP_evenodd_t eo, int variant, int kind2, double *sums) {
+  using namespace qopb;
+  uint4 *p16 = nullptr, *t16 = nullptr, *a16 = nullptr;
+  MixState *dst = nullptr;
+  try {
+    require_init("QOPB_D3_sloppy_ddagd");
+    dd_refuse("QOPB_D3_sloppy_ddagd");
+    handle_check(asqtad, "FermionLinksAsqtad");
+    handle_check(t_out, "ColorVector");
+    handle_check(ap_out, "ColorVector");
+    handle_check(in, "ColorVector");
+    if (eo != QOP_EVEN && eo != QOP_ODD) fail(QOP_FAIL, "QOPB_D3_sloppy_ddagd: eo must be EVEN or ODD");
+    if (variant < 0 || variant > 28) fail(QOP_FAIL, "QOPB_D3_sloppy_ddagd: hop variant %d (0..28)", variant);
+    if (kind2 != 2 && kind2 != 3) fail(QOP_FAIL, "QOPB_D3_sloppy_ddagd: second hop kind %d (2 or 3)", kind2);
+    if (kind2 == 3 && variant < 20) fail(QOP_FAIL, "QOPB_D3_sloppy_ddagd: kind 3 needs a packed variant (20..28)");
+    FlaT<double> *f = reinterpret_cast<FlaT<double> *>(asqtad);
+    VecT<double> *to = reinterpret_cast<VecT<double> *>(t_out), *ao = reinterpret_cast<VecT<double> *>(ap_out);
+    VecT<double> *vi = reinterpret_cast<VecT<double> *>(in);
+    Context &c = ctx();
+    const Geom &g = c.g;
+    const i64 Vh = g.Vh;
+    const int p = eo, q = 1 - eo;
+    SloppyLinks *sl = sloppy_get(f, LK_Q16);
+    const LinksSloppy lk_p = links_parity(sl, LK_Q16, p), lk_q = links_parity(sl, LK_Q16, q);
+    p16 = dalloc<uint4>(Vh);
+    t16 = dalloc<uint4>(Vh);
+    a16 = dalloc<uint4>(Vh);
+    dst = dalloc<MixState>(1);
+    MixState h{};
+    h.flag = MIX_RUN;
+    h.m2 = mass * mass;
+    h.rsq = h.rsq_old = h.maxr2 = 1.0;
+    h.max_iter = 1 << 30;
+    QCHECK(cudaMemcpyAsync(dst, &h, sizeof h, cudaMemcpyHostToDevice, c.s));
+    const int gridv = grid_for(Vh, 256), gridq = (int)((Vh + QB - 1) / QB);
+    NbrGeom ng;
+    for (int d = 0; d < 4; d++) ng.L[d] = g.L[d];
+    ng.str[3] = 1; ng.str[2] = g.L[3]; ng.str[1] = g.L[2] * g.L[3]; ng.str[0] = g.L[1] * g.L[2] * g.L[3];
+    k_to_sloppy<SpQ16><<<gridv, 256, 0, c.s>>>(p16, vi->d + par_off(g, p), Vh);
+    QLAUNCH();
+    const bool recon = sl->recon != 0;
+    const float c_long = (float)sl->c_long;
+    launch_q16<1>(variant, sl->nl, recon, c_long, gridq, t16, p16, (const unsigned char *)lk_q.a, nullptr, g, ng, q,
+                  dst);
+    QLAUNCH();
+    if (kind2 == 3)
+      launch_q16_fused(variant, sl->nl, recon, c_long, gridq, a16, t16, (const unsigned char *)lk_p.a, p16, g, ng, p,
+                       dst, p16, 1);
+    else
+      launch_q16<2>(variant, sl->nl, recon, c_long, gridq, a16, t16, (const unsigned char *)lk_p.a, p16, g, ng, p,
+                    dst);
+    QLAUNCH();
+    k_q16_to_f64<<<gridv, 256, 0, c.s>>>(to->d + par_off(g, q), t16, Vh);
+    k_q16_to_f64<<<gridv, 256, 0, c.s>>>(ao->d + par_off(g, p), a16, Vh);
+    QLAUNCHN(2);
+    QCHECK(cudaMemcpyAsync(&h, dst, sizeof h, cudaMemcpyDeviceToHost, c.s));
+    sync();
+    if (sums) {
+      sums[0] = h.dp2;
+      sums[1] = kind2 == 3 ? h.red3[0] : h.red;
+      sums[2] = kind2 == 3 ? h.red3[1] : 0.0;
+      sums[3] = kind2 == 3 ? h.red3[2] : 0.0;
+    }
+    dfree(p16); dfree(t16); dfree(a16); dfree(dst);
+    if (info) info->status = QOP_SUCCESS;
+    return 0;
+  } catch (Fail &e) {
+    dfree(p16); dfree(t16); dfree(a16); dfree(dst);
+    fprintf(stderr, "QOPB_D3_sloppy_ddagd: %s\n", e.msg.c_str());
+    if (info) info->status = e.status;
+    return -1;
+  }
+}

@@ -164,6 +164,7 @@ struct MixState {
   double rsq, rsq_old, alpha, beta, dp2, maxr2, stop, delta2, m2, red;
   int iter, max_iter, flag, tok;   // tok: iteration whose hop set alpha (fused update)
   double red3[3];
+  int mbar_tries = -1;             // TMA-staged hops: polls per mbarrier wait (< 0: the default)
 };
 
 __device__ __forceinline__ void cfmaf(float2 &a, float2 u, float2 v) {
@@ -294,17 +295,20 @@ __device__ __forceinline__ float2 u16_pair(unsigned w) {
   return __fadd2_rn(b, make_float2(-8421376.0f, -8421376.0f));
 }
 
-// site components times sc, duplicated: vx[c] = (re sc, re sc), vy[c] = (im sc, im sc)
+// site components times sc, duplicated: vx[c] = (re sc, re sc), vy[c] = (im sc, im sc).
+// The integer pair comes out exact (u16_pair) and is scaled by one packed
+// multiply, so each component carries a single rounding; folding the offset
+// into an FMA instead (fma(2^23 + u, s, -(2^23 + 32768) s)) would round the
+// offset product and add up to half a quantisation step per component.
 __device__ __forceinline__ void q16_pk_site(const uint4 nb, float sc, float2 vx[3], float2 vy[3]) {
   const float s = sc * __uint_as_float(nb.w) * (1.0f / 32767.0f);
-  const float o = -8421376.0f * s;
+  const float2 s2 = make_float2(s, s);
   const unsigned w[3] = {nb.x, nb.y, nb.z};
 #pragma unroll
   for (int c = 0; c < 3; c++) {
-    const float re = fmaf(__int_as_float(__byte_perm(w[c], 0x4B000000u, 0x7610)), s, o);
-    const float im = fmaf(__int_as_float(__byte_perm(w[c], 0x4B000000u, 0x7632)), s, o);
-    vx[c] = make_float2(re, re);
-    vy[c] = make_float2(im, im);
+    const float2 v = __fmul2_rn(u16_pair(w[c]), s2);
+    vx[c] = make_float2(v.x, v.x);
+    vy[c] = make_float2(v.y, v.y);
   }
 }
 

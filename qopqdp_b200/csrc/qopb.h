@@ -45,6 +45,11 @@ void count_launches(int n);
 #define QLAUNCHN(n) (::qopb::count_launches(n), ::qopb::check_cuda(cudaGetLastError(), "kernel launch", __FILE__, __LINE__))
 #define QLAUNCH() QLAUNCHN(1)
 [[noreturn]] void fail(QOP_status_t s, const char *fmt, ...);
+// a NaN or Inf norm (of a source, a residual) ends the call with QOP_FAIL;
+// the reference has no such check and would iterate on NaN
+inline void need_finite(double v, const char *what) {
+  if (!(v - v == 0.0)) fail(QOP_FAIL, "%s is not finite (%g): NaN or Inf in the input or the iteration", what, v);
+}
 
 // ---------------------------------------------------------------- geometry
 struct Geom {
@@ -112,6 +117,8 @@ struct Options {
   int fuse_update = 1;           // int16 hop variants 20-26: 1 = the second hop reduces for a fused x / r / p update
   int pdl = 1;                   // fused int16 iteration: 1 = its kernels launched as programmatic dependents
   int serve_policy = 0;          // solve service: 0 = step every engine in turn, 1 = only the one with the oldest request
+  double serve_hbm_mb = 0;       // solve service: device memory all engines together may hold (MB; 0 = free HBM less 2 GiB)
+  int mbar_tries = 1 << 22;      // bounded mbarrier waits of the TMA-staged int16 hops: polls before MIX_ERROR
   // QOP_asqtad_force_set_opts (lib/asqtad_force.c:3-41)
   int force_fnmat_src_min = 2, force_veclength = 4;
   // QOP_hisq_links_set_opts (lib/hisq_links.c:4-78)

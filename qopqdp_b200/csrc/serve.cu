@@ -22,7 +22,9 @@
 // its sources enter one engine together) and a request that does not fit
 // holds back the later requests of its engine.  A new engine is created
 // only if its device memory fits in the free HBM (less a reserve) while
-// other engines run; an engine whose slots are all free is destroyed.
+// other engines run, and within the option serve_hbm_mb when it is set;
+// an engine whose slots are all free is destroyed.  A request whose source
+// holds a NaN or Inf fails alone (QOP_FAIL) before it takes a slot.
 // Timing per request: queue (submit -> admission), solve (admission ->
 // last source finished) and total.  While the service runs the worker owns
 // the library (its global stream, current lattice and option state);
@@ -73,6 +75,7 @@ Service g_srv;
 // one engine with its FP64 solution and source vectors per slot
 struct Lane {
   int lattice = 0, eo = 0;
+  size_t bytes = 0;            // device memory of the engine and its vectors
   const void *links = nullptr;
   std::unique_ptr<BatchEngine> eng;
   std::vector<c2<double> *> x, b;
@@ -133,7 +136,14 @@ struct Worker {
     const Geom &g = ctx().g;
     const size_t need = BatchEngine::bytes(g, BATCH_MAX) + 2 * sizeof(c2<double>) * vec_elems(g) * BATCH_MAX;
     if (any_running() && free_hbm() < need + HBM_RESERVE) return nullptr;
+    // option serve_hbm_mb: the engines together stay within the budget (a
+    // lone engine is always admitted, so that every request can run)
+    const double budget = ctx().opt.serve_hbm_mb * 1048576.0;
+    size_t held = 0;
+    for (auto &o : lanes) held += o->bytes;
+    if (budget > 0 && !lanes.empty() && (double)(held + need) > budget) return nullptr;
     auto l = std::make_unique<Lane>();
+    l->bytes = need;
     l->lattice = r.lattice;
     l->eo = r.evenodd;
     l->links = r.links;
@@ -183,6 +193,13 @@ struct Worker {
           continue;
         }
         const Geom &g = ctx().g;
+        // a source with NaN or Inf fails its own request, before it holds a slot
+        for (int k = 0; k < r.nrhs; k++) {
+          const double *src = j->src[k];
+          double acc = 0;
+          for (i64 e = 0; e < 6 * g.V; e++) acc += src[e] * 0.0;   // NaN or Inf -> NaN
+          need_finite(acc, "serve: source");
+        }
         j->t_start = now_ms();
         j->left = r.nrhs;
         starting = true;

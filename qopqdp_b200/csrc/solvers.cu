@@ -6,6 +6,7 @@
 // lib/asqtad_invert_p.c:80-100 (project/reconstruct), :246-330 (refine),
 // :332-647 (solve_multi), :649-851 (invert), :878-1059 (invert_multi).
 #include "solvers.cuh"
+#include <memory>
 #include "fields.cuh"
 #include <vector>
 #include <cmath>
@@ -37,6 +38,7 @@ void cg(LinOp<T> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t *ra, c2<T> *out, cons
   if (max_restarts < 0) max_restarts = 5;
   ra->final_rsq = 0; ra->final_rel = 0; ra->final_iter = 0; ra->final_restart = 0;
   double insq = B::norm2(in, q);
+  need_finite(insq, "CG: source norm");
   if (insq == 0.) { B::zero(out, q); return; }
   Tmp<T> r, Mp;
   double rsqstop = ra->rsqmin * insq, rsq = 0, oldrsq = 0, relnorm = 1;
@@ -50,6 +52,7 @@ void cg(LinOp<T> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t *ra, c2<T> *out, cons
       iteration = 1; total++;
       B::axpby(r, 1.0, in, -1.0, Mp, q);
       rsq = B::norm2(r, q);
+      need_finite(rsq, "CG: true residual norm");
       if (ra->relmin > 0) relnorm = relnorm2<T>(r, out, eo);
       log0(QOP_VERB_LOW, "CG: (re)start: iter %i rsq = %g rel = %g\n", total, rsq, relnorm);
       if (rsq < rsqstop || relnorm < ra->relmin || total >= max_it) break;
@@ -62,6 +65,7 @@ void cg(LinOp<T> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t *ra, c2<T> *out, cons
     L.d2(Mp, p);
     iteration++; total++;
     double pkp = B::redot(p, Mp, q);
+    need_finite(pkp, "CG: <p, A p>");
     if (pkp <= 0) break;
     double a = rsq / pkp;
     rsq = B::cg_update(out, r, a, p, Mp, q);
@@ -82,6 +86,7 @@ void cgms(LinOp<T> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t **ra, const double 
   const Range q = vrange(ctx().g, eo);
   std::vector<double> a(ns, 0), b(ns, 0), bo(ns, -1), z(ns, 1), zo(ns, 1), zn(ns, 1);
   double insq = B::norm2(in, q);
+  need_finite(insq, "CGMS: source norm");
   if (insq == 0.) {
     for (int i = 0; i < ns; i++) {
       B::zero(out[i], q);
@@ -97,12 +102,12 @@ void cgms(LinOp<T> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t **ra, const double 
   }
   const double rsqstop = ra[irsq]->rsqmin * insq, relstop = ra[irel]->relmin;
   Tmp<T> r, Mp, y, Ay, ry;
-  std::vector<Tmp<T> *> own;
+  std::vector<std::unique_ptr<Tmp<T>>> own;
   std::vector<c2<T> *> pm(ns);
   B::copy(r, in, q);
   for (int i = 0; i < ns; i++) {
     if (i == imin) pm[i] = p;
-    else { own.push_back(new Tmp<T>()); pm[i] = *own.back(); }
+    else { own.emplace_back(new Tmp<T>()); pm[i] = *own.back(); }
     B::zero(out[i], q);
     B::copy(pm[i], r, q);
   }
@@ -115,6 +120,7 @@ void cgms(LinOp<T> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t **ra, const double 
     oldrsq = rsq;
     double pkp = L.d2n(Mp, p);
     iteration++;
+    need_finite(pkp, "CGMS: <p, A p>");
     if (pkp <= 0) break;
     b[imin] = rsq / pkp;
     rsq = B::cg_update(out[imin], r, b[imin], p, Mp, q);
@@ -190,7 +196,6 @@ void cgms(LinOp<T> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t **ra, const double 
     for (int i = 0; i < ns; i++) { bo[i] = b[i]; zo[i] = z[i]; z[i] = zn[i]; }
   }
   B::copy(out[imin], y, q);
-  for (auto *t : own) delete t;
   for (int i = 0; i < ns; i++) {
     double s = zn[i] * zn[i];
     ra[i]->final_rsq = s * trueRsqFac * rsq / insq;
@@ -282,17 +287,16 @@ static void inner_cgms(FlaT<T> *f, LinOp<T> &L, QOP_invert_arg_t *ia, QOP_resid_
     // asqtad_invert_p.c:510-537: single-precision links and vectors
     FlaT<float> *f32 = shadow32(f);
     const Range is = vrange(g, ineo);
-    c2<float> *rf = dalloc<c2<float>>(vec_elems(g)), *tf = dalloc<c2<float>>(vec_elems(g));
-    c2<float> *pf = dalloc<c2<float>>(vec_elems(g));
+    Tmp<float> rf, tf, pf;
+    std::vector<std::unique_ptr<Tmp<float>>> xfo;
     std::vector<c2<float> *> xf(nm);
-    for (int i = 0; i < nm; i++) { xf[i] = dalloc<c2<float>>(vec_elems(g)); dzero(xf[i], sizeof(c2<float>) * vec_elems(g)); }
+    for (int i = 0; i < nm; i++) { xfo.emplace_back(new Tmp<float>()); xf[i] = *xfo.back(); }
     convert<float, T>(rf, rhs, is);
     std::vector<double> m2f(nm);
     for (int i = 0; i < nm; i++) m2f[i] = (double)(float)m2s[i];
     LinOp<float> Lf{f32, (double)(float)L.mass, L.eo, tf};
     cgms<float>(Lf, ia, xra, m2f.data(), nm, xf.data(), rf, pf, ineo);
-    for (int i = 0; i < nm; i++) { convert<T, float>(x[i], xf[i], is); dfree(xf[i]); }
-    dfree(rf); dfree(tf); dfree(pf);
+    for (int i = 0; i < nm; i++) convert<T, float>(x[i], xf[i], is);
     return;
   }
   cgms<T>(L, ia, xra, m2s, nm, x, rhs, cgp, ineo);
@@ -325,9 +329,12 @@ void solve_multi(QOP_info_t *info, FlaT<T> *f, QOP_invert_arg_t *ia, QOP_resid_a
   const int max_iter = ia->max_iter, max_restarts = ia->max_restarts;
   const double mixedrsq = ia->mixed_rsq;
   Tmp<T> tv, cgp, optmp;
-  std::vector<Tmp<T> *> rr(nsolve);
+  std::vector<std::unique_ptr<Tmp<T>>> rr(nsolve);
   std::vector<c2<T> *> r(nsolve);
-  for (int i = 0; i < nsolve; i++) in2[i] = B::norm2(in[i], is);
+  for (int i = 0; i < nsolve; i++) {
+    in2[i] = B::norm2(in[i], is);
+    need_finite(in2[i], "solve: source norm");
+  }
   for (int i = 0; i < nsolve; i++) {
     r2stop[i] = ra[i]->rsqmin * in2[i];
     mass2[i] = masses[i] * masses[i];
@@ -341,7 +348,7 @@ void solve_multi(QOP_info_t *info, FlaT<T> *f, QOP_invert_arg_t *ia, QOP_resid_a
       m2s[j] = mass2[i];
       nm++;
     }
-    rr[i] = new Tmp<T>();
+    rr[i].reset(new Tmp<T>());
     r[i] = *rr[i];
     Dslash<T>::apply(f, 0, r[i], out[i], opeo, ineo);
   }
@@ -354,11 +361,11 @@ void solve_multi(QOP_info_t *info, FlaT<T> *f, QOP_invert_arg_t *ia, QOP_resid_a
   resarg0.rsqmin = 0;
   resarg0.relmin = 0;
   std::vector<QOP_resid_arg_t *> xra(nm);
-  std::vector<Tmp<T> *> xx(nm);
+  std::vector<std::unique_ptr<Tmp<T>>> xx(nm);
   std::vector<c2<T> *> x(nm);
   const double m20 = m2s[0];
   LinOp<T> L{f, std::sqrt(m20), ineo, optmp};
-  for (int i = 0; i < nm; i++) { m2s[i] -= m20; xx[i] = new Tmp<T>(); x[i] = *xx[i]; }
+  for (int i = 0; i < nm; i++) { m2s[i] -= m20; xx[i].reset(new Tmp<T>()); x[i] = *xx[i]; }
   refine<T>(f, out, in, r.data(), r2.data(), mass2.data(), scale.data(), nsolve, ineo, nullptr, nullptr, 0, oi.data(),
             nullptr, nsolve, tv);
   while (true) {
@@ -423,8 +430,6 @@ void solve_multi(QOP_info_t *info, FlaT<T> *f, QOP_invert_arg_t *ia, QOP_resid_a
     ra[i]->final_restart = nrestart > 0 ? nrestart : 0;
   }
   const double nflop = 0.5 * (20 * 3 + 2 * 8 * 3 * 3 * f->nlinks), nflopm = 0.5 * 10 * 3;
-  for (auto *t : xx) delete t;
-  for (auto *t : rr) delete t;
   sync();
   if (info) {
     info->final_sec = dtime;
@@ -459,6 +464,7 @@ void invert(QOP_info_t *info, FlaT<T> *f, QOP_invert_arg_t *ia, QOP_resid_arg_t 
   if (ineo != QOP_ODD) insqe = B::norm2(in, vrange(g, QOP_EVEN));
   if (ineo != QOP_EVEN) insqo = B::norm2(in, vrange(g, QOP_ODD));
   const double insq = insqe + insqo;
+  need_finite(insq, "invert: source norm");
   const int cgeo = insqe >= insqo ? QOP_EVEN : QOP_ODD;
   const Range cs = vrange(g, cgeo), ocs = vrange(g, opp(cgeo));
   Tmp<T> cgp, cgr, tmp2, qin, qout, optmp;

@@ -190,6 +190,12 @@ def load_library(path=None):
         sig("get_asqtad_deps_links_from_hisq", [vp], vp)
     lib.QOP_FD3_asqtad_create_L_from_L.argtypes = [vp]
     lib.QOP_FD3_asqtad_create_L_from_L.restype = vp
+    dp = C.POINTER(C.c_double)
+    lib.QOPB_D3_sloppy_ddagd.argtypes = [C.POINTER(QOP_info_t), vp, C.c_double, vp, vp, vp, ip, ip, ip, dp]
+    lib.QOPB_D3_sloppy_ddagd.restype = ip
+    lib.QOPB_D3_sloppy_ddagd_batch.argtypes = [C.POINTER(QOP_info_t), vp, ip, dp, C.POINTER(vp), C.POINTER(vp),
+                                               C.POINTER(vp), ip, ip, dp]
+    lib.QOPB_D3_sloppy_ddagd_batch.restype = ip
     _lib = lib
     return lib
 
@@ -457,6 +463,23 @@ class Qop:
     def ddagd_norm2(self, fla, mass, out, inp, eo, info=None):
         info = info or QOP_info_t()
         return self.f("asqtad_ddagd_norm2")(C.byref(info), fla, self.real(mass), out, inp, eo)
+
+    def sloppy_ddagd(self, fla, mass, t_out, ap_out, inp, eo, variant=25, kind2=3):
+        """int16 operator of the mixed solver: returns (status, [|t|^2, |p|^2, <p,Ap>, |Ap|^2])."""
+        info = QOP_info_t()
+        sums = (C.c_double * 4)()
+        self.lib.QOPB_D3_sloppy_ddagd(C.byref(info), fla, mass, t_out, ap_out, inp, eo, variant, kind2, sums)
+        return info.status, list(sums)
+
+    def sloppy_ddagd_batch(self, fla, masses, t_outs, ap_outs, ins, eo, variant=-1):
+        """batched int16 operator: returns (status, [(|t_j|^2, <p_j, A_j p_j>)])."""
+        n = len(ins)
+        info = QOP_info_t()
+        sums = (C.c_double * (2 * n))()
+        arr = lambda hs: (C.c_void_p * n)(*hs)
+        self.lib.QOPB_D3_sloppy_ddagd_batch(C.byref(info), fla, n, (C.c_double * n)(*masses), arr(t_outs),
+                                            arr(ap_outs), arr(ins), eo, variant, sums)
+        return info.status, [(sums[2 * j], sums[2 * j + 1]) for j in range(n)]
 
     def invert(self, fla, mass, out, inp, inv_arg, res_arg, info=None):
         info = info or QOP_info_t()

@@ -69,6 +69,42 @@ def test_hisq_links_match_oracle(prec):
 
 
 @pytest.mark.parametrize("prec", ["D", "F"])
+def test_hisq_eps_naik_link_sets_match_oracle(prec):
+    """n_naiks = 3 (lib/hisq_links_p.c:182-243): fn[0] = asqtad(W), fn[k] =
+    eps_k x difference links + fn[0], and the difference links themselves
+    (want_deps), each compared link by link with the oracle."""
+    q = gpu_lattice(L, prec)
+    U = [np.asarray(u, dtype=q.dtype) for u in gauge(L, 0.5, 9)]
+    g = q.create_G(U)
+    hc = LT.hisq_bench_coeffs()
+    hc.n_naiks = 3
+    eps = [0.0, -0.0632, 0.041]
+    for k, e in enumerate(eps):
+        hc.eps_naik[k] = e
+    hc.difference_one_link, hc.difference_naik = 0.0375, -0.0413
+    assert q.set_hisq_opts(want_deps=1) == 0
+    info = QOP_info_t()
+    h = q.hisq_create_L_from_G(hc, g, info)
+    assert info.status == 0
+    sets, (dfat, dlng) = O.Lattice(L).hisq_links_naik(LT.hisq_coeff_vector(hc), [u.astype(np.float64) for u in U],
+                                                      eps)
+    tol = 1e-10 if prec == "D" else 2e-6
+    for k in range(3):
+        fat, lng = q.extract_L(q.hisq_asqtad_links(h, k), V)
+        for mu in range(4):
+            assert site_rel_err(fat[mu], sets[k][0][mu]) <= tol, (k, mu)
+            assert site_rel_err(lng[mu], sets[k][1][mu]) <= tol, (k, mu)
+    deps = q.f("get_asqtad_deps_links_from_hisq")(h)
+    assert deps
+    fat, lng = q.extract_L(deps, V)
+    for mu in range(4):
+        assert site_rel_err(fat[mu], dfat[mu]) <= tol and site_rel_err(lng[mu], dlng[mu]) <= tol
+    assert q.set_hisq_opts(want_deps=0) == 0
+    q.hisq_destroy_L(h)
+    q.destroy_G(g)
+
+
+@pytest.mark.parametrize("prec", ["D", "F"])
 def test_extract_load_roundtrip_and_scaling(prec):
     q = gpu_lattice(L, prec)
     fat, lng = asqtad_links(L, 0.3, 7)

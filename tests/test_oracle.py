@@ -316,3 +316,27 @@ def test_hisq_force_groups_and_projection():
         T = 0.5 * (A - np.conj(np.transpose(A, (0, 2, 1))))
         T -= np.trace(T, axis1=1, axis2=2)[:, None, None] / 3 * np.eye(3)
         assert np.max(np.abs(LT.to_complex(F[mu]) - T)) <= 1e-12 * np.max(np.abs(T))
+
+
+def test_hisq_eps_naik_sets_reduce_to_one_naik():
+    """The oracle's n_naiks > 1 link sets (lib/hisq_links_p.c:182-243): fn[0]
+    equals the n_naiks = 1 links, fn[k] - fn[0] is eps_k times the difference
+    links, and the difference links are the one-link + Naik smearing of W."""
+    L = (4, 4, 4, 4)
+    lat = O.Lattice(L)
+    U = lat.rephase_G(LT.random_gauge(L, 0.5, 9))
+    hc = LT.hisq_bench_coeffs()
+    hc.difference_one_link, hc.difference_naik = 0.0375, -0.0413
+    h = LT.hisq_coeff_vector(hc)
+    fat1, lng1, W, _ = lat.hisq_links(h, U, want_W=True)
+    sets, (dfat, dlng) = lat.hisq_links_naik(h, U, [0.0, 0.5, -0.25])
+    for mu in range(4):
+        assert np.array_equal(sets[0][0][mu], fat1[mu]) and np.array_equal(sets[0][1][mu], lng1[mu])
+        for k, e in ((1, 0.5), (2, -0.25)):
+            assert np.allclose(sets[k][0][mu] - fat1[mu], e * dfat[mu], atol=1e-14)
+            assert np.allclose(sets[k][1][mu] - lng1[mu], e * dlng[mu], atol=1e-14)
+    # difference links: 0.0375 W (one link only) and -0.0413 W W W (Naik)
+    df, dl = lat.make_imp_links([0.0375, 0, 0, 0, 0, -0.0413], W)
+    for mu in range(4):
+        assert np.array_equal(df[mu], dfat[mu]) and np.array_equal(dl[mu], dlng[mu])
+        assert np.allclose(dfat[mu], 0.0375 * np.asarray(W[mu]), atol=1e-14)

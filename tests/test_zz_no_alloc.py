@@ -17,6 +17,7 @@ import numpy as np
 import pytest
 
 from conftest import gpu_lattice
+from devmem import Memory
 from helpers import asqtad_links, site_rel_err
 from qopqdp_b200 import lattice as LT
 from qopqdp_b200.qop import QOP_info_t
@@ -36,42 +37,6 @@ def _fn(q):
 def _launches(q):
     q.lib.QOPB_launch_count.restype = C.c_ulonglong
     return int(q.lib.QOPB_launch_count())
-
-
-class _Memory:
-    """Device memory seen by the driver: the stream-ordered pool's used bytes
-    and their high-water mark (the library allocates its temporaries from
-    that pool), and the device's free memory (plain cudaMalloc)."""
-
-    def __init__(self):
-        from cuda.bindings import driver as d
-        self.d = d
-        assert d.cuInit(0)[0] == d.CUresult.CUDA_SUCCESS
-        err, dev = d.cuCtxGetDevice()
-        assert err == d.CUresult.CUDA_SUCCESS
-        err, self.pool = d.cuDeviceGetDefaultMemPool(dev)
-        assert err == d.CUresult.CUDA_SUCCESS
-
-    def _attr(self, a):
-        err, v = self.d.cuMemPoolGetAttribute(self.pool, a)
-        assert err == self.d.CUresult.CUDA_SUCCESS
-        return int(v)
-
-    def reset_high(self):
-        a = self.d.CUmemPool_attribute.CU_MEMPOOL_ATTR_USED_MEM_HIGH
-        err, = self.d.cuMemPoolSetAttribute(self.pool, a, self.d.cuuint64_t(0))
-        assert err == self.d.CUresult.CUDA_SUCCESS
-
-    def used(self):
-        return self._attr(self.d.CUmemPool_attribute.CU_MEMPOOL_ATTR_USED_MEM_CURRENT)
-
-    def high(self):
-        return self._attr(self.d.CUmemPool_attribute.CU_MEMPOOL_ATTR_USED_MEM_HIGH)
-
-    def free(self):
-        err, free, _ = self.d.cuMemGetInfo()
-        assert err == self.d.CUresult.CUDA_SUCCESS
-        return int(free)
 
 
 def _check_against_allocating(q, L, mass, seed, calls=2):
@@ -123,7 +88,7 @@ def test_noalloc_allocates_nothing():
     hin, hout = q.create_V(src), q.create_V(np.zeros_like(src))
     info = QOP_info_t()
     assert fn(C.byref(info), fla, 0.05, hout, hin, 0) > 0      # first call: scratch address lookup
-    mem = _Memory()
+    mem = Memory()
     # the measurement sees the allocating entry point's temporary
     used0 = mem.used()
     mem.reset_high()
