@@ -163,7 +163,8 @@ int QOPB_serve_stop(void);   /* finishes queued requests, joins the worker */
    fused-update second hop, variants 20..28); sums = |t|^2, |p|^2, <p, Ap>,
    |Ap|^2 as the kernels reduced them (the last two for kind 3 only).
    QOPB_D3_sloppy_ddagd_batch: n <= 16 systems sharing the link stream;
-   variant = a batch_kernel value (0..15) or -1 for the solver's default;
+   variant = a batch_kernel value (0..15: int16 vectors; 16: the tensor-core
+   hop on bf16 hi / lo vectors) or -1 for the solver's default;
    sums[2j], sums[2j+1] = |t_j|^2 and <p_j, A_j p_j>.  Both return 0, or -1
    with info->status = QOP_FAIL. */
 int QOPB_D3_sloppy_ddagd(QOP_info_t *info, QOP_D3_FermionLinksAsqtad *asqtad, double mass,

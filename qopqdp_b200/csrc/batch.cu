@@ -28,6 +28,7 @@
 #include "prof.cuh"
 #include "fields.cuh"
 #include "mixed.cuh"
+#include "bmma.cuh"
 #include <algorithm>
 #include <array>
 #include <map>
@@ -361,7 +362,11 @@ struct BatchEngine::Impl {
   Range is;
   NbrGeom ng;
   int nsb, gridv;
+  // vectors: int16 records [system][Vh], or with the tensor-core hop
+  // (batch_kernel 16, tc) bf16 hi / lo records [Vh][16] (bmma.cuh)
+  bool tc = false;
   uint4 *rs = nullptr, *ps = nullptr, *Aps = nullptr, *ts = nullptr;
+  B16Rec *brs = nullptr, *bps = nullptr, *bAps = nullptr, *bts = nullptr;
   float2 *xs = nullptr;
   c2<double> *r = nullptr, *Ax = nullptr, *tmp = nullptr;
   double *part = nullptr;
@@ -382,13 +387,16 @@ struct BatchEngine::Impl {
   };
   std::vector<Sys> sys;
   std::vector<int> done_now;   // started at their target: reported by the next step
-  static size_t npart(int cap, int nsb, int gridv) {
-    // k_bhop: (groups x BG <= cap + 15) x site blocks; k_bupdate: cap x gridv
+  static size_t npart(int cap, int nsb, int gridv, bool tc) {
+    // k_bhop: (groups x BG <= cap + 15) x site blocks; k_bupdate: cap x gridv;
+    // the tensor-core kernels: 16 per block
+    if (tc) return bmma_part_doubles();
     return std::max<size_t>((size_t)(cap + 15) * nsb, (size_t)cap * gridv);
   }
   void release_all() {
     if (own) cudaStreamSynchronize(own);   // nothing of ours in flight when the memory goes back
     dfree(rs); dfree(ps); dfree(Aps); dfree(ts); dfree(xs); dfree(r); dfree(Ax); dfree(tmp);
+    dfree(brs); dfree(bps); dfree(bAps); dfree(bts);
     dfree(part); dfree(count); dfree(dst);
     if (h) cudaFreeHost(h);
     if (hd) cudaFreeHost(hd);
@@ -408,10 +416,15 @@ struct BatchEngine::Impl {
   }
 };
 
+static bool use_tc() { return ctx().opt.batch_kernel == 16; }
+
 size_t BatchEngine::bytes(const Geom &g, int cap) {
   const int nsb = (int)((g.Vh + QB - 1) / QB), gridv = grid_for(g.Vh, 256);
-  return (size_t)cap * g.Vh * (4 * sizeof(uint4) + 3 * sizeof(float2)) + 3 * sizeof(c2<double>) * vec_elems(g) +
-         sizeof(double) * Impl::npart(cap, nsb, gridv) + (sizeof(unsigned) + sizeof(MixState)) * cap;
+  const bool tc = use_tc();
+  const size_t vec = tc ? (size_t)BSYS * g.Vh * (4 * sizeof(B16Rec) + 3 * sizeof(float2))
+                        : (size_t)cap * g.Vh * (4 * sizeof(uint4) + 3 * sizeof(float2));
+  return vec + 3 * sizeof(c2<double>) * vec_elems(g) + sizeof(double) * Impl::npart(cap, nsb, gridv, tc) +
+         (sizeof(unsigned) + sizeof(MixState)) * cap;
 }
 
 BatchEngine::BatchEngine(FlaT<double> *f, int eo, int cap, bool own_stream) : d(new Impl()) {
@@ -442,16 +455,26 @@ BatchEngine::BatchEngine(FlaT<double> *f, int eo, int cap, bool own_stream) : d(
     }
     sloppy_get(f, LK_Q16);   // the int16 link copy, built on first use
     const i64 Vh = e.Vh;
-    e.rs = dalloc<uint4>(cap * Vh);
-    e.ps = dalloc<uint4>(cap * Vh);
-    e.Aps = dalloc<uint4>(cap * Vh);
-    e.ts = dalloc<uint4>(cap * Vh);
-    e.xs = dalloc<float2>(3 * cap * Vh);
-    dzero(e.xs, sizeof(float2) * 3 * cap * Vh);
+    e.tc = use_tc();
+    if (e.tc) {
+      e.brs = dalloc<B16Rec>(BSYS * Vh);
+      e.bps = dalloc<B16Rec>(BSYS * Vh);
+      e.bAps = dalloc<B16Rec>(BSYS * Vh);
+      e.bts = dalloc<B16Rec>(BSYS * Vh);
+      e.xs = dalloc<float2>(3 * BSYS * Vh);
+      dzero(e.xs, sizeof(float2) * 3 * BSYS * Vh);
+    } else {
+      e.rs = dalloc<uint4>(cap * Vh);
+      e.ps = dalloc<uint4>(cap * Vh);
+      e.Aps = dalloc<uint4>(cap * Vh);
+      e.ts = dalloc<uint4>(cap * Vh);
+      e.xs = dalloc<float2>(3 * cap * Vh);
+      dzero(e.xs, sizeof(float2) * 3 * cap * Vh);
+    }
     e.r = dalloc<c2<double>>(vec_elems(g));
     e.Ax = dalloc<c2<double>>(vec_elems(g));
     e.tmp = dalloc<c2<double>>(vec_elems(g));
-    e.part = dalloc<double>(Impl::npart(cap, e.nsb, e.gridv));
+    e.part = dalloc<double>(Impl::npart(cap, e.nsb, e.gridv, e.tc));
     e.count = dalloc<unsigned>(cap);
     dzero(e.count, sizeof(unsigned) * cap);
     e.dst = dalloc<MixState>(cap);
@@ -529,10 +552,17 @@ void BatchEngine::start(int s, c2<double> *x, const c2<double> *b, double mass, 
     e.done_now.push_back(s);
     return;
   }
-  k_to_sloppy<SpQ16><<<e.gridv, 256, 0, c.s>>>(e.rs + s * Vh, (x_zero ? b : e.r) + e.is.off, Vh);
-  k_copy_elems<uint4><<<grid_for(Vh, 256), 256, 0, c.s>>>(e.ps + s * Vh, e.rs + s * Vh, Vh);
-  QLAUNCHN(2);
-  dzero(e.xs + 3 * s * Vh, sizeof(float2) * 3 * Vh);
+  if (e.tc) {
+    k_b16_from_f64<<<e.gridv, 256, 0, c.s>>>(e.brs, s, (x_zero ? b : e.r) + e.is.off, Vh);
+    k_b16_copy_sys<<<e.gridv, 256, 0, c.s>>>(e.bps, e.brs, s, Vh);
+    k_b16_zero_x<<<e.gridv, 256, 0, c.s>>>(e.xs, s, Vh);
+    QLAUNCHN(3);
+  } else {
+    k_to_sloppy<SpQ16><<<e.gridv, 256, 0, c.s>>>(e.rs + s * Vh, (x_zero ? b : e.r) + e.is.off, Vh);
+    k_copy_elems<uint4><<<grid_for(Vh, 256), 256, 0, c.s>>>(e.ps + s * Vh, e.rs + s * Vh, Vh);
+    QLAUNCHN(2);
+    dzero(e.xs + 3 * s * Vh, sizeof(float2) * 3 * Vh);
+  }
   st.rsq = st.rsq_old = st.maxr2 = y.r2;
   st.flag = MIX_RUN;
 }
@@ -570,6 +600,39 @@ void BatchEngine::launch() {
   // at 24^3x48: 1696 ms per call against 1989 ms with groups of 8 and 4);
   // batch_kernel -2: the fastest of 1, 6, 7, 9, 12 timed on the first step
   // with this lattice and number of systems
+  const double link_site = recon ? (nl / 2) * (40.0 + 28.0) : nl * 40.0;
+  const int chunk = c.opt.chunk;
+  std::vector<int> recs;
+  if (e.tc) {
+    // tensor-core hop: bf16 hi / lo records of 24 bytes per system and site
+    char tname[32];
+    snprintf(tname, sizeof tname, "bhop_mma_x%d", n);
+    const double tb = (double)Vh * (link_site + 2.0 * 24 * active);
+    for (int k = 0; k < chunk; k++) {
+      {
+        ProfScope s1(tname, tb);
+        launch_bmma_hop(1, nl, recon, c_long, e.bts, e.bps, (const unsigned char *)lk_q.a, nullptr, g, e.ng, q, e.dst,
+                        n, e.part, e.count);
+        QLAUNCH();
+        recs.push_back(s1.idx);
+      }
+      {
+        ProfScope s2(tname, tb + (double)Vh * 24 * active);
+        launch_bmma_hop(2, nl, recon, c_long, e.bAps, e.bts, (const unsigned char *)lk_p.a, e.bps, g, e.ng, p,
+                        e.dst, n, e.part, e.count);
+        QLAUNCH();
+        recs.push_back(s2.idx);
+      }
+      launch_b16_update(e.xs, e.brs, e.bps, e.bAps, Vh, e.dst, n, e.part, e.count);
+      launch_b16_p(e.bps, e.brs, Vh, e.dst, n);
+      QLAUNCHN(2);
+    }
+    QCHECK(cudaMemcpyAsync(e.hd, e.dst, sizeof(MixState) * n, cudaMemcpyDeviceToHost, c.s));
+    e.recs.swap(recs);
+    e.launched_n = n;
+    e.inflight = true;
+    return;
+  }
   int variant = c.opt.batch_kernel == -1 ? (n % 8 == 0 ? 7 : 1) : std::min(c.opt.batch_kernel, N_BHOP - 1);
   if (c.opt.batch_kernel == -2) {
     const std::array<int, 7> key{g.L[0], g.L[1], g.L[2], g.L[3], nl, recon ? 1 : 0, n};
@@ -590,13 +653,10 @@ void BatchEngine::launch() {
   }
   const int BG = kBhop[variant].bg;
   const int ngrp = (n + BG - 1) / BG;
-  const int chunk = c.opt.chunk;
   char hname[32];
   snprintf(hname, sizeof hname, "bhop_q16_x%d", n);
-  const double link_site = recon ? (nl / 2) * (40.0 + 28.0) : nl * 40.0;
   // compulsory bytes of one hop for the systems running in this chunk
   const double hop_bytes = (double)Vh * (link_site + 2.0 * 16 * active);
-  std::vector<int> recs;
   for (int k = 0; k < chunk; k++) {
     {
       ProfScope s1(hname, hop_bytes);
@@ -651,7 +711,8 @@ std::vector<int> BatchEngine::collect() {
     if (s.flag != MIX_UPDATE && s.flag != MIX_BREAK) continue;
     y.stalls = ran == 0 ? y.stalls + 1 : 0;   // repeated breakdown without progress
     // reliable update: fold the sloppy solution into FP64, true residual
-    k_fold_x<<<grid_for(3 * Vh, 256), 256, 0, c.s>>>(y.x + e.is.off, e.xs + 3 * j * Vh, 3 * Vh);
+    if (e.tc) k_b16_fold_x<<<gridv, 256, 0, c.s>>>(y.x + e.is.off, e.xs, j, Vh);
+    else k_fold_x<<<grid_for(3 * Vh, 256), 256, 0, c.s>>>(y.x + e.is.off, e.xs + 3 * j * Vh, 3 * Vh);
     QLAUNCH();
     y.r2 = e.true_resid(j);
     need_finite(y.r2, "batched solver: true residual norm");
@@ -665,13 +726,15 @@ std::vector<int> BatchEngine::collect() {
     }
     const bool broke = s.flag == MIX_BREAK || !(s.rsq_old > 0);
     const double rsq_prev = s.rsq_old;
-    k_to_sloppy<SpQ16><<<gridv, 256, 0, c.s>>>(e.rs + j * Vh, e.r + e.is.off, Vh);
+    if (e.tc) k_b16_from_f64<<<gridv, 256, 0, c.s>>>(e.brs, j, e.r + e.is.off, Vh);
+    else k_to_sloppy<SpQ16><<<gridv, 256, 0, c.s>>>(e.rs + j * Vh, e.r + e.is.off, Vh);
     QLAUNCH();
     s.rsq = y.r2;
     s.maxr2 = y.r2;
     s.flag = MIX_RUN;
     if (broke) {   // restart the recursion from the true residual
-      k_copy_elems<uint4><<<grid_for(Vh, 256), 256, 0, c.s>>>(e.ps + j * Vh, e.rs + j * Vh, Vh);
+      if (e.tc) k_b16_copy_sys<<<gridv, 256, 0, c.s>>>(e.bps, e.brs, j, Vh);
+      else k_copy_elems<uint4><<<grid_for(Vh, 256), 256, 0, c.s>>>(e.ps + j * Vh, e.rs + j * Vh, Vh);
       QLAUNCH();
     } else {
       s.beta = y.r2 / rsq_prev;
@@ -680,7 +743,8 @@ std::vector<int> BatchEngine::collect() {
   }
   QCHECK(cudaMemcpyAsync(e.dst, h, sizeof(MixState) * n, cudaMemcpyHostToDevice, c.s));
   for (int j : pupd) {
-    k_bp<<<dim3(gridv, 1), 256, 0, c.s>>>(e.ps + j * Vh, e.rs + j * Vh, Vh, e.dst + j);
+    if (e.tc) launch_b16_p(e.bps, e.brs, Vh, e.dst, n, j);
+    else k_bp<<<dim3(gridv, 1), 256, 0, c.s>>>(e.ps + j * Vh, e.rs + j * Vh, Vh, e.dst + j);
     QLAUNCH();
   }
   return fin;
@@ -710,14 +774,90 @@ namespace qopb {
 __global__ void k_q16_to_f64(double2 *d, const uint4 *s, i64 Vh);   // mixed.cu
 }
 
-// The batched int16 operator of the batched solver, applied once with its
-// own hop kernels to n <= 16 systems: p_j = int16(in_j) on parity eo,
-// t_j = D_oe p_j, Ap_j = m_j^2 p_j - D_eo t_j; t_j and Ap_j are decoded
-// into t_out[j] / ap_out[j].  sums[2j], sums[2j+1] = |t_j|^2 and
-// <p_j, A_j p_j> = |t_j|^2 + m_j^2 |p_j|^2 as the kernels reduced them.  variant: a batch_kernel value (0..15), or
-// -1 for the solver's default choice for n systems.  Restates
-// QOP_asqtad_ddagd_norm2 (lib/asqtad_dslash_p.c:1121-1138) for several
-// vectors at once, as the reference's vectorised hop does
+// the check below for the tensor-core format (batch_kernel 16): p_j split
+// into bf16 hi / lo records, the two MMA hops, t_j and Ap_j decoded
+static int sloppy_ddagd_batch_tc(QOP_info_t *info, qopb::FlaT<double> *f, int n, const double *masses,
+                                 QOP_D3_ColorVector **t_out, QOP_D3_ColorVector **ap_out, QOP_D3_ColorVector **in,
+                                 QOP_evenodd_t eo, double *sums) {
+  using namespace qopb;
+  B16Rec *ps = nullptr, *ts = nullptr, *as = nullptr;
+  MixState *dst = nullptr;
+  double *part = nullptr;
+  unsigned *count = nullptr;
+  auto release = [&]() { dfree(ps); dfree(ts); dfree(as); dfree(dst); dfree(part); dfree(count); };
+  try {
+    Context &c = ctx();
+    const Geom &g = c.g;
+    const i64 Vh = g.Vh;
+    const int p = eo, q = 1 - eo, gridv = grid_for(Vh, 256);
+    SloppyLinks *sl = sloppy_get(f, LK_Q16);
+    const LinksSloppy lk_p = links_parity(sl, LK_Q16, p), lk_q = links_parity(sl, LK_Q16, q);
+    ps = dalloc<B16Rec>(BSYS * Vh);
+    ts = dalloc<B16Rec>(BSYS * Vh);
+    as = dalloc<B16Rec>(BSYS * Vh);
+    dst = dalloc<MixState>(n);
+    part = dalloc<double>(bmma_part_doubles());
+    count = dalloc<unsigned>(1);
+    dzero(count, sizeof(unsigned));
+    std::vector<MixState> h(n);
+    for (int j = 0; j < n; j++) {
+      h[j] = MixState{};
+      h[j].flag = MIX_RUN;
+      h[j].m2 = masses[j] * masses[j];
+      h[j].rsq = h[j].rsq_old = h[j].maxr2 = 1.0;
+      h[j].max_iter = 1 << 30;
+      k_b16_from_f64<<<gridv, 256, 0, c.s>>>(ps, j, reinterpret_cast<VecT<double> *>(in[j])->d + par_off(g, p), Vh);
+      QLAUNCH();
+    }
+    QCHECK(cudaMemcpyAsync(dst, h.data(), sizeof(MixState) * n, cudaMemcpyHostToDevice, c.s));
+    NbrGeom ng;
+    for (int d = 0; d < 4; d++) ng.L[d] = g.L[d];
+    ng.str[3] = 1; ng.str[2] = g.L[3]; ng.str[1] = g.L[2] * g.L[3]; ng.str[0] = g.L[1] * g.L[2] * g.L[3];
+    const double tb = (double)Vh * ((sl->recon ? (sl->nl / 2) * (40.0 + 28.0) : sl->nl * 40.0) + 2.0 * 24 * n);
+    {
+      ProfScope s1("check_bhop_mma", tb);
+      launch_bmma_hop(1, sl->nl, sl->recon != 0, (float)sl->c_long, ts, ps, (const unsigned char *)lk_q.a, nullptr,
+                      g, ng, q, dst, n, part, count);
+      QLAUNCH();
+    }
+    {
+      ProfScope s2("check_bhop_mma", tb + (double)Vh * 24 * n);
+      launch_bmma_hop(2, sl->nl, sl->recon != 0, (float)sl->c_long, as, ts, (const unsigned char *)lk_p.a, ps, g,
+                      ng, p, dst, n, part, count);
+      QLAUNCH();
+    }
+    for (int j = 0; j < n; j++) {
+      k_b16_to_f64<<<gridv, 256, 0, c.s>>>(reinterpret_cast<VecT<double> *>(t_out[j])->d + par_off(g, q), ts, j, Vh);
+      k_b16_to_f64<<<gridv, 256, 0, c.s>>>(reinterpret_cast<VecT<double> *>(ap_out[j])->d + par_off(g, p), as, j, Vh);
+      QLAUNCHN(2);
+    }
+    QCHECK(cudaMemcpyAsync(h.data(), dst, sizeof(MixState) * n, cudaMemcpyDeviceToHost, c.s));
+    sync();
+    if (sums)
+      for (int j = 0; j < n; j++) {
+        sums[2 * j] = h[j].dp2;
+        sums[2 * j + 1] = h[j].alpha > 0 ? 1.0 / h[j].alpha : 0.0;
+      }
+    release();
+    if (info) info->status = QOP_SUCCESS;
+    return 0;
+  } catch (Fail &e) {
+    release();
+    fprintf(stderr, "QOPB_D3_sloppy_ddagd_batch: %s\n", e.msg.c_str());
+    if (info) info->status = e.status;
+    return -1;
+  }
+}
+
+// The batched reduced-precision operator of the batched solver, applied
+// once with its own hop kernels to n <= 16 systems: p_j = sloppy(in_j) on
+// parity eo, t_j = D_oe p_j, Ap_j = m_j^2 p_j - D_eo t_j; t_j and Ap_j are
+// decoded into t_out[j] / ap_out[j].  sums[2j], sums[2j+1] = |t_j|^2 and
+// <p_j, A_j p_j> = |t_j|^2 + m_j^2 |p_j|^2 as the kernels reduced them.
+// variant: a batch_kernel value (0..15: int16 vectors; 16: the tensor-core
+// hop on bf16 hi / lo vectors), or -1 for the solver's default choice for n
+// systems.  Restates QOP_asqtad_ddagd_norm2 (lib/asqtad_dslash_p.c:1121-1138)
+// for several vectors at once, as the reference's vectorised hop does
 // (lib/asqtad_dslash_p.c:1246-1279); it exists so that the batched sloppy
 // operator can be compared site by site with FP64.
 extern "C" int QOPB_D3_sloppy_ddagd_batch(QOP_info_t *info, QOP_D3_FermionLinksAsqtad *asqtad, int n,
@@ -742,8 +882,11 @@ extern "C" int QOPB_D3_sloppy_ddagd_batch(QOP_info_t *info, QOP_D3_FermionLinksA
       handle_check(in[j], "ColorVector");
     }
     if (eo != QOP_EVEN && eo != QOP_ODD) fail(QOP_FAIL, "QOPB_D3_sloppy_ddagd_batch: eo must be EVEN or ODD");
-    if (variant < -1 || variant >= N_BHOP)
-      fail(QOP_FAIL, "QOPB_D3_sloppy_ddagd_batch: variant %d (-1..%d)", variant, N_BHOP - 1);
+    if (variant < -1 || variant > N_BHOP)
+      fail(QOP_FAIL, "QOPB_D3_sloppy_ddagd_batch: variant %d (-1..%d)", variant, N_BHOP);
+    if (variant == N_BHOP)
+      return sloppy_ddagd_batch_tc(info, reinterpret_cast<FlaT<double> *>(asqtad), n, masses, t_out, ap_out, in, eo,
+                                   sums);
     if (variant < 0) variant = n % 8 == 0 ? 7 : 1;
     FlaT<double> *f = reinterpret_cast<FlaT<double> *>(asqtad);
     Context &c = ctx();
@@ -778,12 +921,19 @@ extern "C" int QOPB_D3_sloppy_ddagd_batch(QOP_info_t *info, QOP_D3_FermionLinksA
     ng.str[3] = 1; ng.str[2] = g.L[3]; ng.str[1] = g.L[2] * g.L[3]; ng.str[0] = g.L[1] * g.L[2] * g.L[3];
     const bool recon = sl->recon != 0;
     const float c_long = (float)sl->c_long;
-    launch_bhop<1>(variant, sl->nl, recon, ngrp, nsb, ts, ps, (const unsigned char *)lk_q.a, nullptr, g, ng, q, dst, n,
-                   part, count, c_long);
-    QLAUNCH();
-    launch_bhop<2>(variant, sl->nl, recon, ngrp, nsb, as, ts, (const unsigned char *)lk_p.a, ps, g, ng, p, dst, n,
-                   part, count, c_long);
-    QLAUNCH();
+    const double tb = (double)Vh * ((recon ? (sl->nl / 2) * (40.0 + 28.0) : sl->nl * 40.0) + 2.0 * 16 * n);
+    {
+      ProfScope s1("check_bhop_q16", tb);
+      launch_bhop<1>(variant, sl->nl, recon, ngrp, nsb, ts, ps, (const unsigned char *)lk_q.a, nullptr, g, ng, q, dst,
+                     n, part, count, c_long);
+      QLAUNCH();
+    }
+    {
+      ProfScope s2("check_bhop_q16", tb + (double)Vh * 16 * n);
+      launch_bhop<2>(variant, sl->nl, recon, ngrp, nsb, as, ts, (const unsigned char *)lk_p.a, ps, g, ng, p, dst, n,
+                     part, count, c_long);
+      QLAUNCH();
+    }
     for (int j = 0; j < n; j++) {
       k_q16_to_f64<<<gridv, 256, 0, c.s>>>(reinterpret_cast<VecT<double> *>(t_out[j])->d + par_off(g, q), ts + j * Vh,
                                           Vh);

@@ -305,7 +305,7 @@ QOP_status_t QOP_asqtad_invert_set_opts(QOP_opt_t opts[], int nopts) {
       if (p != 16 && p != 32 && p != 64) return QOP_FAIL;
       n.sloppy_prec = p;
     } else if (!strcmp(t, "batch_kernel")) {
-      if (v < -2 || v > 15) return QOP_FAIL;
+      if (v < -2 || v > 16) return QOP_FAIL;   // 16: the tensor-core hop (bmma.cu)
       n.batch_kernel = (int)v;
     } else if (!strcmp(t, "multi_shift")) {
       n.multi_shift = v != 0;

@@ -74,6 +74,24 @@ def quantize_vector(v):
     return dec(_q16(re, inv)) + 1j * dec(_q16(im, inv))
 
 
+def _bf16(x):
+    """float32 -> bfloat16 (round to nearest even), returned as float32"""
+    b = np.asarray(x, dtype=F32).view(np.uint32).astype(np.uint64)
+    b = (b + 0x7FFF + ((b >> 16) & 1)) & 0xFFFF0000
+    return b.astype(np.uint32).view(F32)
+
+
+def split_vector(v):
+    """site vectors as the tensor-core batched solver stores them: float32
+    values split into bf16 hi + lo (hi + lo is exact in float32)."""
+    def one(x):
+        x = x.astype(F32)
+        hi = _bf16(x)
+        lo = _bf16((x - hi).astype(F32))
+        return hi.astype(np.float64) + lo.astype(np.float64)
+    return one(v.real) + 1j * one(v.imag)
+
+
 def _recon_ok(longs):
     """the device's test for rebuilding row 2: unitarity defect and |c| spread below 1e-7."""
     c2 = np.concatenate([(np.abs(u[:, 0, :]) ** 2).sum(axis=1) for u in longs])

@@ -180,11 +180,13 @@ def test_mixed_multi_mass_iterations(multi_shift):
     q.destroy_L(fla)
 
 
+@pytest.mark.parametrize("bk", [-1, 16])
 @pytest.mark.parametrize("L,kind", [((8, 8, 8, 8), "asqtad"), ((4, 4, 4, 8), "hisq")])
-def test_mixed_multi_source(L, kind):
+def test_mixed_multi_source(L, kind, bk):
     """Many sources, one mass each (some masses repeated, one zero source),
-    odd parity: the batched int16 solver meets every FP64 tolerance, returns
-    m A^{-1} b like the oracle, and a zero source gives a zero solution."""
+    odd parity: the batched solver (int16 hop, or the tensor-core hop with
+    batch_kernel 16) meets every FP64 tolerance, returns m A^{-1} b like the
+    oracle, and a zero source gives a zero solution."""
     V = int(np.prod(L))
     q = gpu_lattice(L, "D")
     if kind == "asqtad":
@@ -198,13 +200,13 @@ def test_mixed_multi_source(L, kind):
     srcs = [LT.gaussian_vector(L, 400 + s) for s in range(nsrc - 1)]
     srcs.append(np.zeros_like(srcs[0]))
     masses = [[0.03], [0.03], [0.05], [0.08], [0.2], [0.05]]
-    assert q.set_opts(prec_sloppy=16) == 0
+    assert q.set_opts(prec_sloppy=16, batch_kernel=bk) == 0
     ras = [[QOP_resid_arg_t(rsq, 0, 0, 0, 0, 0)] for _ in range(nsrc)]
     hins = [q.create_V(s) for s in srcs]
     houts = [[q.create_V(np.zeros_like(srcs[0]))] for _ in range(nsrc)]
     ia = QOP_invert_arg_t(1e9, 20000, 20000, 20, 1)
     info = q.invert_multi(fla, masses, houts, hins, ia, ras)
-    assert q.set_opts(prec_sloppy=64) == 0
+    assert q.set_opts(prec_sloppy=64, batch_kernel=-1) == 0
     assert info.status == 0
     for s in range(nsrc):
         got = q.extract_V(houts[s][0], V)
@@ -315,9 +317,10 @@ def test_programmatic_dependent_launch_solves_like_the_default():
 
 
 def test_every_batch_kernel_variant():
-    """Each selectable batched hop (option batch_kernel 0-15) solves a
-    four-source batch to the FP64 target with the iteration counts of the
-    default variant."""
+    """Each selectable batched hop (option batch_kernel 0-15 on int16 vectors,
+    16 the tensor-core hop on bf16 hi / lo vectors) solves a four-source
+    batch to the FP64 target with the iteration counts of the default
+    variant."""
     L = (8, 8, 8, 8)
     q = gpu_lattice(L, "D")
     fat, lng = asqtad_links(L, 0.4, 11)
@@ -326,15 +329,16 @@ def test_every_batch_kernel_variant():
     srcs = [LT.gaussian_vector(L, 340 + s) for s in range(4)]
     ms = [[0.03], [0.05], [0.03], [0.1]]
     its = {}
-    for v in range(16):
+    for v in range(17):
         assert q.set_opts(prec_sloppy=16, batch_kernel=v) == 0
         info, ras, outs = _run_multi(q, fla, ms, srcs, 1e-20)
         assert info.status == 0
         for s in range(4):
             assert eo_residual(fo, ms[s][0], outs[s][0], srcs[s], L, 0) <= 1.05e-20, (v, s)
         its[v] = [r[0].final_iter for r in ras]
-    assert q.set_opts(batch_kernel=16) != 0
+    assert q.set_opts(batch_kernel=17) != 0
     assert q.set_opts(prec_sloppy=64, batch_kernel=-1) == 0
+    print("batched iterations per variant", its)
     for v, it in its.items():
         assert all(abs(a - b) <= 0.03 * b + 3 for a, b in zip(it, its[7])), its
     q.destroy_L(fla)
@@ -392,11 +396,13 @@ def test_mixed_ragged_site_blocks(L):
     assert q.set_opts(prec_sloppy=16) == 0
     st, _, got = _single_iters(q, fla, srcs[0], 0.05, L)
     assert st == 0 and eo_residual(fo, 0.05, got, srcs[0], L, 0) <= 1.05e-20
-    info, ras, outs = _run_multi(q, fla, [[0.05], [0.1], [0.05]], srcs, 1e-20)
-    assert info.status == 0
-    for s, m in enumerate([0.05, 0.1, 0.05]):
-        assert eo_residual(fo, m, outs[s][0], srcs[s], L, 0) <= 1.05e-20
-        ref, _ = fo.invert(m, srcs[s], O.InvertArg(1e9, 20000, 20000, 5, 0), O.ResidArg(1e-20, 0, 0, 0, 0, 0))
-        assert rel_norm_err(half(outs[s][0], L, 0), half(ref, L, 0)) <= max(1e-6, 30 * 1e-10 / m ** 2)
-    assert q.set_opts(prec_sloppy=64) == 0
+    for bk in (-1, 16):      # int16 and tensor-core batched hops
+        assert q.set_opts(batch_kernel=bk) == 0
+        info, ras, outs = _run_multi(q, fla, [[0.05], [0.1], [0.05]], srcs, 1e-20)
+        assert info.status == 0
+        for s, m in enumerate([0.05, 0.1, 0.05]):
+            assert eo_residual(fo, m, outs[s][0], srcs[s], L, 0) <= 1.05e-20
+            ref, _ = fo.invert(m, srcs[s], O.InvertArg(1e9, 20000, 20000, 5, 0), O.ResidArg(1e-20, 0, 0, 0, 0, 0))
+            assert rel_norm_err(half(outs[s][0], L, 0), half(ref, L, 0)) <= max(1e-6, 30 * 1e-10 / m ** 2)
+    assert q.set_opts(prec_sloppy=64, batch_kernel=-1) == 0
     q.destroy_L(fla)

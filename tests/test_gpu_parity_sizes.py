@@ -12,7 +12,9 @@
   |got - ref| <= 4e-5 |ref| + 1e-6 sum_k |U_k| |v_k| per site.  The norm-wise
   distance to the unquantised FP64 operator is checked too (<= 2^-12).
 * The 16-system batched hop (default 8 systems per thread) and the 12-system
-  shape (4 per thread) on the same lattice, system by system.
+  shape (4 per thread) on the same lattice, system by system, and the
+  tensor-core hop (batch_kernel 16: mma.sync on bf16 hi / lo operands) with
+  16, 12 and 3 systems against the same FP64 operator on its own storage.
 """
 import itertools
 
@@ -81,21 +83,30 @@ def big_hisq():
     return fat, lng, geo, dbl, dq, recon
 
 
-def _check_sloppy(geo, dbl, dq, mass, src, t_got, a_got, eo, label):
+# per-site bounds (tests/q16ref.py site_err): int16 vectors round the output
+# to 15 bits of the site's largest component; the tensor-core form stores
+# bf16 hi + lo (16 bits of each component) and represents the int16 links as
+# bf16 hi + lo too (2^-17 of each element) and drops lo . lo (2^-18 of each
+# product), so its arithmetic term is larger and its output term smaller
+BOUNDS = {"q16": dict(out_scale=4e-5, acc_scale=1e-6), "b16": dict(out_scale=1e-5, acc_scale=1.5e-5)}
+
+
+def _check_sloppy(geo, dbl, dq, mass, src, t_got, a_got, eo, label, fmt="q16"):
     V = geo.V
     q_, p_ = 1 - eo, eo
     sq, sp = R.parity_sites(V, q_), R.parity_sites(V, p_)
     p = np.zeros((V, 3), complex)
-    p[sp] = R.quantize_vector(R.cplx(src)[sp])
+    p[sp] = (R.quantize_vector if fmt == "q16" else R.split_vector)(R.cplx(src)[sp])
     # first hop on exactly the stored p and links
     t_ref, t_mag = R.hop(geo, dq, p, sq)
-    e1 = R.site_err(R.cplx(t_got)[sq], t_ref, t_mag)
+    e1 = R.site_err(R.cplx(t_got)[sq], t_ref, t_mag, **BOUNDS[fmt])
     # second hop on exactly the stored t (the device's own output)
     t = np.zeros((V, 3), complex)
     t[sq] = R.cplx(t_got)[sq]
     h2, m2mag = R.hop(geo, dq, t, sp)
     a_ref = mass * mass * p[sp] - h2
-    e2 = R.site_err(R.cplx(a_got)[sp], a_ref, m2mag + mass * mass * np.sqrt((np.abs(p[sp]) ** 2).sum(axis=1)))
+    e2 = R.site_err(R.cplx(a_got)[sp], a_ref, m2mag + mass * mass * np.sqrt((np.abs(p[sp]) ** 2).sum(axis=1)),
+                    **BOUNDS[fmt])
     # distance to the unquantised FP64 operator
     x = np.zeros((V, 3), complex)
     x[sp] = R.cplx(src)[sp]
@@ -143,7 +154,7 @@ def test_int16_operator_matches_fp64_per_site_24x24x24x24(big_hisq, variant, kin
     q.destroy_L(fla)
 
 
-@pytest.mark.parametrize("n,variant", [(16, -1), (12, -1), (16, 12)])
+@pytest.mark.parametrize("n,variant", [(16, -1), (12, -1), (16, 12), (16, 16), (12, 16), (3, 16)])
 def test_batched_int16_operator_matches_fp64_per_site_24x24x24x24(big_hisq, n, variant):
     fat, lng, geo, dbl, dq, recon = big_hisq
     q = gpu_lattice(BIG, "D")
@@ -157,11 +168,12 @@ def test_batched_int16_operator_matches_fp64_per_site_24x24x24x24(big_hisq, n, v
     ha = [q.create_V(np.zeros_like(srcs[0])) for _ in range(n)]
     st, sums = q.sloppy_ddagd_batch(fla, masses, ht, ha, hin, eo, variant)
     assert st == 0
-    for j in (0, n // 2, n - 1):      # first, middle and last system of the launch
+    fmt = "b16" if variant == 16 else "q16"
+    for j in sorted({0, n // 2, n - 1}):      # first, middle and last system of the launch
         t, p = _check_sloppy(geo, dbl, dq, masses[j], srcs[j], q.extract_V(ht[j], V), q.extract_V(ha[j], V), eo,
-                             "batch n %d variant %d system %d" % (n, variant, j))
+                             "batch n %d variant %d system %d" % (n, variant, j), fmt)
         t2 = (np.abs(t) ** 2).sum()
-        # the batched hop reduces |t|^2 before rounding t to int16
+        # the batched hops reduce |t|^2 before rounding t to its storage
         assert abs(sums[j][0] - t2) <= 1e-4 * t2
         pap = t2 + masses[j] ** 2 * (np.abs(p) ** 2).sum()
         assert abs(sums[j][1] - pap) <= 1e-4 * pap
