@@ -75,8 +75,10 @@ def parse():
                     help="FP64 CG iterations of one solve, for the reference arm's solves/s (default: the "
                          "measured count of the headline workload)")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--prof-every", type=int, default=8,
-                    help="headline solve: bracket every n-th launch of each kernel class with CUDA events")
+    ap.add_argument("--prof-every", type=int, default=7,
+                    help="headline solve: bracket every n-th launch of each kernel class with CUDA events (odd n: "
+                         "the samples rotate over the positions in a 16-iteration chunk, so the first launch "
+                         "after each host check is not over-represented)")
     ap.add_argument("--quick", action="store_true", help="skip FP64 baseline and e2e (development)")
     ap.add_argument("--dd-mask", type=int, default=15, help="dd workload on one GPU: self-split directions")
     ap.add_argument("--hop-kernel", type=int, default=None, help="int16 hop variant (library default if unset)")

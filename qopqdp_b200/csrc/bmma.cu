@@ -101,9 +101,9 @@ k_bmma_hop(B16Rec *__restrict__ out, const B16Rec *__restrict__ src, const unsig
   // this lane's 8-byte word in a neighbour's record block: system g, colour
   // q.  Lanes q = 3 fill the padding columns k = 6, 7 of A with colour 2 of
   // their system (finite for a running system) instead of zero: B's rows
-  // 6, 7 are zero, so those products add exactly 0 and no load needs a
-  // predicate.  Rows of systems that are not running may hold anything: an
-  // MMA row affects only the same row of C, which is not stored.
+  // 6, 7 are zero, so those products add exactly 0.  Systems that are not
+  // running load nothing (late in a multi-mass solve most have finished):
+  // their A rows are zero, and an MMA row affects only the same row of C.
   const int lane_w = gq * 3 + (qq < 3 ? qq : 2);
   double acc0 = 0.0, acc1 = 0.0;
   const int nchunk = (int)((Vh + BM_SITES - 1) / BM_SITES);
@@ -176,8 +176,8 @@ k_bmma_hop(B16Rec *__restrict__ out, const B16Rec *__restrict__ src, const unsig
 #pragma unroll
         for (int u = 0; u < 4; u++) {
           const uint2 *ap = reinterpret_cast<const uint2 *>(src + (i64)nn[u] * BSYS) + lane_w;
-          ra[s + u][0] = __ldg(ap);
-          ra[s + u][1] = __ldg(ap + 24);
+          ra[s + u][0] = act0 ? __ldg(ap) : make_uint2(0u, 0u);
+          ra[s + u][1] = act1 ? __ldg(ap + 24) : make_uint2(0u, 0u);
         }
       }
       // kind 2: p at the output site, requested with the fragments
