@@ -2,10 +2,10 @@
 
 Only the test suite, __graft_entry__.smoke() and bench.py's CPU-baseline leg
 use this module, always as the checker or the timed CPU reference.  The
-oracle is a plain-C FP64 restatement of the reference's asqtad/HISQ path;
-see qop_oracle.h for the parity status (numerically unpinned: the reference
-needs the absent QDP/QLA/QMP libraries and ships no golden vectors; its
-check_op / check_resids identities are reproduced instead).
+oracle is a plain-C FP64 restatement of the reference's asqtad/HISQ path,
+pinned to the reference itself: refqop.py drives the reference's own
+sources compiled by oracle/ref, and tests/test_ref_pin.py compares the two
+(and this oracle with the reference's committed outputs under tests/golden).
 """
 import ctypes as C
 import os

@@ -5,9 +5,14 @@
  * names the reference file:line whose algorithm it restates.  The
  * reference's QDP field operations become plain site loops over host
  * arrays; its QLA site algebra becomes the small complex helpers below.
- * Parity: numerically unpinned (no golden vectors exist, and the reference
- * needs the absent QDP/QLA/QMP libraries); pinned to the reference's
- * check_op / check_resids identities (examples/asqtad_test.c:37-130).
+ * Parity: pinned to the reference itself.  oracle/ref compiles the
+ * reference's own asqtad/HISQ sources, unmodified, against a CPU stand-in
+ * for the QDP/QLA/QMP calls they make (oracle/_ref/libqopref.so);
+ * tests/test_ref_pin.py compares this file with that library (rephase,
+ * asqtad and HISQ links, the nine Dslash cases, invert, invert_multi) and
+ * with its committed outputs (tests/golden/qopref_4x4x4x4.npz); the
+ * reference's check_op / check_resids identities (examples/asqtad_test.c:
+ * 37-130) are checked too.
  */
 #include "qop_oracle.h"
 #include <complex.h>

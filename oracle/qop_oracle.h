@@ -5,12 +5,15 @@
  * asqtad/HISQ hot path.  It is the parity checker for the CUDA library and
  * the timed CPU baseline; nothing in the product links or calls it.
  *
- * Parity status: numerically UNPINNED.  The reference cannot be built here
- * (it needs the external QDP/C, QLA and QMP libraries, none present) and it
- * ships no golden vectors.  The oracle is pinned to the reference's own
- * self-consistency tests instead: examples/asqtad_test.c check_op (the
- * Dslash definition, sign and normalisation, rebuilt from unscaled links
- * and plain shifts) and check_resids (the eo-solve residual definition).
+ * Parity status: pinned to the reference itself.  The reference's sources
+ * need the external QDP/C, QLA and QMP libraries (absent); oracle/ref
+ * supplies a single-process CPU stand-in for the calls its asqtad/HISQ path
+ * makes and compiles those sources, unmodified, into
+ * oracle/_ref/libqopref.so.  tests/test_ref_pin.py checks this oracle
+ * against that library (links, Dslash, invert, invert_multi: rounding-level
+ * agreement, equal iteration counts) and against its committed outputs in
+ * tests/golden/qopref_4x4x4x4.npz.  The reference's own self-consistency
+ * tests (examples/asqtad_test.c check_op, check_resids) are checked too.
  *
  * Fields are host arrays of doubles in the reference raw layout:
  *   vector  : V x 3 x (re,im)       matrix : V x 3 x 3 x (re,im)
