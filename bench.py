@@ -50,9 +50,10 @@ PEAK_FALLBACK_GBS = 6650.0
 # Iterations of the plain FP64 CG (the reference algorithm) on the headline
 # workload (HISQ 32^3x64, eps 0.5, seed 2024, m 0.01, |r|/|b| <= 1e-10),
 # measured on a B200 with QOP_D3_asqtad_invert at prec_sloppy 64: 5920.
-# The CPU reference arm times a bounded number of oracle CG iterations and
-# scales by this count (a full FP64 CPU solve takes ~6 minutes on 16 host
-# threads); the device arm reports its own FP64 iteration count beside it.
+# The CPU reference arm times a bounded number of the reference's FP64 CG
+# iterations and scales by this count (a full FP64 CPU solve takes tens of
+# minutes on the host cores); the device arm reports its own FP64 iteration
+# count beside it.
 FP64_ITERS_HEADLINE = 5920
 
 
@@ -207,19 +208,31 @@ def job_throughput(steps, world, max_ms):
 
 # ---------------------------------------------------------------- reference arm
 def cpu_iteration_time(fat, lng, L, src, mass, iters, threads):
-    """Seconds per CG iteration of the oracle (the reference algorithm restated
-    in C, FP64, OpenMP) on the host cores: a bounded run of `iters`."""
+    """Seconds per FP64 CG iteration of the reference algorithm on the host
+    cores, from a bounded EVEN solve of `iters` iterations (max_restarts 0,
+    an unreachable rsqmin): the reference's own compiled path
+    (oracle/_ref/libqopref.so: QOP_D3_asqtad_invert_qdp over its QDP/C
+    stand-in, OpenMP site loops) where it was built, else the oracle's C
+    restatement.  Returns (s/iter, iterations, threads, kind, what)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
-    O.set_threads(threads)
-    lat = O.Lattice(L)
-    fo = O.Fla(lat, fat, lng)
+    import refqop as R
     ia = O.InvertArg(1e9, iters, iters, 0, 0)
     ra = O.ResidArg(1e-30, 0, 0, 0, 0, 0)
+    if R.available():
+        th = R.set_threads(L, threads)
+        fo = R.RefFla(L, fat, lng, R.D3)
+        kind, what = "reference", "QOP_D3_asqtad_invert (the reference's own lib/asqtad_invert_p.c, compiled by oracle/ref)"
+    else:
+        O.set_threads(threads)
+        th = O.get_threads()
+        fo = O.Fla(O.Lattice(L), fat, lng)
+        kind, what = "port", "the oracle (the reference algorithm restated in C, OpenMP)"
     t0 = time.perf_counter()
     fo.invert(mass, src, ia, ra)
     dt = time.perf_counter() - t0
-    return dt / max(ra.final_iter, 1), ra.final_iter, O.get_threads()
+    del fo
+    return dt / max(ra.final_iter, 1), ra.final_iter, th, kind, what
 
 
 def oracle_true_rsq(fat, lng, L, src, out, mass, threads):
@@ -239,34 +252,50 @@ def oracle_true_rsq(fat, lng, L, src, out, mass, threads):
 
 
 def run_reference(a):
+    """The reference's own CPU implementation of the path, on the host cores:
+    HISQ links built by its QOP_hisq_create_L_from_G, then bounded FP64 CG
+    iterations of its QOP_D3_asqtad_invert (its default path: mixed_rsq
+    1e9 keeps every iteration in FP64) per step, extrapolated to the FP64
+    iteration count of the workload.  Without oracle/_ref (the reference
+    sources were absent when the tree was built) the oracle's restatement
+    stands in and the line says kind "port"."""
     rank, _, world = rank_info()
     if rank != 0:
         return
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
+    import refqop as R
     from qopqdp_b200 import lattice as LT
     L = tuple(int(x) for x in (a.lattice or "32,32,32,64").split(","))
     threads = os.cpu_count() or 1
-    O.set_threads(threads)
     U = LT.random_gauge(L, a.eps, a.seed, device="cpu")
-    lat = O.Lattice(L)
-    U = lat.rephase_G(U, LT.BENCH_R0, LT.BENCH_BC, LT.BENCH_SIGNMASK)
-    fat, lng, _, _ = lat.hisq_links(LT.hisq_coeff_vector(LT.hisq_bench_coeffs()), U)
+    hc = LT.hisq_coeff_vector(LT.hisq_bench_coeffs())
+    if R.available():
+        R.set_threads(L, threads)
+        U = R.rephase_G(L, U, LT.BENCH_R0, LT.BENCH_BC, LT.BENCH_SIGNMASK)
+        sets, _, _ = R.hisq_links(L, hc, U)
+        fat, lng = sets[0]
+        del sets
+    else:
+        O.set_threads(threads)
+        lat = O.Lattice(L)
+        U = lat.rephase_G(U, LT.BENCH_R0, LT.BENCH_BC, LT.BENCH_SIGNMASK)
+        fat, lng, _, _ = lat.hisq_links(hc, U)
     del U
     src = LT.gaussian_vector(L, a.seed)
     n_solve = a.ref_iters or (FP64_ITERS_HEADLINE if workload_name(a, L) == workload_name(a, (32, 32, 32, 64))
                               and (a.mass, a.tol, a.eps, a.seed) == (0.01, 1e-10, 0.5, 2024) else None)
     per = []
     for k in range(a.warmup + a.steps):
-        s, it, th = cpu_iteration_time(fat, lng, L, src, a.mass, a.cpu_iters, threads)
+        s, it, th, kind, what = cpu_iteration_time(fat, lng, L, src, a.mass, a.cpu_iters, threads)
         if k >= a.warmup:
             per.append(s)
     s_it = float(np.median(per))
     if n_solve:
         value = 1.0 / (s_it * n_solve)
-        sample = ("%d CG iterations of the FP64 reference algorithm (oracle, C/OpenMP) per step on %d host "
-                  "threads, %.4f s per iteration (median of %d steps); solves/s extrapolated to %d iterations, the "
-                  "FP64 CG iteration count of this workload" % (it, th, s_it, a.steps, n_solve))
+        sample = ("%d FP64 CG iterations of %s per step on %d host threads, %.4f s per iteration (median of %d "
+                  "steps); solves/s extrapolated to %d iterations, the FP64 CG iteration count of this workload"
+                  % (it, what, th, s_it, a.steps, n_solve))
     else:
         value = None
         sample = "%d CG iterations per step; no FP64 iteration count for this workload (--ref-iters)" % a.cpu_iters
@@ -278,7 +307,7 @@ def run_reference(a):
             "config": headline_config(a, L, world),
             "impl": "reference",
             "measured": {"sec_per_iter": s_it, "iters_per_step": it, "fp64_iters_per_solve": n_solve},
-            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": th, "kind": "port", "sample": sample,
+            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": th, "kind": kind, "sample": sample,
                              "sec_per_iter": s_it},
             "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -449,12 +478,12 @@ def run_b200(a):
         # recomputed by the oracle from the device's links
         oracle_rsq = oracle_true_rsq(fat, lng, L, src, sol, a.mass, threads)
         if world == 1:
-            s_it, nit, th = cpu_iteration_time(fat, lng, L, src, a.mass, a.cpu_iters, threads)
+            s_it, nit, th, kind, what = cpu_iteration_time(fat, lng, L, src, a.mass, a.cpu_iters, threads)
             n_ref = n_fp64 or FP64_ITERS_HEADLINE
-            cpu = {"value": 1.0 / (s_it * n_ref), "unit": "solves/s", "cores": th, "kind": "port",
-                   "sample": "%d CG iterations of the oracle (FP64 reference algorithm, C/OpenMP) on %d host "
-                             "threads, %.4f s/iteration, extrapolated to the %d iterations of the FP64 solve" %
-                             (nit, th, s_it, n_ref), "sec_per_iter": s_it}
+            cpu = {"value": 1.0 / (s_it * n_ref), "unit": "solves/s", "cores": th, "kind": kind,
+                   "sample": "%d FP64 CG iterations of %s on %d host threads, %.4f s/iteration, extrapolated "
+                             "to the %d iterations of the FP64 solve" % (nit, what, th, s_it, n_ref),
+                   "sec_per_iter": s_it}
         del fat, lng
     if rank == 0:
         lat_sorted = np.sort(lat_ms)

@@ -1,8 +1,9 @@
 /* qdp_shim_p.c -- the field operations of the single-process QDP interface
    in qdp.h for one precision (compiled with QDP_Precision 'F' and 'D'):
    test infrastructure for building the reference's asqtad path.  Every
-   operation loops over the sites of its subset (contiguous in raw order);
-   site arithmetic is in the field's precision, reductions in double. */
+   operation loops over the sites of its subset (contiguous in raw order),
+   threaded with OpenMP as QDP's own site loops are; site arithmetic is in
+   the field's precision, reductions in double. */
 #define QLA_Precision QDP_Precision
 #include <string.h>
 #include "qdp.h"
@@ -16,7 +17,10 @@ typedef QLA_Complex C;
 typedef QLA_ColorVector QV;
 typedef QLA_ColorMatrix QM;
 
-#define SITES(sub) for (int i = (sub)->start; i < (sub)->start + (sub)->len; i++)
+#define SHIM_PRAGMA(x) _Pragma(#x)
+#define SITES_SERIAL(sub) for (int i = (sub)->start; i < (sub)->start + (sub)->len; i++)
+#define SITES(sub) SHIM_PRAGMA(omp parallel for schedule(static)) SITES_SERIAL(sub)
+#define SITES_SUM(sub, ...) SHIM_PRAGMA(omp parallel for schedule(static) reduction(+ : __VA_ARGS__)) SITES_SERIAL(sub)
 
 static void *shim_alloc(size_t n) {
   void *p = calloc(1, n);
@@ -280,7 +284,7 @@ void QDP_V_eq_funcit(QDP_ColorVector *r, void (*f)(QV *, int), QDP_Subset s) { S
 /* reductions (double accumulation) */
 void QDP_r_eq_norm2_V(QLA_Real *r, QDP_ColorVector *a, QDP_Subset s) {
   double acc = 0;
-  SITES(s) for (int c = 0; c < 3; c++) {
+  SITES_SUM(s, acc) for (int c = 0; c < 3; c++) {
       const C z = a->d[i].c[c];
       acc += (double)z.real * z.real + (double)z.imag * z.imag;
     }
@@ -291,7 +295,7 @@ void QDP_r_veq_norm2_V(QLA_Real *r, QDP_ColorVector **a, QDP_Subset s, int n) {
 }
 void QDP_c_eq_V_dot_V(QLA_Complex *r, QDP_ColorVector *a, QDP_ColorVector *b, QDP_Subset s) {
   double re = 0, im = 0;
-  SITES(s) for (int c = 0; c < 3; c++) {
+  SITES_SUM(s, re, im) for (int c = 0; c < 3; c++) {
       const C x = a->d[i].c[c], y = b->d[i].c[c];
       re += (double)x.real * y.real + (double)x.imag * y.imag;
       im += (double)x.real * y.imag - (double)x.imag * y.real;
@@ -370,7 +374,7 @@ void QDP_M_eq_funct(QDP_ColorMatrix *r, void (*f)(QM *, int[]), QDP_Subset s) {
 }
 void QDP_r_eq_norm2_M(QLA_Real *r, QDP_ColorMatrix *a, QDP_Subset s) {
   double acc = 0;
-  SITES(s) for (int x = 0; x < 3; x++) for (int y = 0; y < 3; y++) {
+  SITES_SUM(s, acc) for (int x = 0; x < 3; x++) for (int y = 0; y < 3; y++) {
         const C z = a->d[i].e[x][y];
         acc += (double)z.real * z.real + (double)z.imag * z.imag;
       }
@@ -378,7 +382,7 @@ void QDP_r_eq_norm2_M(QLA_Real *r, QDP_ColorMatrix *a, QDP_Subset s) {
 }
 void QDP_m_eq_sum_M(QM *r, QDP_ColorMatrix *a, QDP_Subset s) {
   double re[3][3] = {{0}}, im[3][3] = {{0}};
-  SITES(s) for (int x = 0; x < 3; x++) for (int y = 0; y < 3; y++) {
+  SITES_SERIAL(s) for (int x = 0; x < 3; x++) for (int y = 0; y < 3; y++) {
         re[x][y] += a->d[i].e[x][y].real;
         im[x][y] += a->d[i].e[x][y].imag;
       }

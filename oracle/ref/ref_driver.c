@@ -257,3 +257,18 @@ int qr_asqtad_links_from_G(const double coeffs[6], double *gauge[4], double *fat
   QOP_D3_destroy_G(gf);
   return info.status;
 }
+
+/* host threads for the OpenMP site loops (QDP's threading); returns the
+   number in effect */
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+int qr_set_threads(int n) {
+#ifdef _OPENMP
+  if (n > 0) omp_set_num_threads(n);
+  return omp_get_max_threads();
+#else
+  (void)n;
+  return 1;
+#endif
+}

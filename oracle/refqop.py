@@ -72,6 +72,7 @@ def _load(L):
     l.qr_invert_multi.argtypes = [C.c_int, vp, C.POINTER(InvertArg), C.POINTER(C.POINTER(C.POINTER(ResidArg))),
                                   C.POINTER(DP), C.POINTER(C.c_int), C.POINTER(C.POINTER(DP)), C.POINTER(DP),
                                   C.c_int, C.POINTER(C.c_double)]
+    l.qr_set_threads.argtypes = [C.c_int]
     l.qr_rephase_G.argtypes = [C.POINTER(DP), C.POINTER(C.c_int), DP, C.POINTER(C.c_int)]
     l.qr_asqtad_links_from_G.argtypes = [DP, C.POINTER(DP), C.POINTER(DP), C.POINTER(DP)]
     l.qr_hisq_links.argtypes = [DP, C.c_int, DP, C.POINTER(DP), C.POINTER(DP), C.POINTER(DP), C.POINTER(DP),
@@ -188,3 +189,9 @@ def hisq_links(L, hcoef, gauge, eps_naik=(0.0,), want_deps=False):
         raise RuntimeError("QOP_hisq_create_L_from_G status %d" % st)
     sets = [(fat[4 * k:4 * k + 4], lng[4 * k:4 * k + 4]) for k in range(nk)]
     return sets, W, ((dfat, dlng) if want_deps else None)
+
+
+def set_threads(L, n):
+    """OpenMP threads of the site loops in the copy serving L (n <= 0 keeps
+    the current number); returns the number in effect."""
+    return _load(tuple(L)).qr_set_threads(int(n))

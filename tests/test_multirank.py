@@ -59,4 +59,8 @@ def test_reference_arm_rank0_line():
     assert r.returncode == 0, r.stderr
     line = json.loads(r.stdout.strip().splitlines()[-1])
     assert line["impl"] == "reference" and line["e2e"]["h2d_bytes_per_step"] == 0
-    assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import refqop
+    # the reference's own compiled path where oracle/_ref was built, else the port
+    assert line["cpu_baseline"]["kind"] == ("reference" if refqop.available() else "port")
+    assert line["cpu_baseline"]["cores"] >= 1 and line["value"] is None
