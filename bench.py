@@ -251,6 +251,22 @@ def oracle_true_rsq(fat, lng, L, src, out, mass, threads):
     return float((r ** 2).sum() / (b ** 2).sum())
 
 
+class _StdoutToStderr:
+    """Sends what C code prints to stdout (the reference's own progress and
+    SVD messages) to stderr, so that stdout carries only the JSON line."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        os.dup2(2, 1)
+        return self
+
+    def __exit__(self, *exc):
+        sys.stdout.flush()
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+
+
 def run_reference(a):
     """The reference's own CPU implementation of the path, on the host cores:
     HISQ links built by its QOP_hisq_create_L_from_G, then bounded FP64 CG
@@ -270,6 +286,8 @@ def run_reference(a):
     threads = os.cpu_count() or 1
     U = LT.random_gauge(L, a.eps, a.seed, device="cpu")
     hc = LT.hisq_coeff_vector(LT.hisq_bench_coeffs())
+    quiet = _StdoutToStderr()
+    quiet.__enter__()
     if R.available():
         R.set_threads(L, threads)
         U = R.rephase_G(L, U, LT.BENCH_R0, LT.BENCH_BC, LT.BENCH_SIGNMASK)
@@ -290,6 +308,7 @@ def run_reference(a):
         s, it, th, kind, what = cpu_iteration_time(fat, lng, L, src, a.mass, a.cpu_iters, threads)
         if k >= a.warmup:
             per.append(s)
+    quiet.__exit__()
     s_it = float(np.median(per))
     if n_solve:
         value = 1.0 / (s_it * n_solve)
@@ -478,7 +497,8 @@ def run_b200(a):
         # recomputed by the oracle from the device's links
         oracle_rsq = oracle_true_rsq(fat, lng, L, src, sol, a.mass, threads)
         if world == 1:
-            s_it, nit, th, kind, what = cpu_iteration_time(fat, lng, L, src, a.mass, a.cpu_iters, threads)
+            with _StdoutToStderr():
+                s_it, nit, th, kind, what = cpu_iteration_time(fat, lng, L, src, a.mass, a.cpu_iters, threads)
             n_ref = n_fp64 or FP64_ITERS_HEADLINE
             cpu = {"value": 1.0 / (s_it * n_ref), "unit": "solves/s", "cores": th, "kind": kind,
                    "sample": "%d FP64 CG iterations of %s on %d host threads, %.4f s/iteration, extrapolated "

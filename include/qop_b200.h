@@ -100,6 +100,19 @@ int QOPB_layout_hyper(const int latsize[4], int nranks, int nsquares[4]);
 int QOPB_layout_node_number(const int latsize[4], const int nsquares[4], const int coords[4]);
 long QOPB_layout_node_index(const int latsize[4], const int nsquares[4], const int coords[4]);
 int QOPB_layout_neighbors(const int nsquares[4], int rank, int nbr[8]);
+/* The halo plan of the decomposed hop, for host-side checks (no GPU, no
+   QOP_init).  local: the block's extents (even, >= 4).  QOPB_dd_pack_site
+   gives the local site x packed into element (slab, face) of direction mu's
+   halo for a parity-`parity` input (nlinks 8 or 16): the return value is -1
+   for a raw slab (the input vector at x, sent to the -mu neighbour's up
+   halo) or the link slot of a product slab (-U^+ psi at x with that slot's
+   forward link, sent to the +mu neighbour's down halo), -2 for invalid
+   arguments.  QOPB_dd_halo_ref says where the hop term (mu, disp) of local
+   site x reads its neighbour: 0 inside the block, 1 the up halo, 2 the down
+   halo (then *slab, *face locate the element), -1 for invalid arguments.
+   Slabs hold 3 colours x fh face sites, fh = local volume / local[mu] / 2. */
+int QOPB_dd_pack_site(const int local[4], int mu, int nlinks, int parity, int slab, int face, int x[4]);
+int QOPB_dd_halo_ref(const int local[4], const int x[4], int mu, int disp, int *slab, int *face);
 
 /* Several lattices in one process (no counterpart in the reference, whose
    QOP_init fixes one geometry per process).  QOP_init defines lattice 0;

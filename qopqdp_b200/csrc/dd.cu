@@ -303,20 +303,8 @@ __global__ void k_dd_pack(const c2<T> *__restrict__ in, const c2<T> *__restrict_
   if (!dd_plan_entry(pl, blockIdx.x * (i64)blockDim.x + threadIdx.x, j, s, fi)) return;
   const int mu = pl.mu[j], fh = pl.fh[j];
   c2<T> *sraw = (c2<T> *)pl.sraw[j], *sprod = (c2<T> *)pl.sprod[j];
-  int xm, slot = -1;
-  if (s < depth) {
-    xm = s;
-  } else {
-    const int j = s - depth;
-    xm = g.L[mu] - 1 - (j == 0 ? 0 : j - 1);
-    slot = nl == 16 ? (j == 0 ? 4 * mu : 4 * mu + 1) : 2 * mu;
-  }
   int x[4];
-  int rem = 2 * fi;
-  for (int nu = 3; nu >= 0; nu--)
-    if (nu != mu) { x[nu] = rem % g.L[nu]; rem /= g.L[nu]; }
-  x[mu] = xm;
-  if (((x[0] + x[1] + x[2] + x[3]) & 1) != q) x[mu == 3 ? 2 : 3] += 1;   // the pair's other site
+  const int slot = dd_pack_site(g.L, mu, nl, q, s, fi, x);
   const i64 Vh = g.Vh;
   const int i = site_index(g, x[0], x[1], x[2], x[3]);
   const c2<T> v0 = in[i], v1 = in[Vh + i], v2 = in[2 * Vh + i];
@@ -393,20 +381,8 @@ __global__ void k_dd_pack_q16(const uint4 *__restrict__ in, const double2 *__res
   if (!dd_plan_entry(pl, blockIdx.x * (i64)blockDim.x + threadIdx.x, j, s, fi)) return;
   const int mu = pl.mu[j], fh = pl.fh[j];
   uint4 *sraw = (uint4 *)pl.sraw[j], *sprod = (uint4 *)pl.sprod[j];
-  int xm, slot = -1;
-  if (s < depth) {
-    xm = s;
-  } else {
-    const int j = s - depth;
-    xm = g.L[mu] - 1 - (j == 0 ? 0 : j - 1);
-    slot = nl == 16 ? (j == 0 ? 4 * mu : 4 * mu + 1) : 2 * mu;
-  }
   int x[4];
-  int rem = 2 * fi;
-  for (int nu = 3; nu >= 0; nu--)
-    if (nu != mu) { x[nu] = rem % g.L[nu]; rem /= g.L[nu]; }
-  x[mu] = xm;
-  if (((x[0] + x[1] + x[2] + x[3]) & 1) != q) x[mu == 3 ? 2 : 3] += 1;
+  const int slot = dd_pack_site(g.L, mu, nl, q, s, fi, x);
   const i64 Vh = g.Vh;
   const int i = site_index(g, x[0], x[1], x[2], x[3]);
   if (slot < 0) {
@@ -541,6 +517,33 @@ int QOPB_dd_info(int nsquares[4], int coords[4], int local[4], int *mask) {
   }
   if (mask) *mask = c.dd ? c.dd->mask : 0;
   return c.dd ? c.dd->rank : 0;
+}
+
+static bool dd_block_ok(const int local[4]) {
+  if (!local) return false;
+  for (int i = 0; i < 4; i++)
+    if (local[i] < 4 || (local[i] & 1)) return false;
+  return true;
+}
+
+int QOPB_dd_pack_site(const int local[4], int mu, int nlinks, int parity, int slab, int face, int x[4]) {
+  if (!dd_block_ok(local) || !x || mu < 0 || mu > 3 || (nlinks != 8 && nlinks != 16) || (parity & ~1)) return -2;
+  const long fh = (long)local[0] * local[1] * local[2] * local[3] / local[mu] / 2;
+  if (slab < 0 || slab >= dd_depth(nlinks) + dd_nprod(nlinks) || face < 0 || face >= fh) return -2;
+  return dd_pack_site(local, mu, nlinks, parity, slab, face, x);
+}
+
+int QOPB_dd_halo_ref(const int local[4], const int x[4], int mu, int disp, int *slab, int *face) {
+  if (!dd_block_ok(local) || !x || !slab || !face || mu < 0 || mu > 3 ||
+      (disp != 1 && disp != -1 && disp != 3 && disp != -3))
+    return -1;
+  for (int i = 0; i < 4; i++)
+    if (x[i] < 0 || x[i] >= local[i]) return -1;
+  const int y = x[mu] + disp;
+  if ((unsigned)y < (unsigned)local[mu]) return 0;
+  *slab = dd_halo_slab(local[mu], y, disp);
+  *face = dd_face_index_L(local, x, mu);
+  return y < 0 ? 2 : 1;
 }
 
 }  // extern "C"

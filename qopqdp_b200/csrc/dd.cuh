@@ -33,12 +33,52 @@ template <typename T> struct DdGhost {
 __host__ __device__ inline int dd_depth(int nl) { return nl == 16 ? 3 : 1; }
 __host__ __device__ inline int dd_nprod(int nl) { return nl == 16 ? 4 : 1; }
 
-__device__ __forceinline__ int dd_face_index(const Geom &g, const int x[4], int mu) {
+// The halo plan.  These index functions are the only place the layout of
+// the halos is defined: the pack kernels (producer), the hop kernels
+// (consumer) and the host-side test hooks QOPB_dd_pack_site /
+// QOPB_dd_halo_ref all call them.
+
+// face index of local site x in a slab of direction mu
+__host__ __device__ inline int dd_face_index_L(const int L[4], const int x[4], int mu) {
   int l = 0;
 #pragma unroll
   for (int nu = 0; nu < 4; nu++)
-    if (nu != mu) l = l * g.L[nu] + x[nu];
+    if (nu != mu) l = l * L[nu] + x[nu];
   return l >> 1;
+}
+__device__ __forceinline__ int dd_face_index(const Geom &g, const int x[4], int mu) {
+  return dd_face_index_L(g.L, x, mu);
+}
+
+// consumer: a hop term (mu, d) from local site x leaves the block when
+// y = x_mu + d is outside [0, L_mu); it reads up-halo slab y - L_mu, or
+// down-halo slab 0 (the fat product, d = -1) or -y (the long products)
+__host__ __device__ inline int dd_halo_slab(int Lmu, int y, int d) {
+  return y < 0 ? (d == -1 ? 0 : -y) : y - Lmu;
+}
+
+// producer: the local site packed at (slab s, face index fi) of direction
+// mu for the parity-q input; returns the link slot multiplied into a
+// product slab (s >= depth), or -1 for a raw slab (s < depth: x_mu = s, for
+// the -mu neighbour's up halo).  Product slab depth + j holds -U^+ psi at
+// x_mu = L_mu - 1 - max(j - 1, 0) with the fat link (j = 0) or the long
+// link (j >= 1), for the +mu neighbour's down halo.
+__host__ __device__ inline int dd_pack_site(const int L[4], int mu, int nl, int q, int s, int fi, int x[4]) {
+  const int depth = dd_depth(nl);
+  int xm, slot = -1;
+  if (s < depth) {
+    xm = s;
+  } else {
+    const int j = s - depth;
+    xm = L[mu] - 1 - (j == 0 ? 0 : j - 1);
+    slot = nl == 16 ? (j == 0 ? 4 * mu : 4 * mu + 1) : 2 * mu;
+  }
+  int rem = 2 * fi;
+  for (int nu = 3; nu >= 0; nu--)
+    if (nu != mu) { x[nu] = rem % L[nu]; rem /= L[nu]; }
+  x[mu] = xm;
+  if (((x[0] + x[1] + x[2] + x[3]) & 1) != q) x[mu == 3 ? 2 : 3] += 1;   // the pair's other site
+  return slot;
 }
 
 // packs the input halo of parity q (in: the parity-q block [colour][Vh]) and

@@ -25,12 +25,13 @@ __device__ __forceinline__ bool hop_input(const Geom &g, const int x[4], int mu,
   const i64 Vh = g.Vh;
   if (DD && (gh.mask >> mu & 1) && (unsigned)(x[mu] + d) >= (unsigned)g.L[mu]) {
     const int y = x[mu] + d, fh = gh.fh[mu], fi = dd_face_index(g, x, mu);
+    const int sl = dd_halo_slab(g.L[mu], y, d);
     if (y < 0) {   // slab 0: the fat product at y = -1; slab -y: the long product
-      const c2<T> *G = gh.dn[mu] + (i64)((d == -1 ? 0 : -y) * 3) * fh + fi;
+      const c2<T> *G = gh.dn[mu] + (i64)(sl * 3) * fh + fi;
       a[0] = cadd<T>(a[0], G[0]); a[1] = cadd<T>(a[1], G[fh]); a[2] = cadd<T>(a[2], G[2 * fh]);
       return false;
     }
-    const c2<T> *G = gh.up[mu] + (i64)((y - g.L[mu]) * 3) * fh + fi;
+    const c2<T> *G = gh.up[mu] + (i64)(sl * 3) * fh + fi;
     v0 = G[0]; v1 = G[fh]; v2 = G[2 * fh];
     return true;
   }

@@ -847,8 +847,8 @@ k_mix_hop_q16r(uint4 *__restrict__ out, const uint4 *__restrict__ src, const uns
           // one load per slot (each warp of a split x3 row has boundary lanes)
           const int y = x[mu] + dsp, fh = gh.fh[mu], fi = hfi[mu];
           const bool cross = (unsigned)y >= (unsigned)g.L[mu];
-          const uint4 *hp = y < 0 ? gh.dn[mu] + (i64)(dsp == -1 ? 0 : -y) * fh + fi
-                                  : gh.up[mu] + (i64)max(y - g.L[mu], 0) * fh + fi;   // in range when unused
+          const int sl = max(dd_halo_slab(g.L[mu], y, dsp), 0);   // in range when unused
+          const uint4 *hp = (y < 0 ? gh.dn[mu] : gh.up[mu]) + (i64)sl * fh + fi;
           np = cross ? hp : np;
           prd[s] = cross && y < 0;
         }

@@ -131,6 +131,9 @@ def load_library(path=None):
     lib.QOPB_layout_node_index.argtypes = [C.POINTER(C.c_int)] * 3
     lib.QOPB_layout_node_index.restype = C.c_long
     lib.QOPB_layout_neighbors.argtypes = [C.POINTER(C.c_int), ip, C.POINTER(C.c_int)]
+    lib.QOPB_dd_pack_site.argtypes = [C.POINTER(C.c_int), ip, ip, ip, ip, ip, C.POINTER(C.c_int)]
+    lib.QOPB_dd_halo_ref.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_int), ip, ip, C.POINTER(C.c_int),
+                                     C.POINTER(C.c_int)]
     lib.QOPB_lattice_create.argtypes = [C.POINTER(C.c_int)]
     lib.QOPB_lattice_create.restype = ip
     lib.QOPB_lattice_use.argtypes = [ip]
@@ -571,3 +574,23 @@ def layout_neighbors(P, rank):
     nb = (C.c_int * 8)()
     load_library().QOPB_layout_neighbors((C.c_int * 4)(*P), rank, nb)
     return [(nb[2 * i], nb[2 * i + 1]) for i in range(4)]
+
+
+def dd_pack_site(local, mu, nlinks, parity, slab, face):
+    """(local site x, link slot or -1) packed at (slab, face) of direction
+    mu's halo, from the library's halo plan."""
+    x = (C.c_int * 4)()
+    slot = load_library().QOPB_dd_pack_site((C.c_int * 4)(*local), mu, nlinks, parity, slab, face, x)
+    if slot < -1:
+        raise ValueError("bad halo plan arguments")
+    return tuple(x), slot
+
+
+def dd_halo_ref(local, x, mu, disp):
+    """Where the hop term (mu, disp) of local site x reads its neighbour:
+    None inside the block, else ('up' | 'dn', slab, face)."""
+    sl, fc = C.c_int(), C.c_int()
+    r = load_library().QOPB_dd_halo_ref((C.c_int * 4)(*local), (C.c_int * 4)(*x), mu, disp, C.byref(sl), C.byref(fc))
+    if r < 0:
+        raise ValueError("bad halo plan arguments")
+    return None if r == 0 else ("up" if r == 1 else "dn", sl.value, fc.value)

@@ -172,3 +172,150 @@ def test_two_process_halo_exchange_layout():
     for rank, P, errors in res:
         assert P == (1, 1, 2, 1)
         assert errors == 0, (rank, errors)
+
+
+# ---------------------------------------------------------------- the library's halo plan
+def _plan_hop_worker(rank, world, port, GLb, P, q_out):
+    """One rank of the decomposed hop, assembled on the CPU from the
+    library's own plan: node numbers and node-local raw indices
+    (QOPB_layout_node_number / _node_index), neighbour ranks
+    (QOPB_layout_neighbors), the packed halo sites and link slots
+    (QOPB_dd_pack_site) and where each boundary term reads its halo
+    (QOPB_dd_halo_ref).  The result on the rank's sites is compared with the
+    oracle's Dslash of the global field."""
+    import torch
+    import torch.distributed as dist
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from qopqdp_b200 import lattice as LT
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        GL = tuple(GLb)
+        b = tuple(GL[i] // P[i] for i in range(4))
+        Vg, Vl = int(np.prod(GL)), int(np.prod(b))
+        rng = np.random.default_rng(23)
+        psi = rng.standard_normal((Vg, 3, 2))
+        fat = [rng.standard_normal((Vg, 3, 3, 2)) for _ in range(4)]
+        lng = [rng.standard_normal((Vg, 3, 3, 2)) for _ in range(4)]
+        cz = lambda a: a[..., 0] + 1j * a[..., 1]
+        psic, fatc, lngc = cz(psi), [cz(a) for a in fat], [cz(a) for a in lng]
+        xs = LT.raw_coords(GL)
+        # this rank's sites, in its node-local raw order
+        loc = {}
+        for g in range(Vg):
+            x = tuple(int(v) for v in xs[g])
+            if qop.layout_node_number(GL, P, x) == rank:
+                loc[qop.layout_node_index(GL, P, x)] = g
+        assert sorted(loc) == list(range(Vl))
+        lg = np.array([loc[i] for i in range(Vl)])           # local raw index -> global raw index
+        origin = xs[lg].min(axis=0)
+        assert all(o % 2 == 0 for o in origin)
+        lraw = {tuple(int(v) for v in xs[g] - origin): i for i, g in enumerate(lg)}
+        nb = qop.layout_neighbors(P, rank)
+        ref_fla = O.Fla(O.Lattice(GL), fat, lng)
+        errs = []
+        for p in (0, 1):
+            q = 1 - p
+            up, dn = {}, {}
+            for mu in range(4):
+                if P[mu] == 1:
+                    continue
+                fh = Vl // b[mu] // 2
+                sraw = np.zeros((3, 3, fh), complex)
+                sprod = np.zeros((4, 3, fh), complex)
+                for s in range(7):
+                    for fi in range(fh):
+                        x, slot = qop.dd_pack_site(b, mu, 16, q, s, fi)
+                        assert sum(x) % 2 == q
+                        g = lg[lraw[x]]
+                        if slot < 0:
+                            sraw[s, :, fi] = psic[g]
+                        else:
+                            U = (fatc if slot == 4 * mu else lngc)[mu][g] * 0.5
+                            sprod[s - 3, :, fi] = -U.conj().T @ psic[g]
+                gup, gdn = np.zeros_like(sraw), np.zeros_like(sprod)
+                reqs = []
+                for buf, peer, send, tag in ((sraw, nb[mu][0], True, 1), (gup, nb[mu][1], False, 1),
+                                             (sprod, nb[mu][1], True, 2), (gdn, nb[mu][0], False, 2)):
+                    t = torch.from_numpy(buf.view(np.float64))
+                    reqs.append((dist.isend if send else dist.irecv)(t, peer, tag=tag))
+                for rq in reqs:
+                    rq.wait()
+                up[mu], dn[mu] = gup, gdn
+            want = cz(ref_fla.dslash(0.0, psi, p, q))
+            worst = 0.0
+            for i in range(Vl):
+                x = tuple(int(v) for v in xs[lg[i]] - origin)
+                if sum(x) % 2 != p:
+                    continue
+                acc = np.zeros(3, complex)
+                for mu in range(4):
+                    for d in (1, 3, -1, -3):
+                        # directions that are not split wrap inside the block
+                        where = qop.dd_halo_ref(b, x, mu, d) if P[mu] > 1 else None
+                        U_here = (fatc if abs(d) == 1 else lngc)[mu][lg[i]] * 0.5
+                        if where is None:
+                            y = list(x)
+                            y[mu] = (y[mu] + d) % b[mu]
+                            gy = lg[lraw[tuple(y)]]
+                            if d > 0:
+                                acc += U_here @ psic[gy]
+                            else:
+                                U = (fatc if d == -1 else lngc)[mu][gy] * 0.5
+                                acc -= U.conj().T @ psic[gy]
+                        elif where[0] == "up":
+                            acc += U_here @ up[mu][where[1], :, where[2]]
+                        else:
+                            acc += dn[mu][where[1], :, where[2]]
+                w = want[lg[i]]
+                worst = max(worst, float(np.abs(acc - w).max() / np.abs(w).max()))
+            errs.append(worst)
+        dist.barrier()
+        q_out.put((rank, errs))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("GL,P", [((4, 4, 4, 8), (1, 1, 1, 2)), ((8, 4, 4, 4), (2, 1, 1, 1)),
+                                  ((4, 8, 6, 4), (1, 2, 1, 1))])
+def test_two_process_hop_through_library_halo_plan(GL, P):
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = 29700 + (os.getpid() + 7 * P.index(2)) % 1000
+    ps = [ctx.Process(target=_plan_hop_worker, args=(r, 2, port, GL, P, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    res = []
+    import queue
+    import time
+    t0 = time.time()
+    while len(res) < len(ps):
+        try:
+            res.append(q.get(timeout=2))
+        except queue.Empty:
+            # a rank that died (an exception) ends the test instead of a wait
+            assert all(p.exitcode in (None, 0) for p in ps), [p.exitcode for p in ps]
+            assert time.time() - t0 < 300
+    res.sort()
+    for p in ps:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for rank, errs in res:
+        assert max(errs) < 1e-14, (rank, errs)
+
+
+def test_halo_plan_hooks_reject_bad_arguments():
+    with pytest.raises(ValueError):
+        qop.dd_pack_site((4, 4, 4, 5), 0, 16, 0, 0, 0)       # odd extent
+    with pytest.raises(ValueError):
+        qop.dd_pack_site((4, 4, 4, 4), 0, 16, 0, 7, 0)       # slab past depth + products
+    with pytest.raises(ValueError):
+        qop.dd_pack_site((4, 4, 4, 4), 0, 16, 0, 0, 32)      # face past fh
+    with pytest.raises(ValueError):
+        qop.dd_halo_ref((4, 4, 4, 4), (0, 0, 0, 4), 3, 1)    # site outside the block
+    with pytest.raises(ValueError):
+        qop.dd_halo_ref((4, 4, 4, 4), (0, 0, 0, 0), 3, 2)    # not a hop displacement
+    assert qop.dd_halo_ref((4, 4, 4, 4), (1, 1, 1, 1), 3, 1) is None
+    assert qop.dd_halo_ref((4, 4, 4, 4), (1, 1, 1, 3), 3, 3)[0:2] == ("up", 2)
+    assert qop.dd_halo_ref((4, 4, 4, 4), (1, 1, 1, 0), 3, -3)[0:2] == ("dn", 3)

@@ -103,7 +103,7 @@ def test_golden_hisq_links_and_dslash(gold):
 
 # ---------------------------------------------------------------- live library
 
-LIVE_L = [(4, 4, 4, 4), (4, 4, 4, 6), (6, 4, 4, 8)]
+LIVE_L = [(4, 4, 4, 4), (4, 4, 4, 6), (8, 8, 8, 8), (6, 4, 4, 8)]
 
 
 def _gauge(L, seed=5, eps=0.3):
@@ -185,7 +185,7 @@ def test_live_dslash_nine_cases(L, naik):
 
 
 @live
-@pytest.mark.parametrize("L", LIVE_L[:2])
+@pytest.mark.parametrize("L", LIVE_L[:3])
 @pytest.mark.parametrize("eo", [0, 1, 2])
 def test_live_invert_fp64(L, eo):
     fo, fat, lng = _ops(L)
