@@ -551,8 +551,10 @@ MULTI = {
 def run_multi(a):
     """One step = one QOP_D3_asqtad_invert_multi call on the EVEN parity:
     `multimass` solves one source at 12 masses, `multisrc` 16 sources at
-    one mass, every solve to |r|/|b| <= tol.  The int16 path runs all solves
-    of the call as one batched reliable-update CG sharing each hop's links.
+    one mass, every solve to |r|/|b| <= tol.  The int16 path runs the masses
+    of one source as an int16 multi-shift CG and then refines every solve in
+    one batched reliable-update CG sharing each hop's links (multisrc: the
+    batched CG alone).
     Compared with the same call in FP64 (the reference algorithm: CGMS +
     refine for multimass; for multisrc one FP64 single-source solve times 16,
     which bounds the reference's sequential restarts from below)."""
@@ -600,8 +602,8 @@ def run_multi(a):
     stream = torch.cuda.ExternalStream(lib.QOPB_stream())
     rsq = a.tol * a.tol
 
-    def step(prec, ms=masses, ins=hins):
-        q.set_opts(prec_sloppy=prec, half_format=0, ru_delta=a.ru_delta, **kernel_opts(a))
+    def step(prec, ms=masses, ins=hins, multi_shift=1):
+        q.set_opts(prec_sloppy=prec, half_format=0, ru_delta=a.ru_delta, multi_shift=multi_shift, **kernel_opts(a))
         outs = [[q.create_V(np.zeros_like(srcs[0])) for _ in m] for m in ms]
         ras = [[QOP_resid_arg_t(rsq, 0, 0, 0, 0, 0) for _ in m] for m in ms]
         ia = QOP_invert_arg_t(1e9, 200000, 200000, 50, QOP_EVEN)
@@ -662,6 +664,21 @@ def run_multi(a):
         fp64 = {"ms_per_step": ms64, "solves_per_s": nsolve / (ms64 / 1e3),
                 "max_final_rsq": max(r.final_rsq for r in r64),
                 "how": "one FP64 single-source solve x %d" % nsolve if mult > 1 else "the same call in FP64"}
+    # the other int16 multi-mass mode (option multi_shift = 0: every mass a
+    # system of the batched solver from the start; not timed into value)
+    mshift = None
+    if not a.quick and a.workload == "multimass" and a.prec == 16:
+        step(16, multi_shift=0)
+        torch.cuda.synchronize()
+        s0 = ev()
+        rms = step(16, multi_shift=0)
+        s1 = ev()
+        s1.synchronize()
+        msm = s0.elapsed_time(s1)
+        mshift = {"ms_per_step": msm, "solves_per_s": nsolve / (msm / 1e3),
+                  "max_final_rsq": max(r.final_rsq for r in rms), "iters_max": max(r.final_iter for r in rms),
+                  "how": "option multi_shift = 0: the batched solver alone, every mass from zero"}
+        q.set_opts(multi_shift=1)
     peak, peak_kind = measured_peak()
     dom = max(kst.items(), key=lambda kv: kv[1][1]) if kst else None
     roof = None
@@ -680,7 +697,7 @@ def run_multi(a):
                            "masses": w["masses"], "sources": w["nsrc"], "tol": a.tol,
                            "parallelism": "replicas x%d" % world},
                 "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-                "final_rsq_max": float(max(rsqs)), "fp64": fp64,
+                "final_rsq_max": float(max(rsqs)), "fp64": fp64, "batched_mode": mshift,
                 "speedup_vs_fp64": (value / world) / fp64["solves_per_s"] if fp64 else None,
                 "roofline": roof, "kernels": {k: {"launches": v[0], "avg_us": 1e3 * v[1] / max(v[0], 1)}
                                               for k, v in kst.items()},

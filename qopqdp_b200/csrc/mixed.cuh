@@ -332,21 +332,48 @@ __device__ __forceinline__ void q16_slot_pk(const uint4 ua, const uint4 ub, cons
   q16_pk_mul(U, vx, vy, t, s);
 }
 
+// conj(a b - c d) of complex pairs
+__device__ __forceinline__ float2 conj_cross(const float2 a, const float2 b, const float2 c, const float2 d) {
+  float re = a.x * b.x;
+  re = fmaf(-a.y, b.y, re);
+  re = fmaf(-c.x, d.x, re);
+  re = fmaf(c.y, d.y, re);
+  float im = -(a.x * b.y);
+  im = fmaf(-a.y, b.x, im);
+  im = fmaf(c.x, d.y, im);
+  im = fmaf(c.y, d.x, im);
+  return make_float2(re, im);
+}
+
+// The third row never forms: row 2 = det conj(row0 x row1), so its product
+// with the site is z sum_c conj(c_c) v_c (z = det / 32767), one complex dot
+// folded into the row-2 accumulator after the phase.
 __device__ __forceinline__ void q16_slot_recon_pk(const uint4 ua, const uint2 ub, const float phase, const uint4 nb,
                                                   const float cl, float2 t[3], float2 s[3]) {
   float2 vx[3], vy[3];
   q16_pk_site(nb, cl * (1.0f / 32767.0f), vx, vy);
-  float2 U[9] = {u16_pair(ua.x), u16_pair(ua.y), u16_pair(ua.z), u16_pair(ua.w), u16_pair(ub.x), u16_pair(ub.y)};
+  const float2 U[6] = {u16_pair(ua.x), u16_pair(ua.y), u16_pair(ua.z), u16_pair(ua.w), u16_pair(ub.x), u16_pair(ub.y)};
+#pragma unroll
+  for (int r = 0; r < 2; r++)
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      t[r] = __ffma2_rn(U[3 * r + c], vx[c], t[r]);
+      s[r] = __ffma2_rn(U[3 * r + c], vy[c], s[r]);
+    }
+  const float2 k0 = conj_cross(U[1], U[5], U[2], U[4]);
+  const float2 k1 = conj_cross(U[2], U[3], U[0], U[5]);
+  const float2 k2 = conj_cross(U[0], U[4], U[1], U[3]);
+  float2 tw = __fmul2_rn(k0, vx[0]), sw = __fmul2_rn(k0, vy[0]);
+  tw = __ffma2_rn(k1, vx[1], tw);
+  sw = __ffma2_rn(k1, vy[1], sw);
+  tw = __ffma2_rn(k2, vx[2], tw);
+  sw = __ffma2_rn(k2, vy[2], sw);
+  const float2 w = make_float2(tw.x - sw.y, tw.y + sw.x);
   float sn, cs;
   __sincosf(phase, &sn, &cs);
-  const float2 z = make_float2(cs * (1.0f / 32767.0f), sn * (1.0f / 32767.0f));
-  const float2 c0 = csub<float>(cmul<float>(U[1], U[5]), cmul<float>(U[2], U[4]));
-  const float2 c1 = csub<float>(cmul<float>(U[2], U[3]), cmul<float>(U[0], U[5]));
-  const float2 c2 = csub<float>(cmul<float>(U[0], U[4]), cmul<float>(U[1], U[3]));
-  U[6] = cmul<float>(z, make_float2(c0.x, -c0.y));
-  U[7] = cmul<float>(z, make_float2(c1.x, -c1.y));
-  U[8] = cmul<float>(z, make_float2(c2.x, -c2.y));
-  q16_pk_mul(U, vx, vy, t, s);
+  const float zx = cs * (1.0f / 32767.0f), zy = sn * (1.0f / 32767.0f);
+  const float2 zw = make_float2(fmaf(zx, w.x, -zy * w.y), fmaf(zx, w.y, zy * w.x));
+  t[2] = __fadd2_rn(t[2], zw);
 }
 
 __device__ __forceinline__ void q16_pk_rows(const float2 t[3], const float2 s[3], float2 a[3]) {

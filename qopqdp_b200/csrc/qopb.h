@@ -113,7 +113,7 @@ struct Options {
   int hop_kernel = 25;           // int16 hop variant (mixed.cu launch_q16); 25 measured fastest; -1 autotuned
   int recon_long = 1;            // int16 long links as two rows + det phase when exact
   int batch_kernel = -1;         // batched int16 hop variant (batch.cu kBhop); -1: by the number of systems, -2: autotuned
-  int multi_shift = 0;           // int16 multi-mass: 1 = sloppy multi-shift CG before the batched refinement
+  int multi_shift = 1;           // int16 multi-mass: 1 = sloppy multi-shift CG before the batched refinement (default), 0 = batched only
   int fuse_update = 1;           // int16 hop variants 20-26: 1 = the second hop reduces for a fused x / r / p update
   int pdl = 1;                   // fused int16 iteration: 1 = its kernels launched as programmatic dependents
   int serve_policy = 0;          // solve service: 0 = step every engine in turn, 1 = only the one with the oldest request

@@ -180,3 +180,46 @@ def test_batched_int16_operator_matches_fp64_per_site_24x24x24x24(big_hisq, n, v
     for h in hin + ht + ha:
         q.destroy_V(h)
     q.destroy_L(fla)
+
+
+def test_config3_multimass_every_mass_meets_target():
+    """Config 3 at its own size: HISQ 24^3x48 (eps 0.5, links built on the
+    device), one source, 12 masses sqrt(logspace(-4, 0)), rsqmin 1e-20,
+    through QOP_D3_asqtad_invert_multi with the int16 defaults (multi-shift
+    phase, then the batched refinement).  Every mass's solution, checked by
+    the oracle's FP64 operator on the device's own links
+    (examples/asqtad_test.c:84-130 check_resids), has
+    |b - A x|^2 / |b|^2 <= 1.05e-20, and the reported final_rsq is that
+    true residual."""
+    from qopqdp_b200.qop import QOP_invert_arg_t, QOP_resid_arg_t, QOP_EVEN
+    from helpers import eo_residual
+    L = (24, 24, 24, 48)
+    V = int(np.prod(L))
+    q = gpu_lattice(L, "D")
+    G = q.create_G(LT.random_gauge(L, 0.5, 2024, device="cuda"))
+    q.rephase_G(G, LT.BENCH_R0, LT.BENCH_BC, LT.BENCH_SIGNMASK)
+    H = q.hisq_create_L_from_G(LT.hisq_bench_coeffs(), G)
+    fla = q.hisq_asqtad_links(H, 0)
+    q.destroy_G(G)
+    masses = [float(x) for x in np.sqrt(np.logspace(-4, 0, 12))]
+    src = LT.gaussian_vector(L, 2024)
+    hin = q.create_V(src, QOP_EVEN)
+    outs = [q.create_V(np.zeros_like(src)) for _ in masses]
+    ras = [QOP_resid_arg_t(1e-20, 0, 0, 0, 0, 0) for _ in masses]
+    assert q.set_opts(prec_sloppy=16) == 0
+    try:
+        info = q.invert_multi(fla, [masses], [outs], [hin], QOP_invert_arg_t(1e9, 200000, 200000, 50, QOP_EVEN),
+                              [ras])
+    finally:
+        assert q.set_opts(prec_sloppy=64) == 0
+    assert info.status == 0
+    fat, lng = q.extract_L(fla, V)
+    fo = O.Fla(O.Lattice(L), fat, lng)
+    for k, m in enumerate(masses):
+        x = q.extract_V(outs[k], V)
+        true = eo_residual(fo, m, x, src, L, 0)
+        assert true <= 1.05e-20, (m, true)
+        assert abs(ras[k].final_rsq - true) <= 0.05 * true + 1e-26, (m, ras[k].final_rsq, true)
+        q.destroy_V(outs[k])
+    q.destroy_V(hin)
+    q.hisq_destroy_L(H)
