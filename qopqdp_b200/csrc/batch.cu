@@ -654,7 +654,7 @@ void BatchEngine::launch() {
   const int BG = kBhop[variant].bg;
   const int ngrp = (n + BG - 1) / BG;
   char hname[32];
-  snprintf(hname, sizeof hname, "bhop_q16_x%d", n);
+  snprintf(hname, sizeof hname, "bhop_q16_x%d", active);   // timing class: systems running in the launch
   // compulsory bytes of one hop for the systems running in this chunk
   const double hop_bytes = (double)Vh * (link_site + 2.0 * 16 * active);
   for (int k = 0; k < chunk; k++) {

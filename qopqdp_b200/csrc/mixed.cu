@@ -1475,9 +1475,20 @@ void solve_multi_mixed(QOP_info_t *info, FlaT<double> *f, QOP_invert_arg_t *ia, 
       const double t = ra[j]->rsqmin * b2;
       stop[s] = stop[s] < 0 ? t : std::min(stop[s], t);
     }
+    struct Owned {   // the phase's vectors, freed on every way out (an allocation failure included)
+      std::vector<c2<double> *> v;
+      ~Owned() {
+        for (c2<double> *q : v) dfree(q);
+      }
+      c2<double> *add() {
+        v.reserve(v.size() + 1);
+        v.push_back(dalloc<c2<double>>(vec_elems(ctx().g)));
+        return v.back();
+      }
+    } own;
     std::vector<c2<double> *> xv(ns);
-    for (int s = 0; s < ns; s++) xv[s] = dalloc<c2<double>>(vec_elems(g));
-    c2<double> *tmp = dalloc<c2<double>>(vec_elems(g));
+    for (int s = 0; s < ns; s++) xv[s] = own.add();
+    c2<double> *tmp = own.add();
     LinOp<double> L{f, std::sqrt(m2[0]), eo, tmp};
     QOP_invert_arg_t ia1 = *ia;
     QOP_resid_arg_t ra1 = QOP_RESID_ARG_DEFAULT;
@@ -1487,7 +1498,7 @@ void solve_multi_mixed(QOP_info_t *info, FlaT<double> *f, QOP_invert_arg_t *ia, 
     it1 += ra1.final_iter;
     flop += (nflop + nflopm * (ns - 1)) * ra1.final_iter * (double)g.V;
     if (ctx().verbosity >= QOP_VERB_MED) {
-      c2<double> *ax = dalloc<c2<double>>(vec_elems(g));
+      c2<double> *ax = own.add();
       for (int s = 0; s < ns; s++) {
         LinOp<double> Ls{f, std::sqrt(m2[s]), eo, tmp};
         Ls.d2(ax, xv[s]);
@@ -1495,14 +1506,11 @@ void solve_multi_mixed(QOP_info_t *info, FlaT<double> *f, QOP_invert_arg_t *ia, 
         log0(QOP_VERB_MED, "SOLVE(mixed multi-mass): mass %g true rsq %g target %g\n", std::sqrt(m2[s]),
              Blas<double>::norm2(ax, is) / b2, stop[s] / b2);
       }
-      dfree(ax);
     }
     for (int j : grp) {
       const int s = (int)(std::lower_bound(m2.begin(), m2.end(), masses[j] * masses[j]) - m2.begin());
       Blas<double>::copy(out[j], xv[s], is);
     }
-    for (int s = 0; s < ns; s++) dfree(xv[s]);
-    dfree(tmp);
   }
   int it2 = 0, nres = 0;
   std::vector<int> bat;
