@@ -506,6 +506,9 @@ int BatchEngine::running() const {
   for (int j = 0; j < d->cap; j++) n += d->sys[j].busy && d->h[j].flag != MIX_DONE;
   return n;
 }
+bool BatchEngine::running(int s) const {
+  return s >= 0 && s < d->cap && d->sys[s].busy && d->h[s].flag != MIX_DONE;
+}
 int BatchEngine::free_slot() const {
   for (int j = 0; j < d->cap; j++)
     if (!d->sys[j].busy) return j;
@@ -513,6 +516,18 @@ int BatchEngine::free_slot() const {
 }
 int BatchEngine::iters(int s) const { return d->h[s].iter + d->sys[s].nru; }
 double BatchEngine::final_rsq(int s) const { return d->sys[s].b2 > 0 ? d->sys[s].r2 / d->sys[s].b2 : 0.0; }
+
+void BatchEngine::fold(int s) {
+  Impl &e = *d;
+  StreamScope ss(e.own);
+  if (s < 0 || s >= e.cap || !e.sys[s].busy) return;
+  if (e.inflight) fail(QOP_FAIL, "batched solver: a chunk is in flight");
+  const Context &c = ctx();
+  const i64 Vh = e.Vh;
+  if (e.tc) k_b16_fold_x<<<e.gridv, 256, 0, c.s>>>(e.sys[s].x + e.is.off, e.xs, s, Vh);
+  else k_fold_x<<<grid_for(3 * Vh, 256), 256, 0, c.s>>>(e.sys[s].x + e.is.off, e.xs + 3 * s * Vh, 3 * Vh);
+  QLAUNCH();
+}
 
 void BatchEngine::release(int s) {
   if (s < 0 || s >= d->cap) return;
@@ -754,17 +769,67 @@ void run_batch(FlaT<double> *f, int eo, int n, const double *mass, c2<double> **
                const double *rsqmin, int max_iter, int *iters, double *final_rsq) {
   if (n < 1) return;
   if (n > BATCH_MAX) fail(QOP_FAIL, "run_batch: %d systems exceed the batch limit %d", n, BATCH_MAX);
-  BatchEngine e(f, eo, n);
-  for (int j = 0; j < n; j++) e.start(j, x[j], b[j], mass[j], rsqmin[j], max_iter, false);
-  for (int left = n; left > 0;) {
-    const int k = (int)e.step().size();
-    if (k == 0 && e.running() == 0) break;
-    left -= k;
+  // With option batch_tail, the last system still running leaves the batch
+  // and finishes in the one-system solver (its fused kernels cost about a
+  // third of a batched hop that carries one system): the correction
+  // A e = b - A x from its current x, to the same FP64 target.
+  const bool tail_ok = ctx().opt.batch_tail && n > 1 && !use_tc();
+  int tail = -1;
+  {
+    BatchEngine e(f, eo, n);
+    for (int j = 0; j < n; j++) e.start(j, x[j], b[j], mass[j], rsqmin[j], max_iter, false);
+    for (int left = n; left > 0;) {
+      const int k = (int)e.step().size();
+      if (k == 0 && e.running() == 0) break;
+      left -= k;
+      if (tail_ok && left == 1 && e.running() == 1) {
+        for (int j = 0; j < n; j++)
+          if (e.running(j)) tail = j;
+        break;
+      }
+    }
+    if (tail >= 0) e.fold(tail);
+    for (int j = 0; j < n; j++) {
+      iters[j] = e.iters(j);
+      final_rsq[j] = e.final_rsq(j);
+    }
+    sync();
   }
-  for (int j = 0; j < n; j++) {
-    iters[j] = e.iters(j);
-    final_rsq[j] = e.final_rsq(j);
+  if (tail < 0) return;
+  const Geom &g = ctx().g;
+  const Range is = vrange(g, eo);
+  struct Owned {
+    std::vector<c2<double> *> v;
+    ~Owned() {
+      for (c2<double> *q : v) dfree(q);
+    }
+    c2<double> *add() {
+      v.reserve(v.size() + 1);
+      v.push_back(dalloc<c2<double>>(vec_elems(ctx().g)));
+      return v.back();
+    }
+  } own;
+  c2<double> *r = own.add(), *ex = own.add(), *tmp = own.add();
+  LinOp<double> L{f, mass[tail], eo, tmp};
+  L.d2(r, x[tail]);
+  Blas<double>::axpby(r, 1.0, b[tail], -1.0, r, is);   // r = b - A x
+  const double b2 = Blas<double>::norm2(b[tail], is), r2 = Blas<double>::norm2(r, is);
+  need_finite(r2, "batched solver: residual of the last system");
+  if (!(r2 > rsqmin[tail] * b2)) {   // converged at the hand-off
+    final_rsq[tail] = b2 > 0 ? r2 / b2 : 0.0;
+    return;
   }
+  QOP_invert_arg_t ia = QOP_INVERT_ARG_DEFAULT;
+  ia.max_iter = std::max(1, max_iter - iters[tail]);
+  ia.evenodd = (QOP_evenodd_t)eo;
+  QOP_resid_arg_t ra = QOP_RESID_ARG_DEFAULT;
+  ra.rsqmin = rsqmin[tail] * b2 / r2;
+  QOP_resid_arg_t *rap = &ra;
+  const double zero = 0.0;
+  mixed_cgms(L, &ia, &rap, &zero, 1, &ex, r, eo, 16);
+  Blas<double>::axpy(x[tail], 1.0, ex, is);   // x += e
+  iters[tail] += ra.final_iter;
+  final_rsq[tail] = ra.final_rsq * r2 / b2;
   sync();
 }
 

@@ -1329,8 +1329,15 @@ static void run_mixed(LinOp<double> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t *r
         recs.push_back(ps2.idx);
       }
       if (ns > 1) {
-        k_ms_update<Sp><<<gridv, 256, 0, c.s>>>(xs, rs, ps, Aps, Vh, dst, c.d_part, c.d_count, dsh, ns, mv);
-        k_ms_p<Sp><<<gridv, 256, 0, c.s>>>(ps, rs, Vh, dst, dsh, ns, mv);
+        {
+          // compulsory bytes with every shift active: base x (FP32) rw, r rw,
+          // p and Ap read, x_s rw and p_s read per shift; then p rw, r read,
+          // p_s rw per shift
+          ProfScope pm("ms_update", (double)Vh * (4 * Sp::site_bytes + 48.0 + (ns - 1) * (48.0 + Sp::site_bytes) +
+                                                  3 * Sp::site_bytes + (ns - 1) * 2 * Sp::site_bytes));
+          k_ms_update<Sp><<<gridv, 256, 0, c.s>>>(xs, rs, ps, Aps, Vh, dst, c.d_part, c.d_count, dsh, ns, mv);
+          k_ms_p<Sp><<<gridv, 256, 0, c.s>>>(ps, rs, Vh, dst, dsh, ns, mv);
+        }
         QLAUNCHN(4);
       } else if (fuse) {
         launch_k(pdl, k_mix_update_p<Sp>, gridv, 256, c.s, xs, rs, ps, (const E *)Aps, Vh, (const MixState *)dst, seq);

@@ -115,6 +115,7 @@ struct Options {
   int batch_kernel = -1;         // batched int16 hop variant (batch.cu kBhop); -1: by the number of systems, -2: autotuned
   int multi_shift = 1;           // int16 multi-mass: 1 = sloppy multi-shift CG before the batched refinement (default), 0 = batched only
   int fuse_update = 1;           // int16 hop variants 20-26: 1 = the second hop reduces for a fused x / r / p update
+  int batch_tail = 1;            // batched solves: 1 = the last running system finishes in the one-system solver
   int pdl = 1;                   // fused int16 iteration: 1 = its kernels launched as programmatic dependents
   int serve_policy = 0;          // solve service: 0 = step every engine in turn, 1 = only the one with the oldest request
   double serve_hbm_mb = 0;       // solve service: device memory all engines together may hold (MB; 0 = free HBM less 2 GiB)

@@ -86,6 +86,7 @@ class BatchEngine {
   int cap() const;
   int busy() const;       // slots holding a system (running or finished)
   int running() const;    // slots still iterating
+  bool running(int s) const;   // slot s still iterating
   int free_slot() const;  // lowest free slot, or -1
   // start (m^2 - D D) x = b in free slot s; x (the starting guess, or zero
   // with x_zero) and b are FP64 device vectors the caller keeps until the
@@ -103,6 +104,9 @@ class BatchEngine {
   int iters(int s) const;         // hop pairs plus reliable updates
   double final_rsq(int s) const;  // FP64 |r|^2 / |b|^2
   void release(int s);
+  // folds slot s's reduced-precision partial solution into its FP64 x
+  // (between chunks), so that x is the system's current solution
+  void fold(int s);
 
  private:
   struct Impl;
