@@ -213,6 +213,7 @@ k_mix_update_p(float2 *__restrict__ xs, typename Sp::elem *__restrict__ r, typen
 constexpr int MS_MAX = 32;
 struct MsShift {
   double sigma, z, zo, bo, stop;   // index 0 (base): bo = previous alpha
+  double beo;                      // index 0 (base): previous beta (the fused update's recurrences)
   int active, pad;
 };
 struct MsVecs {
@@ -310,14 +311,16 @@ k_ms_update(float2 *__restrict__ xs, typename Sp::elem *__restrict__ r, const ty
 }
 
 // p = r + beta p;  p_s = zeta_s r + beta_s p_s for the shifts still active
+// (also records beta as the previous beta of the fused update's recurrences)
 template <class Sp>
 __global__ void __launch_bounds__(256)
 k_ms_p(typename Sp::elem *__restrict__ p, const typename Sp::elem *__restrict__ r, i64 Vh, MixState *st,
-       const MsShift *sh, int ns, MsVecs mv) {
+       MsShift *sh, int ns, MsVecs mv) {
   typedef typename Sp::elem E;
   if (st->flag) return;
   __shared__ float pz[MS_MAX], pb[MS_MAX];
   const double be = st->beta, al = st->alpha;
+  if (blockIdx.x == 0 && threadIdx.x == 0) sh[0].beo = be;   // no block reads sh[0] here
   if (threadIdx.x < MS_MAX) {
     const int s = threadIdx.x;
     float z = 0.f, b = 0.f;
@@ -352,6 +355,105 @@ k_ms_p(typename Sp::elem *__restrict__ p, const typename Sp::elem *__restrict__ 
   }
 }
 
+
+// The multi-shift update after the fused-update hop (KIND 3), in one pass:
+// base x += alpha p, r -= alpha Ap, p = r + beta p; every shift active at
+// launch x_s += alpha_s p_s and p_s = zeta_{k+1} r + beta_s p_s.  alpha,
+// beta and the new |r|^2 come from the hop; the shift scalars from the
+// recurrences above (ms_step, and beta_s as in k_ms_p), derived in every
+// block from the state at launch; the last block advances them and retires
+// the shifts whose zeta^2 |r|^2 reached their target.  When the hop asked
+// for a reliable update, p and the p_s are left to it (k_ms_p after the
+// update, with beta recomputed).  Runs only for the iteration whose hop
+// recorded `seq`.
+template <class Sp>
+__global__ void __launch_bounds__(256)
+k_ms_update_fused(float2 *__restrict__ xs, typename Sp::elem *__restrict__ r, typename Sp::elem *__restrict__ p,
+                  const typename Sp::elem *__restrict__ Ap, i64 Vh, MixState *st, int seq, double *part,
+                  unsigned *count, MsShift *sh, int ns, MsVecs mv) {
+  typedef typename Sp::elem E;
+  pdl_wait();
+  if (st->tok != seq) return;
+  const int fl = st->flag;
+  if (fl != MIX_RUN && fl != MIX_UPDATE) return;   // uniform: no block takes part in the ticket below
+  __shared__ float al_s[MS_MAX], z_s[MS_MAX], b_s[MS_MAX];
+  const double al = st->alpha, be = st->beta, rn = st->rsq, be_old = sh[0].beo, al_old = sh[0].bo;
+  if (threadIdx.x < MS_MAX) {
+    const int s = threadIdx.x;
+    float a = 0.f, z = 0.f, b = 0.f;
+    if (s > 0 && s < ns && sh[s].active) {
+      double zn, as;
+      ms_step(sh[s], al, be_old, al_old, zn, as);
+      const double d = sh[s].z * al;
+      a = (float)as;
+      z = (float)zn;
+      b = d != 0.0 ? (float)(be * zn * as / d) : 0.f;
+    }
+    al_s[s] = a;
+    z_s[s] = z;
+    b_s[s] = b;
+  }
+  __syncthreads();
+  const bool run = fl == MIX_RUN;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < Vh) {
+    const float alf = (float)al, bef = (float)be;
+    float2 pv[3], av[3], rv[3];
+    Sp::load(p, i, Vh, pv);
+    Sp::load(Ap, i, Vh, av);
+    Sp::load(r, i, Vh, rv);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      float2 xv = xs[c * Vh + i];
+      xv.x = fmaf(alf, pv[c].x, xv.x);
+      xv.y = fmaf(alf, pv[c].y, xv.y);
+      xs[c * Vh + i] = xv;
+      rv[c].x = fmaf(-alf, av[c].x, rv[c].x);
+      rv[c].y = fmaf(-alf, av[c].y, rv[c].y);
+    }
+    Sp::store(r, i, Vh, rv);
+    if (run) {
+#pragma unroll
+      for (int c = 0; c < 3; c++) pv[c] = make_float2(fmaf(bef, pv[c].x, rv[c].x), fmaf(bef, pv[c].y, rv[c].y));
+      Sp::store(p, i, Vh, pv);
+    }
+    for (int s = 1; s < ns; s++) {
+      const float a = al_s[s];
+      if (a == 0.f) continue;
+      E *q = reinterpret_cast<E *>(mv.p[s]);
+      float2 ps[3];
+      Sp::load(q, i, Vh, ps);
+      float2 *xp = mv.x[s];
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        float2 xv = xp[c * Vh + i];
+        xv.x = fmaf(a, ps[c].x, xv.x);
+        xv.y = fmaf(a, ps[c].y, xv.y);
+        xp[c * Vh + i] = xv;
+      }
+      if (!run) continue;
+      const float z = z_s[s], b = b_s[s];
+#pragma unroll
+      for (int c = 0; c < 3; c++) ps[c] = make_float2(fmaf(b, ps[c].x, z * rv[c].x), fmaf(b, ps[c].y, z * rv[c].y));
+      Sp::store(q, i, Vh, ps);
+    }
+  }
+  double acc1[1] = {0.0};   // the reduction serves only to find the last block
+  if (grid_sum<1>(acc1, part, count, &st->red)) {
+    for (int s = 1; s < ns; s++) {
+      MsShift &q = sh[s];
+      if (!q.active) continue;
+      double zn, as;
+      ms_step(q, al, be_old, al_old, zn, as);
+      q.zo = q.z;
+      q.z = zn;
+      q.bo = as;
+      if (zn * zn * rn <= q.stop) q.active = 0;
+    }
+    sh[0].bo = al;
+    sh[0].beo = be;
+  }
+}
 
 // x += xs (FP64 += FP32), xs = 0
 __global__ void k_fold_x(double2 *x, float2 *xs, i64 n) {
@@ -1186,7 +1288,7 @@ static void run_mixed(LinOp<double> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t *r
   dst = dalloc<MixState>(1);
   if (ns > 1) {
     std::vector<MsShift> hs(ns);
-    for (int s = 0; s < ns; s++) hs[s] = MsShift{ms->sigma[s], 1.0, 1.0, -1.0, ms->stop[s], 1, 0};
+    for (int s = 0; s < ns; s++) hs[s] = MsShift{ms->sigma[s], 1.0, 1.0, -1.0, ms->stop[s], 0.0, 1, 0};
     dsh = dalloc<MsShift>(ns);
     QCHECK(cudaMemcpyAsync(dsh, hs.data(), sizeof(MsShift) * ns, cudaMemcpyHostToDevice, c.s));
     for (int s = 1; s < ns; s++) {
@@ -1262,7 +1364,7 @@ static void run_mixed(LinOp<double> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t *r
       }
     }
   }
-  const bool fuse = q16v && ns == 1 && c.opt.fuse_update && hk >= 20;
+  const bool fuse = q16v && c.opt.fuse_update && hk >= 20;
   // the three kernels of the fused iteration as programmatic dependents
   const bool pdl = fuse && c.opt.pdl;
   int seq = 0;
@@ -1328,7 +1430,16 @@ static void run_mixed(LinOp<double> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t *r
         }
         recs.push_back(ps2.idx);
       }
-      if (ns > 1) {
+      if (ns > 1 && fuse) {
+        {
+          // compulsory bytes with every shift active: base x (FP32) rw, r rw,
+          // p rw, Ap read; x_s rw and p_s rw per shift
+          ProfScope pm("ms_update", (double)Vh * (48.0 + 5 * Sp::site_bytes + (ns - 1) * (48.0 + 2 * Sp::site_bytes)));
+          launch_k(pdl, k_ms_update_fused<Sp>, gridv, 256, c.s, xs, rs, ps, (const E *)Aps, Vh, dst, seq, c.d_part,
+                   c.d_count, dsh, ns, mv);
+        }
+        QLAUNCHN(3);
+      } else if (ns > 1) {
         {
           // compulsory bytes with every shift active: base x (FP32) rw, r rw,
           // p and Ap read, x_s rw and p_s read per shift; then p rw, r read,

@@ -407,3 +407,35 @@ def test_mixed_ragged_site_blocks(L):
             assert rel_norm_err(half(outs[s][0], L, 0), half(ref, L, 0)) <= max(1e-6, 30 * 1e-10 / m ** 2)
     assert q.set_opts(prec_sloppy=64, batch_kernel=-1) == 0
     q.destroy_L(fla)
+
+
+@pytest.mark.parametrize("multi_shift", [0, 1])
+def test_batch_tail_handoff_meets_targets(multi_shift):
+    """Option batch_tail: the last system running in a batch finishes in the
+    one-system solver (the correction A e = b - A x from its current x).
+    With and without the hand-off every mass meets its FP64 target (checked
+    with the oracle), and the hand-off costs the handed-off system no more
+    than a few percent of iterations."""
+    L = (8, 8, 8, 8)
+    q = gpu_lattice(L, "D")
+    fat, lng, _, _ = hisq_links(L, 0.5, 9)
+    fo = O.Fla(O.Lattice(L), fat, lng)
+    fla = q.create_L_from_raw(fat, lng)
+    rsq = 1e-20
+    ms = [0.01, 0.05, 0.2]
+    src = LT.gaussian_vector(L, 330)
+    its = {}
+    try:
+        for tail in (0, 1):
+            assert q.set_opts(prec_sloppy=16, multi_shift=multi_shift, batch_tail=tail) == 0
+            _, ras, outs = _run_multi(q, fla, [ms], [src], rsq)
+            its[tail] = [r.final_iter for r in ras[0]]
+            for j, m in enumerate(ms):
+                true = eo_residual(fo, m, outs[0][j], src, L, 0)
+                assert true <= rsq * 1.05, (tail, m, true)
+                assert abs(ras[0][j].final_rsq - true) <= 0.05 * true + 1e-26
+    finally:
+        assert q.set_opts(prec_sloppy=64, multi_shift=1, batch_tail=1) == 0
+    print("iterations without / with the hand-off", its)
+    assert max(its[1]) <= 1.1 * max(its[0]) + 20, its
+    q.destroy_L(fla)
