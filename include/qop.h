@@ -190,6 +190,11 @@ QOP_status_t QOP_asqtad_invert_set_opts(QOP_opt_t opts[], int nopts);
 QOP_status_t QOP_asqtad_force_set_opts(QOP_opt_t opts[], int nopts);
 QOP_status_t QOP_hisq_invert_set_opts(QOP_opt_t opts[], int nopts);
 QOP_status_t QOP_hisq_links_set_opts(QOP_opt_t opts[], int nopts);
+/* lib/hisq_force.c:29-52: fnmat_src_min (>= 0) and veclength (> 0) are
+   validated and kept; force_filter (>= 0, default 5e-5) regularises the
+   derivative of the U(3) projection at links whose V^+V has an eigenvalue
+   below it (the derivative of V (V^+V + force_filter)^-1/2 there). */
+QOP_status_t QOP_hisq_force_set_opts(QOP_opt_t opts[], int nopts);
 
 /* ---- per precision (include/qop_f3.h / qop_d3.h) ----------------------- */
 #define QOPB_DECLARE_PC(PC, REAL)                                              \

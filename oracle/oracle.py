@@ -59,7 +59,7 @@ def lib():
         l.or_hisq_links.restype = C.c_int
         l.or_fla_create.argtypes = [vp, C.POINTER(DP), C.POINTER(DP)]
         l.or_asqtad_deriv.argtypes = [vp, DP, C.POINTER(DP), C.POINTER(DP), C.POINTER(DP), C.POINTER(DP)]
-        l.or_asqtad_force.argtypes = [vp, DP, C.POINTER(DP), C.POINTER(DP), DP, C.POINTER(DP), C.c_int]
+        l.or_asqtad_force.argtypes = [vp, DP, C.POINTER(DP), C.POINTER(DP), DP, C.POINTER(DP), C.c_int, C.c_int]
         l.or_hisq_deriv.argtypes = [vp, DP, C.POINTER(DP), C.c_int, DP, C.POINTER(DP), C.POINTER(DP), C.POINTER(DP)]
         l.or_hisq_force.argtypes = [vp, DP, C.POINTER(DP), C.c_int, DP, C.POINTER(DP), DP, C.POINTER(DP),
                                     C.POINTER(C.c_int)]
@@ -134,15 +134,18 @@ class Lattice:
         lib().or_asqtad_deriv(self.h, _p(c), _p4(gauge), _p4(midF), _p4(midN) if midN is not None else None, _p4(der))
         return der
 
-    def asqtad_force(self, coeffs, gauge, eps, xs, force=None):
-        """force_mu += -2 TA(U_mu deriv_mu^+) for the outer products of xs."""
+    def asqtad_force(self, coeffs, gauge, eps, xs, force=None, fnmat_src_min=2):
+        """force_mu += -2 TA(U_mu deriv_mu^+) for the outer products of xs
+        (FNMAT); with fewer sources than fnmat_src_min (2, the reference's
+        default) the reference's ASVEC result, force = TA(force) - TA(U deriv^+)."""
         gauge = [f64(a) for a in gauge]
         force = [np.zeros_like(gauge[0]) for _ in range(4)] if force is None else [f64(a).copy() for a in force]
         xs = [f64(x) for x in xs]
         xp = (DP * len(xs))(*[_p(x) for x in xs])
         e = np.array(eps, dtype=np.float64)
         c = np.array(coeffs, dtype=np.float64)
-        lib().or_asqtad_force(self.h, _p(c), _p4(gauge), _p4(force), _p(e), xp, len(xs))
+        lib().or_asqtad_force(self.h, _p(c), _p4(gauge), _p4(force), _p(e), xp, len(xs),
+                              1 if len(xs) < fnmat_src_min else 0)
         return force
 
     def hisq_deriv(self, hcoef, gauge, eps_naik, midF, midN):

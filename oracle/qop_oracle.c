@@ -423,7 +423,7 @@ int or_u3reunit(const or_lat *g, double *Vf, double *Wf) {
 
 /* HISQ: lib/hisq_links_p.c:62-256 (n_naiks = 1 path; difference links only
    when n_naiks > 1, which the oracle does not need) */
-int or_hisq_links(const or_lat *g, const double h[17], double *gauge[4],
+int or_hisq_links(const or_lat *g, const double h[18], double *gauge[4],
                   double *fat[4], double *lng[4], double *Wout[4]) {
   size_t fsz = sizeof(double) * 18 * g->V;
   double *Vl[4], *Wl[4];
@@ -1285,7 +1285,7 @@ void or_asqtad_deriv(const or_lat *g, const double coef[6], double *Ur[4], doubl
 }
 
 void or_asqtad_force(const or_lat *g, const double coef[6], double *Ur[4], double *forcer[4], const double *eps,
-                     double *xr[], int nsrc) {
+                     double *xr[], int nsrc, int asvec) {
   const size_t n = 9 * (size_t)g->V;
   double *mid[8], *der[4];
   for (int i = 0; i < 8; i++) mid[i] = calloc(2 * n, sizeof(double));
@@ -1308,20 +1308,35 @@ void or_asqtad_force(const or_lat *g, const double coef[6], double *Ur[4], doubl
     }
   }
   or_asqtad_deriv(g, coef, Ur, mid, coef[5] != 0 ? mid + 4 : NULL, der);
+  /* FNMAT (asqtad_force_fnmat_p.c:530-540): force += -2 TA(U deriv^+).
+     ASVEC (asqtad_force_asvec_p.c:180-184, 403-408; chosen by
+     asqtad_force_p.c:22 when nsrc < fnmat_src_min): the outer products are
+     accumulated into the force field itself and the traceless anti-Hermitian
+     part of the sum is stored, force = TA(force + C); for the same inputs
+     TA(C) = -TA(U deriv^+), half the FNMAT contribution (as the reference,
+     compiled by oracle/ref, computes it). */
+  const double fac = asvec ? -1.0 : -2.0;
   for (int mu = 0; mu < 4; mu++) {
     const dc *Um = (const dc *)Ur[mu], *Dm = (const dc *)der[mu];
     dc *F = (dc *)forcer[mu];
 #pragma omp parallel for
     for (long z = 0; z < g->V; z++) {
-      dc a[9];
+      dc a[9], f[9];
       m_mul_na(a, Um + 9 * z, Dm + 9 * z);                 /* U deriv^+ */
-      dc tr = 0;
+      dc tr = 0, trf = 0;
       for (int k = 0; k < 3; k++) tr += a[4 * k] - conj(a[4 * k]);
+      for (int e = 0; e < 9; e++) f[e] = F[9 * z + e];
+      for (int k = 0; k < 3; k++) trf += f[4 * k] - conj(f[4 * k]);
       for (int i = 0; i < 3; i++)
         for (int j = 0; j < 3; j++) {
           dc ta = 0.5 * (a[3 * i + j] - conj(a[3 * j + i]));
           if (i == j) ta -= tr / 6.0;
-          F[9 * z + 3 * i + j] += -2.0 * ta;
+          dc base = f[3 * i + j];
+          if (asvec) {   /* TA of the incoming force */
+            base = 0.5 * (f[3 * i + j] - conj(f[3 * j + i]));
+            if (i == j) base -= trf / 6.0;
+          }
+          F[9 * z + 3 * i + j] = base + fac * ta;
         }
     }
   }
@@ -1339,12 +1354,18 @@ void or_asqtad_force(const or_lat *g, const double coef[6], double *Ur[4], doubl
 /*   GV = GW f + V (B + B^+),  B = Z [(Z^+ V^+ GW Z) o Gamma] Z^+,        */
 /*   Gamma_ij = (f(w_i) - f(w_j)) / (w_i - w_j)                           */
 /*            = -1 / (s_i s_j (s_i + s_j)),  s = sqrt(w)  (i = j: f'(w)).  */
+/* Force filter (lib/hisq_reunit_utilities_p.c:463-481, the option        */
+/* force_filter of QOP_hisq_force_set_opts, 5e-5 by default): when the    */
+/* smallest eigenvalue of Q is below ff, the derivative is the one of     */
+/* V (Q + ff)^-1/2, every w shifted by ff (the projection itself is not). */
 /* ------------------------------------------------------------------ */
-static void reunit_adj(const dc *V, const dc *GW, dc *GV) {
+static void reunit_adj(const dc *V, const dc *GW, dc *GV, double ff) {
   dc Q[9], Z[9], f[9], A[9], t[9], At[9], B[9], u[9];
   double w[3], s[3];
   m_mul_an(Q, V, V);
   herm_eig3(Q, w, Z);
+  if (ff > 0 && fmin(w[0], fmin(w[1], w[2])) < ff)
+    for (int i = 0; i < 3; i++) w[i] += ff;
   for (int i = 0; i < 3; i++) s[i] = sqrt(w[i]);
   for (int i = 0; i < 3; i++)
     for (int j = 0; j < 3; j++) {
@@ -1366,7 +1387,7 @@ static void reunit_adj(const dc *V, const dc *GW, dc *GV) {
   for (int e = 0; e < 9; e++) GV[e] += u[e];
 }
 
-void or_hisq_deriv(const or_lat *g, const double h[17], double *U[4], int n_naiks, const double *eps_naik,
+void or_hisq_deriv(const or_lat *g, const double h[18], double *U[4], int n_naiks, const double *eps_naik,
                    double **midF, double **midN, double *deriv[4]) {
   const size_t n = 18 * (size_t)g->V;
   double *Vl[4], *Wl[4], *GW[4], *tmp[4], *GV[4];
@@ -1390,12 +1411,12 @@ void or_hisq_deriv(const or_lat *g, const double h[17], double *U[4], int n_naik
   for (int i = 0; i < 4; i++)
 #pragma omp parallel for
     for (long s = 0; s < g->V; s++)
-      reunit_adj((const dc *)Vl[i] + 9 * s, (const dc *)GW[i] + 9 * s, (dc *)GV[i] + 9 * s);
+      reunit_adj((const dc *)Vl[i] + 9 * s, (const dc *)GW[i] + 9 * s, (dc *)GV[i] + 9 * s, h[17]);
   or_asqtad_deriv(g, c7, U, GV, NULL, deriv);
   for (int i = 0; i < 4; i++) { free(Vl[i]); free(Wl[i]); free(GW[i]); free(tmp[i]); free(GV[i]); }
 }
 
-void or_hisq_force(const or_lat *g, const double h[17], double *Ur[4], int n_naiks, const double *eps_naik,
+void or_hisq_force(const or_lat *g, const double h[18], double *Ur[4], int n_naiks, const double *eps_naik,
                    double *forcer[4], const double *res, double *xr[], const int *n_orders_naik) {
   const size_t n = 18 * (size_t)g->V;
   double **mid = malloc(sizeof(double *) * 8 * n_naiks), *der[4];

@@ -54,10 +54,11 @@ int or_u3_un_analytic(const double V[18], double W[18], int allow_svd,
                       double svd_rel_err, double svd_abs_err);
 int or_u3reunit(const or_lat *g, double *Vf, double *Wf);
 /* HISQ: returns number of SVD-fallback sites. out fat/long = asqtad stage
-   (eps index 0); hcoef layout = 17 doubles:
+   (eps index 0); hcoef layout = 18 doubles:
    fat7[1,3,5,7,lepage], asqtad[1,3,5,7,lepage,naik], diff[1,naik],
-   use_fat7_lepage, allow_svd, svd_rel, svd_abs */
-int or_hisq_links(const or_lat *g, const double hcoef[17], double *gauge[4],
+   use_fat7_lepage, allow_svd, svd_rel, svd_abs, force_filter (the last one
+   read by the force routines only) */
+int or_hisq_links(const or_lat *g, const double hcoef[18], double *gauge[4],
                   double *fat[4], double *lng[4], double *W[4] /* may be NULL */);
 
 /* asqtad operator object (links scaled by 1/2, double stored) */
@@ -92,11 +93,14 @@ void or_solve_multi(or_fla *f, or_invert_arg *ia, or_resid_arg *ra[],
    dE = Re sum tr[ deriv^+ dU ]; midN may be NULL (no Naik term).
    force: the outer products midF_mu(x) = -s(x) sum_i eps_i x_i(x) x_i(x+mu)^+
    (midN with x+3mu; s = +1 even, -1 odd sites), deriv, and
-   force_mu += -2 TA(U_mu deriv_mu^+), TA the traceless anti-Hermitian part. */
+   force_mu += -2 TA(U_mu deriv_mu^+), TA the traceless anti-Hermitian part
+   (the FNMAT algorithm); asvec != 0 gives the reference's ASVEC result,
+   force_mu = TA(force_mu) - TA(U_mu deriv_mu^+) (asqtad_force_p.c:22 picks it
+   for nsrc < fnmat_src_min, 2 by default). */
 void or_asqtad_deriv(const or_lat *g, const double coef[6], double *U[4],
                      double *midF[4], double *midN[4], double *deriv[4]);
 void or_asqtad_force(const or_lat *g, const double coef[6], double *U[4],
-                     double *force[4], const double *eps, double *x[], int nsrc);
+                     double *force[4], const double *eps, double *x[], int nsrc, int asvec);
 
 /* HISQ fermion force (lib/hisq_force_p.c:50-80, hisq_force_fnmat2_p.c:7-231).
    W = reunit(V), V = fat7(U) (or_hisq_links).  deriv is the derivative of
@@ -105,9 +109,9 @@ void or_asqtad_force(const or_lat *g, const double coef[6], double *U[4],
    c_k = eps_naik[k]); mids are n_naiks x 4 fields.  The force builds
    MF_k = s(x) sum_i res_i x_i(x) x_i(x+mu)^+ over group k's sources (group 0:
    all sources; s = +1 even, -1 odd) and adds TA(U_mu (2 deriv_mu)^+). */
-void or_hisq_deriv(const or_lat *g, const double hcoef[17], double *U[4], int n_naiks, const double *eps_naik,
+void or_hisq_deriv(const or_lat *g, const double hcoef[18], double *U[4], int n_naiks, const double *eps_naik,
                    double **midF, double **midN, double *deriv[4]);
-void or_hisq_force(const or_lat *g, const double hcoef[17], double *U[4], int n_naiks, const double *eps_naik,
+void or_hisq_force(const or_lat *g, const double hcoef[18], double *U[4], int n_naiks, const double *eps_naik,
                    double *force[4], const double *res, double *x[], const int *n_orders_naik);
 
 /* threads used by OpenMP regions (0 = leave default) */

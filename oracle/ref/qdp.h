@@ -168,7 +168,28 @@ typedef struct { int *d; } QDP_Int;
   void QDP_##PC##_destroy_D(QDP_##PC##_DiracFermion *);                                                        \
   void QDP_##PC##_D_eq_D(QDP_##PC##_DiracFermion *, QDP_##PC##_DiracFermion *, QDP_Subset);                    \
   void QDP_##PC##_insert_D(QDP_##PC##_DiracFermion *, QLA_##PC##_DiracFermion *, QDP_Subset);                  \
-  void QDP_##PC##_extract_D(QLA_##PC##_DiracFermion *, QDP_##PC##_DiracFermion *, QDP_Subset);
+  void QDP_##PC##_extract_D(QLA_##PC##_DiracFermion *, QDP_##PC##_DiracFermion *, QDP_Subset);                 \
+  void QDP_##PC##_M_eq_Ma(QDP_##PC##_ColorMatrix *, QDP_##PC##_ColorMatrix *, QDP_Subset);                      \
+  void QDP_##PC##_M_peq_Ma(QDP_##PC##_ColorMatrix *, QDP_##PC##_ColorMatrix *, QDP_Subset);                     \
+  void QDP_##PC##_M_eqm_M(QDP_##PC##_ColorMatrix *, QDP_##PC##_ColorMatrix *, QDP_Subset);                      \
+  void QDP_##PC##_M_meq_M(QDP_##PC##_ColorMatrix *, QDP_##PC##_ColorMatrix *, QDP_Subset);                      \
+  void QDP_##PC##_M_eq_antiherm_M(QDP_##PC##_ColorMatrix *, QDP_##PC##_ColorMatrix *, QDP_Subset);              \
+  void QDP_##PC##_M_eq_r_times_M_plus_M(QDP_##PC##_ColorMatrix *, QLA_##P##_Real *, QDP_##PC##_ColorMatrix *,   \
+                                        QDP_##PC##_ColorMatrix *, QDP_Subset);                                   \
+  void QDP_##PC##_M_eq_Ma_times_Ma(QDP_##PC##_ColorMatrix *, QDP_##PC##_ColorMatrix *,                         \
+                                   QDP_##PC##_ColorMatrix *, QDP_Subset);                                        \
+  void QDP_##PC##_M_peq_M_times_M(QDP_##PC##_ColorMatrix *, QDP_##PC##_ColorMatrix *,                          \
+                                  QDP_##PC##_ColorMatrix *, QDP_Subset);                                         \
+  void QDP_##PC##_M_meq_M_times_M(QDP_##PC##_ColorMatrix *, QDP_##PC##_ColorMatrix *,                          \
+                                  QDP_##PC##_ColorMatrix *, QDP_Subset);                                         \
+  void QDP_##PC##_M_peq_M_times_Ma(QDP_##PC##_ColorMatrix *, QDP_##PC##_ColorMatrix *,                         \
+                                   QDP_##PC##_ColorMatrix *, QDP_Subset);                                        \
+  void QDP_##PC##_M_eq_V_times_Va(QDP_##PC##_ColorMatrix *, QDP_##PC##_ColorVector *,                          \
+                                  QDP_##PC##_ColorVector *, QDP_Subset);                                         \
+  void QDP_##PC##_M_vpeq_V_times_Va(QDP_##PC##_ColorMatrix **, QDP_##PC##_ColorVector **,                      \
+                                    QDP_##PC##_ColorVector **, QDP_Subset, int);                                 \
+  void QDP_##PC##_V_veq_M_times_V(QDP_##PC##_ColorVector **, QDP_##PC##_ColorMatrix **,                        \
+                                  QDP_##PC##_ColorVector **, QDP_Subset, int);
 QDP_SHIM_DECLARE(F3, F)
 QDP_SHIM_DECLARE(D3, D)
 
@@ -329,6 +350,19 @@ typedef QDP_D3_DiracFermion QDP_D_DiracFermion;
 #define QDP_D_eq_D QDP_SHIM_P(D_eq_D)
 #define QDP_insert_D QDP_SHIM_P(insert_D)
 #define QDP_extract_D QDP_SHIM_P(extract_D)
+#define QDP_M_eq_Ma QDP_SHIM_P(M_eq_Ma)
+#define QDP_M_peq_Ma QDP_SHIM_P(M_peq_Ma)
+#define QDP_M_eqm_M QDP_SHIM_P(M_eqm_M)
+#define QDP_M_meq_M QDP_SHIM_P(M_meq_M)
+#define QDP_M_eq_antiherm_M QDP_SHIM_P(M_eq_antiherm_M)
+#define QDP_M_eq_r_times_M_plus_M QDP_SHIM_P(M_eq_r_times_M_plus_M)
+#define QDP_M_eq_Ma_times_Ma QDP_SHIM_P(M_eq_Ma_times_Ma)
+#define QDP_M_peq_M_times_M QDP_SHIM_P(M_peq_M_times_M)
+#define QDP_M_meq_M_times_M QDP_SHIM_P(M_meq_M_times_M)
+#define QDP_M_peq_M_times_Ma QDP_SHIM_P(M_peq_M_times_Ma)
+#define QDP_M_eq_V_times_Va QDP_SHIM_P(M_eq_V_times_Va)
+#define QDP_M_vpeq_V_times_Va QDP_SHIM_P(M_vpeq_V_times_Va)
+#define QDP_V_veq_M_times_V QDP_SHIM_P(V_veq_M_times_V)
 
 #ifdef __cplusplus
 }

@@ -392,3 +392,110 @@ void QDP_m_eq_sum_M(QM *r, QDP_ColorMatrix *a, QDP_Subset s) {
       r->e[x][y].imag = im[x][y];
     }
 }
+
+/* ---------------------------------------------------------------- force algebra */
+void QDP_M_eq_Ma(QDP_ColorMatrix *r, QDP_ColorMatrix *a, QDP_Subset s) {
+  SITES(s) {
+    QM t;
+    for (int x = 0; x < 3; x++)
+      for (int y = 0; y < 3; y++) {
+        t.e[x][y].real = a->d[i].e[y][x].real;
+        t.e[x][y].imag = -a->d[i].e[y][x].imag;
+      }
+    r->d[i] = t;
+  }
+}
+void QDP_M_peq_Ma(QDP_ColorMatrix *r, QDP_ColorMatrix *a, QDP_Subset s) {
+  SITES(s) {
+    QM t;
+    for (int x = 0; x < 3; x++)
+      for (int y = 0; y < 3; y++) {
+        t.e[x][y].real = r->d[i].e[x][y].real + a->d[i].e[y][x].real;
+        t.e[x][y].imag = r->d[i].e[x][y].imag - a->d[i].e[y][x].imag;
+      }
+    r->d[i] = t;
+  }
+}
+void QDP_M_eqm_M(QDP_ColorMatrix *r, QDP_ColorMatrix *a, QDP_Subset s) {
+  SITES(s) for (int x = 0; x < 3; x++) for (int y = 0; y < 3; y++) {
+        r->d[i].e[x][y].real = -a->d[i].e[x][y].real;
+        r->d[i].e[x][y].imag = -a->d[i].e[x][y].imag;
+      }
+}
+void QDP_M_meq_M(QDP_ColorMatrix *r, QDP_ColorMatrix *a, QDP_Subset s) {
+  SITES(s) for (int x = 0; x < 3; x++) for (int y = 0; y < 3; y++) {
+        r->d[i].e[x][y].real -= a->d[i].e[x][y].real;
+        r->d[i].e[x][y].imag -= a->d[i].e[x][y].imag;
+      }
+}
+/* traceless anti-Hermitian part: (a - a^+)/2 minus its trace / 3 on the diagonal */
+void QDP_M_eq_antiherm_M(QDP_ColorMatrix *r, QDP_ColorMatrix *a, QDP_Subset s) {
+  SITES(s) {
+    const QM *m = &a->d[i];
+    QM t;
+    double trim = 0;
+    for (int k = 0; k < 3; k++) trim += m->e[k][k].imag;
+    for (int x = 0; x < 3; x++)
+      for (int y = 0; y < 3; y++) {
+        t.e[x][y].real = 0.5 * (m->e[x][y].real - m->e[y][x].real);
+        t.e[x][y].imag = 0.5 * (m->e[x][y].imag + m->e[y][x].imag);
+      }
+    for (int k = 0; k < 3; k++) t.e[k][k].imag -= trim / 3.0;
+    r->d[i] = t;
+  }
+}
+void QDP_M_eq_r_times_M_plus_M(QDP_ColorMatrix *r, QLA_Real *f, QDP_ColorMatrix *a, QDP_ColorMatrix *b,
+                               QDP_Subset s) {
+  const R k = *f;
+  SITES(s) for (int x = 0; x < 3; x++) for (int y = 0; y < 3; y++) {
+        const R re = k * a->d[i].e[x][y].real + b->d[i].e[x][y].real;
+        const R im = k * a->d[i].e[x][y].imag + b->d[i].e[x][y].imag;
+        r->d[i].e[x][y].real = re;
+        r->d[i].e[x][y].imag = im;
+      }
+}
+void QDP_M_eq_Ma_times_Ma(QDP_ColorMatrix *r, QDP_ColorMatrix *a, QDP_ColorMatrix *b, QDP_Subset s) {
+  SITES(s) mm(&r->d[i], &a->d[i], 1, &b->d[i], 1);
+}
+static inline void m_acc(QM *r, const QM *t, R sign) {
+  for (int x = 0; x < 3; x++)
+    for (int y = 0; y < 3; y++) {
+      r->e[x][y].real += sign * t->e[x][y].real;
+      r->e[x][y].imag += sign * t->e[x][y].imag;
+    }
+}
+void QDP_M_peq_M_times_M(QDP_ColorMatrix *r, QDP_ColorMatrix *a, QDP_ColorMatrix *b, QDP_Subset s) {
+  SITES(s) {
+    QM t;
+    mm(&t, &a->d[i], 0, &b->d[i], 0);
+    m_acc(&r->d[i], &t, 1);
+  }
+}
+void QDP_M_meq_M_times_M(QDP_ColorMatrix *r, QDP_ColorMatrix *a, QDP_ColorMatrix *b, QDP_Subset s) {
+  SITES(s) {
+    QM t;
+    mm(&t, &a->d[i], 0, &b->d[i], 0);
+    m_acc(&r->d[i], &t, -1);
+  }
+}
+void QDP_M_peq_M_times_Ma(QDP_ColorMatrix *r, QDP_ColorMatrix *a, QDP_ColorMatrix *b, QDP_Subset s) {
+  SITES(s) {
+    QM t;
+    mm(&t, &a->d[i], 0, &b->d[i], 1);
+    m_acc(&r->d[i], &t, 1);
+  }
+}
+/* outer product r_xy = v_x conj(w_y) */
+void QDP_M_eq_V_times_Va(QDP_ColorMatrix *r, QDP_ColorVector *v, QDP_ColorVector *w, QDP_Subset s) {
+  SITES(s) for (int x = 0; x < 3; x++) for (int y = 0; y < 3; y++) r->d[i].e[x][y] = cconjmul(w->d[i].c[y], v->d[i].c[x]);
+}
+void QDP_M_vpeq_V_times_Va(QDP_ColorMatrix **r, QDP_ColorVector **v, QDP_ColorVector **w, QDP_Subset s, int n) {
+  for (int k = 0; k < n; k++) SITES(s) for (int x = 0; x < 3; x++) for (int y = 0; y < 3; y++) {
+          const C p = cconjmul(w[k]->d[i].c[y], v[k]->d[i].c[x]);
+          r[k]->d[i].e[x][y].real += p.real;
+          r[k]->d[i].e[x][y].imag += p.imag;
+        }
+}
+void QDP_V_veq_M_times_V(QDP_ColorVector **r, QDP_ColorMatrix **m, QDP_ColorVector **v, QDP_Subset s, int n) {
+  for (int k = 0; k < n; k++) SITES(s) mv(&r[k]->d[i], &m[k]->d[i], &v[k]->d[i]);
+}

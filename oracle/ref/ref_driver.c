@@ -272,3 +272,80 @@ int qr_set_threads(int n) {
   return 1;
 #endif
 }
+
+/* ------------------------------------------------------------- forces */
+/* force[mu] (V x 18 doubles, accumulated into) += the asqtad fermion force
+   of QOP_D3_asqtad_force_multi_qdp (lib/asqtad_force_p.c:15-38) for the
+   gauge field `gauge`, coefficients as in qr_asqtad_links_from_G, and nsrc
+   raw vectors x[k] (V x 6) with weights eps[k]; fnmat_src_min (the
+   QOP_asqtad_force_set_opts option) selects the ASVEC algorithm for
+   nsrc < fnmat_src_min, else FNMAT */
+int qr_asqtad_force(const double coeffs[6], double *gauge[4], double *force[4], const double *eps, double *x[],
+                    int nsrc, int fnmat_src_min) {
+  QOP_info_t info = QOP_INFO_ZERO;
+  QOP_opt_t o[1] = {{"fnmat_src_min", (double)fnmat_src_min, NULL}};
+  if (QOP_asqtad_force_set_opts(o, 1) != QOP_SUCCESS) return QOP_FAIL;
+  QDP_D3_ColorMatrix *g[4], *f[4];
+  QDP_D3_ColorVector *xv[nsrc];
+  double e[nsrc];
+  for (int mu = 0; mu < 4; mu++) {
+    g[mu] = QDP_D3_create_M();
+    f[mu] = QDP_D3_create_M();
+    memcpy(g[mu]->d, gauge[mu], sizeof(double) * 18 * QDP_shim_V);
+    memcpy(f[mu]->d, force[mu], sizeof(double) * 18 * QDP_shim_V);
+  }
+  for (int k = 0; k < nsrc; k++) {
+    xv[k] = vd_from(x[k]);
+    e[k] = eps[k];
+  }
+  QOP_asqtad_coeffs_t c;
+  c.one_link = coeffs[0];
+  c.three_staple = coeffs[1];
+  c.five_staple = coeffs[2];
+  c.seven_staple = coeffs[3];
+  c.lepage = coeffs[4];
+  c.naik = coeffs[5];
+  QOP_D3_asqtad_force_multi_qdp(&info, g, f, &c, e, xv, nsrc);
+  for (int mu = 0; mu < 4; mu++) {
+    memcpy(force[mu], f[mu]->d, sizeof(double) * 18 * QDP_shim_V);
+    QDP_D3_destroy_M(g[mu]);
+    QDP_D3_destroy_M(f[mu]);
+  }
+  for (int k = 0; k < nsrc; k++) QDP_D3_destroy_V(xv[k]);
+  return info.status;
+}
+
+/* deriv[mu] (V x 18 doubles, accumulated into) += the derivative of
+   Re sum tr[midF^+ fat + midN^+ long] with respect to the gauge links, as
+   the reference's QOP_D3_asqtad_deriv forms it (lib/asqtad_force_fnmat_p.c;
+   midN may be NULL) */
+int qr_asqtad_deriv(const double coeffs[6], double *gauge[4], double *deriv[4], double *midF[4], double *midN[4]) {
+  QOP_info_t info = QOP_INFO_ZERO;
+  QDP_D3_ColorMatrix *g[4], *d[4], *mf[4], *mn[4];
+  for (int mu = 0; mu < 4; mu++) {
+    g[mu] = QDP_D3_create_M();
+    d[mu] = QDP_D3_create_M();
+    mf[mu] = QDP_D3_create_M();
+    mn[mu] = QDP_D3_create_M();
+    memcpy(g[mu]->d, gauge[mu], sizeof(double) * 18 * QDP_shim_V);
+    memcpy(d[mu]->d, deriv[mu], sizeof(double) * 18 * QDP_shim_V);
+    memcpy(mf[mu]->d, midF[mu], sizeof(double) * 18 * QDP_shim_V);
+    if (midN) memcpy(mn[mu]->d, midN[mu], sizeof(double) * 18 * QDP_shim_V);
+  }
+  QOP_asqtad_coeffs_t c;
+  c.one_link = coeffs[0];
+  c.three_staple = coeffs[1];
+  c.five_staple = coeffs[2];
+  c.seven_staple = coeffs[3];
+  c.lepage = coeffs[4];
+  c.naik = coeffs[5];
+  QOP_D3_asqtad_deriv(&info, g, d, &c, mf, midN ? mn : NULL);
+  for (int mu = 0; mu < 4; mu++) {
+    memcpy(deriv[mu], d[mu]->d, sizeof(double) * 18 * QDP_shim_V);
+    QDP_D3_destroy_M(g[mu]);
+    QDP_D3_destroy_M(d[mu]);
+    QDP_D3_destroy_M(mf[mu]);
+    QDP_D3_destroy_M(mn[mu]);
+  }
+  return info.status;
+}

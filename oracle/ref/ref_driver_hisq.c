@@ -77,3 +77,68 @@ int qr_hisq_links(const double hc[13], int n_naiks, const double *eps_naik, doub
   for (int mu = 0; mu < 4; mu++) QDP_D3_destroy_M(g[mu]);
   return info.status;
 }
+
+/* force[mu] (V x 18 doubles, accumulated into) += the HISQ fermion force of
+   QOP_D3_hisq_force_multi_qdp (lib/hisq_force_p.c:44-58) for the links
+   QOP_D3_hisq_create_L_from_G builds from `gauge` (coefficients as in
+   qr_hisq_links, Naik epsilons eps_naik[n_naiks]), with the raw vectors
+   x[k] (V x 6) weighted by res[k] and grouped by Naik term as n_orders[k]
+   says; force_filter is the QOP_hisq_force_set_opts option (5e-5 by
+   default in the reference) */
+int qr_hisq_force(const double hc[13], int n_naiks, const double *eps_naik, double *gauge[4], double *force[4],
+                  const double *res, double *x[], const int *n_orders, double force_filter) {
+  QOP_info_t info = QOP_INFO_ZERO;
+  QOP_opt_t fopt[1] = {{"force_filter", force_filter, NULL}};
+  if (QOP_hisq_force_set_opts(fopt, 1) != QOP_SUCCESS) return QOP_FAIL;
+  QOP_opt_t opt[2] = {{"want_deps", n_naiks > 1 ? 1.0 : 0.0, NULL}, {"want_aux", 1.0, NULL}};
+  QOP_hisq_links_set_opts(opt, 2);
+  QOP_hisq_coeffs_t c;
+  memset(&c, 0, sizeof c);
+  c.n_naiks = n_naiks;
+  for (int k = 0; k < n_naiks; k++) c.eps_naik[k] = eps_naik[k];
+  c.ugroup = QOP_UNITARIZE_U3;
+  c.umethod = QOP_UNITARIZE_RATIONAL;   /* the force path of the analytic U(3) derivative (lib/hisq_force_fnmat_p.c:138-160) */
+  c.fat7_one_link = hc[0];
+  c.fat7_three_staple = hc[1];
+  c.fat7_five_staple = hc[2];
+  c.fat7_seven_staple = hc[3];
+  c.fat7_lepage = hc[4];
+  c.asqtad_one_link = hc[5];
+  c.asqtad_three_staple = hc[6];
+  c.asqtad_five_staple = hc[7];
+  c.asqtad_seven_staple = hc[8];
+  c.asqtad_lepage = hc[9];
+  c.asqtad_naik = hc[10];
+  c.difference_one_link = hc[11];
+  c.difference_naik = hc[12];
+  int nterms = 0;
+  for (int k = 0; k < n_naiks; k++) nterms += n_orders[k];
+  QDP_D3_ColorMatrix *g[4], *f[4];
+  QDP_D3_ColorVector *xv[nterms];
+  QLA_D_Real r[nterms];
+  int no[n_naiks];
+  for (int k = 0; k < n_naiks; k++) no[k] = n_orders[k];
+  for (int mu = 0; mu < 4; mu++) {
+    g[mu] = QDP_D3_create_M();
+    f[mu] = QDP_D3_create_M();
+    memcpy(g[mu]->d, gauge[mu], sizeof(double) * 18 * QDP_shim_V);
+    memcpy(f[mu]->d, force[mu], sizeof(double) * 18 * QDP_shim_V);
+  }
+  for (int k = 0; k < nterms; k++) {
+    xv[k] = QDP_D3_create_V();
+    memcpy(xv[k]->d, x[k], sizeof(double) * 6 * QDP_shim_V);
+    r[k] = res[k];
+  }
+  QOP_D3_GaugeField *gf = QOP_D3_create_G_from_qdp(g);
+  QOP_D3_FermionLinksHisq *flh = QOP_D3_hisq_create_L_from_G(&info, &c, gf);
+  QOP_D3_hisq_force_multi_qdp(&info, flh, f, &c, r, xv, no);
+  for (int mu = 0; mu < 4; mu++) {
+    memcpy(force[mu], f[mu]->d, sizeof(double) * 18 * QDP_shim_V);
+    QDP_D3_destroy_M(g[mu]);
+    QDP_D3_destroy_M(f[mu]);
+  }
+  for (int k = 0; k < nterms; k++) QDP_D3_destroy_V(xv[k]);
+  QOP_D3_hisq_destroy_L(flh);
+  QOP_D3_destroy_G(gf);
+  return info.status;
+}

@@ -77,6 +77,12 @@ def _load(L):
     l.qr_asqtad_links_from_G.argtypes = [DP, C.POINTER(DP), C.POINTER(DP), C.POINTER(DP)]
     l.qr_hisq_links.argtypes = [DP, C.c_int, DP, C.POINTER(DP), C.POINTER(DP), C.POINTER(DP), C.POINTER(DP),
                                 C.POINTER(DP), C.POINTER(DP)]
+    l.qr_asqtad_deriv.argtypes = [DP, C.POINTER(DP), C.POINTER(DP), C.POINTER(DP), C.POINTER(DP)]
+    l.QOP_D3_u3_un_der_analytic.argtypes = [C.c_void_p, DP, DP, DP, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    l.QOP_hisq_force_set_opts.argtypes = [C.c_void_p, C.c_int]
+    l.qr_asqtad_force.argtypes = [DP, C.POINTER(DP), C.POINTER(DP), DP, C.POINTER(DP), C.c_int, C.c_int]
+    l.qr_hisq_force.argtypes = [DP, C.c_int, DP, C.POINTER(DP), C.POINTER(DP), DP, C.POINTER(DP),
+                                C.POINTER(C.c_int), C.c_double]
     st = l.qr_init((C.c_int * 4)(*key))
     if st != 0:
         raise RuntimeError("QOP_init failed (%d)" % st)
@@ -195,3 +201,74 @@ def set_threads(L, n):
     """OpenMP threads of the site loops in the copy serving L (n <= 0 keeps
     the current number); returns the number in effect."""
     return _load(tuple(L)).qr_set_threads(int(n))
+
+
+def asqtad_force(L, coeffs, gauge, eps, xs, force=None, fnmat_src_min=2):
+    """force_mu += the asqtad fermion force of QOP_D3_asqtad_force_multi_qdp
+    for raw vectors xs with weights eps (oracle.Lattice.asqtad_force call
+    surface); fnmat_src_min picks the reference's ASVEC (nsrc below it) or
+    FNMAT algorithm."""
+    gauge = [f64(a) for a in gauge]
+    force = [np.zeros_like(gauge[0]) for _ in range(4)] if force is None else [f64(a).copy() for a in force]
+    xs = [f64(x) for x in xs]
+    P = lambda arrs: (DP * len(arrs))(*[_p(a) for a in arrs])
+    st = _load(tuple(L)).qr_asqtad_force(_p(f64(coeffs)), P(gauge), P(force), _p(f64(eps)), P(xs), len(xs),
+                                         int(fnmat_src_min))
+    if st != 0:
+        raise RuntimeError("QOP_asqtad_force_multi_qdp status %d" % st)
+    return force
+
+
+def hisq_force(L, hcoef, gauge, eps_naik, res, xs, n_orders, force=None):
+    """force_mu += the HISQ fermion force of QOP_D3_hisq_force_multi_qdp on
+    the links QOP_D3_hisq_create_L_from_G builds from gauge
+    (oracle.Lattice.hisq_force call surface)."""
+    gauge = [f64(a) for a in gauge]
+    force = [np.zeros_like(gauge[0]) for _ in range(4)] if force is None else [f64(a).copy() for a in force]
+    xs = [f64(x) for x in xs]
+    P = lambda arrs: (DP * len(arrs))(*[_p(a) for a in arrs])
+    hcoef = np.asarray(hcoef)
+    ff = float(hcoef[17]) if len(hcoef) > 17 else 5e-5
+    st = _load(tuple(L)).qr_hisq_force(_p(f64(hcoef[:13])), len(eps_naik), _p(f64(eps_naik)), P(gauge),
+                                       P(force), _p(f64(res)), P(xs), (C.c_int * len(n_orders))(*n_orders), ff)
+    if st != 0:
+        raise RuntimeError("QOP_hisq_force_multi_qdp status %d" % st)
+    return force
+
+
+def asqtad_deriv(L, coeffs, gauge, midF, midN=None):
+    """The reference's QOP_D3_asqtad_deriv (oracle.Lattice.asqtad_deriv call
+    surface): its derivative field equals the oracle's up to terms U H, H
+    Hermitian, that the force's projection TA(U D^+) removes."""
+    gauge = [f64(a) for a in gauge]
+    der = [np.zeros_like(gauge[0]) for _ in range(4)]
+    st = _load(tuple(L)).qr_asqtad_deriv(_p(f64(coeffs)), _p4(gauge), _p4(der), _p4([f64(a) for a in midF]),
+                                         _p4([f64(a) for a in midN]) if midN is not None else None)
+    if st != 0:
+        raise RuntimeError("QOP_asqtad_deriv status %d" % st)
+    return der
+
+
+class _Info(C.Structure):
+    _fields_ = [("final_sec", C.c_double), ("final_flop", C.c_double), ("status", C.c_int), ("count1", C.c_int),
+                ("count2", C.c_int)]
+
+
+class _Opt(C.Structure):
+    _fields_ = [("tag", C.c_char_p), ("value", C.c_double), ("extra", C.c_void_p)]
+
+
+def u3_der(L, V, force_filter=5e-5):
+    """The reference's QOP_D3_u3_un_der_analytic for one 3x3 complex matrix V:
+    (dW/dV, dW^+/dV) as [i, j, m, n] = d(.)_ij / dV_mn, and whether the force
+    filter was applied (QOP_hisq_force_set_opts force_filter)."""
+    l = _load(tuple(L))
+    o = _Opt(b"force_filter", float(force_filter), None)
+    if l.QOP_hisq_force_set_opts(C.addressof(o), 1) != 0:
+        raise RuntimeError("QOP_hisq_force_set_opts failed")
+    v = np.ascontiguousarray(np.stack([np.real(V), np.imag(V)], -1), dtype=np.float64)
+    dw, dwd = np.zeros((3, 3, 3, 3, 2)), np.zeros((3, 3, 3, 3, 2))
+    svd, ff, info = C.c_int(0), C.c_int(0), _Info()
+    l.QOP_D3_u3_un_der_analytic(C.addressof(info), _p(v), _p(dw), _p(dwd), C.byref(svd), C.byref(ff))
+    cz = lambda a: np.einsum("imnj->ijmn", a[..., 0] + 1j * a[..., 1])
+    return cz(dw), cz(dwd), bool(ff.value)

@@ -420,8 +420,29 @@ QOPB_DEFINE_FORCE(D3, double, double)
 QOPB_DEFINE_EIGCG(F3, float)
 QOPB_DEFINE_EIGCG(D3, double)
 
-// lib/asqtad_force.c:19-41: validated and kept; the device force has one
-// algorithm for every number of sources, so they select nothing here
+// lib/asqtad_force.c:19-41: fnmat_src_min selects the normalisation of the
+// reference's ASVEC algorithm for calls with fewer sources (asqtad_force in
+// force.cu); veclength (ASVEC's block of sources) is validated and kept
+// lib/hisq_force.c:29-52 (the reference has one HISQ force algorithm; its
+// fnmat_src_min and veclength are validated and kept, force_filter is used
+// by the U(3) projection's adjoint in force.cu)
+extern "C" QOP_status_t QOP_hisq_force_set_opts(QOP_opt_t opts[], int nopts) {
+  Options &o = ctx().opt;
+  int fsm = o.hisq_fnmat_src_min, vl = o.hisq_veclength;
+  double ff = o.hisq_force_filter;
+  for (int i = 0; i < nopts; i++) {
+    if (!opts[i].tag) continue;
+    if (!strcmp(opts[i].tag, "fnmat_src_min")) fsm = (int)opts[i].value;
+    else if (!strcmp(opts[i].tag, "veclength")) vl = (int)opts[i].value;
+    else if (!strcmp(opts[i].tag, "force_filter")) ff = opts[i].value;
+  }
+  if (fsm < 0 || vl <= 0 || !(ff >= 0)) return QOP_FAIL;
+  o.hisq_fnmat_src_min = fsm;
+  o.hisq_veclength = vl;
+  o.hisq_force_filter = ff;
+  return QOP_SUCCESS;
+}
+
 extern "C" QOP_status_t QOP_asqtad_force_set_opts(QOP_opt_t opts[], int nopts) {
   int fsm = ctx().opt.force_fnmat_src_min, vl = ctx().opt.force_veclength;
   for (int i = 0; i < nopts; i++) {

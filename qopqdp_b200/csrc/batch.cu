@@ -798,17 +798,7 @@ void run_batch(FlaT<double> *f, int eo, int n, const double *mass, c2<double> **
   if (tail < 0) return;
   const Geom &g = ctx().g;
   const Range is = vrange(g, eo);
-  struct Owned {
-    std::vector<c2<double> *> v;
-    ~Owned() {
-      for (c2<double> *q : v) dfree(q);
-    }
-    c2<double> *add() {
-      v.reserve(v.size() + 1);
-      v.push_back(dalloc<c2<double>>(vec_elems(ctx().g)));
-      return v.back();
-    }
-  } own;
+  ScopedVecs own;
   c2<double> *r = own.add(), *ex = own.add(), *tmp = own.add();
   LinOp<double> L{f, mass[tail], eo, tmp};
   L.d2(r, x[tail]);

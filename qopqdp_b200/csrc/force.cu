@@ -174,6 +174,36 @@ __global__ void k_force_mid(double2 *midF, double2 *midN, const c2<T> *const *xs
   }
 }
 
+// F_mu(x) = TA(F_mu(x)): the projection the reference's ASVEC algorithm
+// applies to the whole accumulated force (lib/asqtad_force_asvec_p.c:403-408)
+template <typename T>
+__global__ void k_force_ta_self(c2<T> *F, Geom g) {
+  const i64 s = blockIdx.x * (i64)blockDim.x + threadIdx.x;
+  if (s >= 8 * g.Vh) return;           // [4 mu][2 parities][Vh]
+  const i64 Vh = g.Vh;
+  const i64 off = (s / Vh) * 9 * Vh + s % Vh;
+  double2 a[9];
+#pragma unroll
+  for (int e = 0; e < 9; e++) {
+    const c2<T> v = F[off + (i64)e * Vh];
+    a[e] = make_double2((double)v.x, (double)v.y);
+  }
+  double tri = 0;
+#pragma unroll
+  for (int k = 0; k < 3; k++) tri += a[4 * k].y;
+#pragma unroll
+  for (int r = 0; r < 3; r++)
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const double2 x = a[3 * r + c], y = a[3 * c + r];
+      double re = 0.5 * (x.x - y.x), im = 0.5 * (x.y + y.y);
+      if (r == c) im -= tri / 3.0;
+      c2<T> &f = F[off + (i64)(3 * r + c) * Vh];
+      f.x = (T)re;
+      f.y = (T)im;
+    }
+}
+
 // F_mu(x) += fac TA(U_mu(x) D_mu(x)^+), TA = traceless anti-Hermitian part
 template <typename T>
 __global__ void k_force_ta(c2<T> *F, const double2 *U, const double2 *D, double fac, Geom g) {
@@ -201,8 +231,10 @@ __global__ void k_force_ta(c2<T> *F, const double2 *U, const double2 *D, double 
 
 // adjoint of the U(3) projection W = V f(Q), Q = V^+V, f(q) = q^-1/2:
 // GV = GW f + V (B + B^+),  B = Z [(Z^+ V^+ GW Z) o Gamma] Z^+,
-// Gamma_ij = (f(w_i) - f(w_j)) / (w_i - w_j) = -1 / (s_i s_j (s_i + s_j)), s = sqrt(w)
-__global__ void k_reunit_adj(double2 *GV, const double2 *V, const double2 *GW, i64 n4) {
+// Gamma_ij = (f(w_i) - f(w_j)) / (w_i - w_j) = -1 / (s_i s_j (s_i + s_j)), s = sqrt(w).
+// Force filter (lib/hisq_reunit_utilities_p.c:463-481): where the smallest
+// eigenvalue of Q is below ff, the derivative is the one of V (Q + ff)^-1/2.
+__global__ void k_reunit_adj(double2 *GV, const double2 *V, const double2 *GW, i64 n4, double ff) {
   const i64 s = blockIdx.x * (i64)blockDim.x + threadIdx.x;   // over [4 mu][2 parities][Vh]
   if (s >= n4) return;
   const i64 Vh = n4 / 8, blk = s / Vh, i = s % Vh, off = blk * 9 * Vh + i;
@@ -210,6 +242,10 @@ __global__ void k_reunit_adj(double2 *GV, const double2 *V, const double2 *GW, i
   M3 Z;
   double w[3], sq[3];
   herm_eig3(mul_an(v, v), w, Z);
+  if (ff > 0 && fmin(w[0], fmin(w[1], w[2])) < ff) {
+#pragma unroll
+    for (int k = 0; k < 3; k++) w[k] += ff;
+  }
 #pragma unroll
   for (int k = 0; k < 3; k++) sq[k] = sqrt(w[k]);
   M3 f;
@@ -348,7 +384,15 @@ void asqtad_force(QOP_info_t *info, GaugeT<T> *G, GaugeT<T> *F, const QOP_asqtad
   force_mids<T>(mid, naik ? mid + F4 : nullptr, x, eps, nsrc, -1.0);   // scale -1 (fnmat_p.c:497)
   const double co[6] = {cf->one_link, cf->three_staple, cf->five_staple, cf->seven_staple, cf->lepage, cf->naik};
   const int nk = smear_adjoint(U, co, mid, naik ? mid + F4 : nullptr, D, w);
-  k_force_ta<T><<<grid_for(8 * Vh, 128), 128, 0, c.s>>>(F->d, U, D, -2.0, g);
+  // the reference's algorithm choice (lib/asqtad_force_p.c:22): FNMAT adds
+  // -2 TA(U D^+); ASVEC (fewer sources than fnmat_src_min) stores
+  // TA(force + C) with TA(C) = -TA(U D^+), half the FNMAT term
+  const bool asvec = nsrc < c.opt.force_fnmat_src_min;
+  if (asvec) {
+    k_force_ta_self<T><<<grid_for(8 * Vh, 128), 128, 0, c.s>>>(F->d, g);
+    QLAUNCH();
+  }
+  k_force_ta<T><<<grid_for(8 * Vh, 128), 128, 0, c.s>>>(F->d, U, D, asvec ? -1.0 : -2.0, g);
   QLAUNCH();
   sync();
   dfree(mid); dfree(D); dfree(w.S3); dfree(w.S5); dfree(w.G3); dfree(w.G5);
@@ -396,7 +440,7 @@ void hisq_force(QOP_info_t *info, HisqT<T> *h, GaugeT<T> *F, const QOP_hisq_coef
     k_field_axpby<<<grid_for(F4, 256), 256, 0, c.s>>>(GW, 1.0, T1, k == 0 ? 1.0 : cf->eps_naik[k], F4);
     QLAUNCH();
   }
-  k_reunit_adj<<<grid_for(8 * Vh, 128), 128, 0, c.s>>>(T1, V, GW, 8 * Vh);   // T1 = GV
+  k_reunit_adj<<<grid_for(8 * Vh, 128), 128, 0, c.s>>>(T1, V, GW, 8 * Vh, c.opt.hisq_force_filter);   // T1 = GV
   QLAUNCH();
   const double c7[6] = {cf->fat7_one_link, cf->fat7_three_staple, cf->fat7_five_staple, cf->fat7_seven_staple,
                         c.opt.use_fat7_lepage ? cf->fat7_lepage : 0.0, 0.0};

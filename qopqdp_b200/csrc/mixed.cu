@@ -1593,17 +1593,7 @@ void solve_multi_mixed(QOP_info_t *info, FlaT<double> *f, QOP_invert_arg_t *ia, 
       const double t = ra[j]->rsqmin * b2;
       stop[s] = stop[s] < 0 ? t : std::min(stop[s], t);
     }
-    struct Owned {   // the phase's vectors, freed on every way out (an allocation failure included)
-      std::vector<c2<double> *> v;
-      ~Owned() {
-        for (c2<double> *q : v) dfree(q);
-      }
-      c2<double> *add() {
-        v.reserve(v.size() + 1);
-        v.push_back(dalloc<c2<double>>(vec_elems(ctx().g)));
-        return v.back();
-      }
-    } own;
+    ScopedVecs own;   // the phase's vectors
     std::vector<c2<double> *> xv(ns);
     for (int s = 0; s < ns; s++) xv[s] = own.add();
     c2<double> *tmp = own.add();

@@ -122,6 +122,9 @@ struct Options {
   int mbar_tries = 1 << 22;      // bounded mbarrier waits of the TMA-staged int16 hops: polls before MIX_ERROR
   // QOP_asqtad_force_set_opts (lib/asqtad_force.c:3-41)
   int force_fnmat_src_min = 2, force_veclength = 4;
+  // QOP_hisq_force_set_opts (lib/hisq_force.c:4-52)
+  int hisq_fnmat_src_min = 1, hisq_veclength = 4;
+  double hisq_force_filter = 5e-5;
   // QOP_hisq_links_set_opts (lib/hisq_links.c:4-78)
   int want_deps = 0, want_aux = 1, reunit_allow_svd = 1, reunit_svd_only = 0;
   double reunit_svd_rel_error = 1e-8, reunit_svd_abs_error = 1e-8;

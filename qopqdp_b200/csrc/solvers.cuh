@@ -1,6 +1,7 @@
 // solvers.cuh -- Krylov solvers and inverter drivers (solvers.cu, mixed.cu).
 #pragma once
 #include "qopb.h"
+#include <vector>
 
 namespace qopb {
 
@@ -13,6 +14,23 @@ template <typename T> struct LinOp {
   c2<T> *tmp;   // full-volume scratch; its opposite-parity half holds D_oe in
   void d2(c2<T> *out, const c2<T> *in) { Dslash<T>::ddagd(f, mass, out, in, eo, tmp, false); }
   double d2n(c2<T> *out, const c2<T> *in) { return Dslash<T>::ddagd(f, mass, out, in, eo, tmp, true); }
+};
+
+// full-volume FP64 vectors owned by a scope: freed on every way out of it,
+// an allocation failure or a failed check included
+struct ScopedVecs {
+  std::vector<c2<double> *> v;
+  ScopedVecs() = default;
+  ScopedVecs(const ScopedVecs &) = delete;
+  ScopedVecs &operator=(const ScopedVecs &) = delete;
+  ~ScopedVecs() {
+    for (c2<double> *q : v) dfree(q);
+  }
+  c2<double> *add() {
+    v.reserve(v.size() + 1);
+    v.push_back(dalloc<c2<double>>(vec_elems(ctx().g)));
+    return v.back();
+  }
 };
 
 template <typename T>

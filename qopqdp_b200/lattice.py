@@ -36,12 +36,15 @@ def hisq_bench_coeffs():
     return c
 
 
-def hisq_coeff_vector(c):
-    """17-double layout used by the oracle's or_hisq_links."""
+def hisq_coeff_vector(c, force_filter=5e-5):
+    """18-double layout used by the oracle's HISQ routines: the 13
+    coefficients, then use_fat7_lepage, reunit_allow_svd, svd_rel_error,
+    svd_abs_error (QOP_hisq_links_set_opts defaults) and the force filter
+    (QOP_hisq_force_set_opts default, lib/hisq_force.c:4-9)."""
     return np.array([c.fat7_one_link, c.fat7_three_staple, c.fat7_five_staple, c.fat7_seven_staple, c.fat7_lepage,
                      c.asqtad_one_link, c.asqtad_three_staple, c.asqtad_five_staple, c.asqtad_seven_staple,
                      c.asqtad_lepage, c.asqtad_naik, c.difference_one_link, c.difference_naik,
-                     0.0, 1.0, 1e-8, 1e-8], dtype=np.float64)
+                     0.0, 1.0, 1e-8, 1e-8, force_filter], dtype=np.float64)
 
 
 def volume(L):

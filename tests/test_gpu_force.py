@@ -73,6 +73,8 @@ def test_force_errors_and_options():
     assert q.lib.QOP_asqtad_force_set_opts(arr, 2) == 0
     arr, _k = _c_opts({"veclength": 0})
     assert q.lib.QOP_asqtad_force_set_opts(arr, 1) != 0
+    arr, _k = _c_opts({"fnmat_src_min": 2, "veclength": 4})   # the defaults again
+    assert q.lib.QOP_asqtad_force_set_opts(arr, 2) == 0
     q.destroy_V(hv)
     q.destroy_F(F)
     q.destroy_G(G)
@@ -116,5 +118,41 @@ def test_hisq_force_matches_oracle(prec, tol):
         q.destroy_V(h)
     q.hisq_destroy_L(H)
     q.hisq_destroy_L(H2)
+    q.destroy_F(F)
+    q.destroy_G(G)
+
+
+@pytest.mark.parametrize("nsrc,fsm", [(1, 0), (1, 2), (3, 2), (3, 4)])
+def test_force_algorithm_choice_matches_oracle(nsrc, fsm):
+    """The reference picks ASVEC for nsrc < fnmat_src_min and FNMAT otherwise
+    (lib/asqtad_force_p.c:22-37); compiled from its sources, ASVEC stores
+    TA(force + C) with TA(C) half the FNMAT term.  The device follows the
+    option like the reference, checked against the oracle with the same
+    choice (accumulating into a force field that is not anti-Hermitian, so
+    the ASVEC projection of the incoming force shows)."""
+    from qopqdp_b200.qop import _c_opts
+    q = gpu_lattice(L, "D")
+    U = [np.asarray(u) for u in gauge(L, 0.3, 5)]
+    xs = [LT.gaussian_vector(L, 80 + i) for i in range(nsrc)]
+    eps = [0.7, -0.4, 0.25][:nsrc]
+    coef = (1.0, 0.1, 0.1, 0.1, 0.1, 0.1)
+    f0 = [np.random.default_rng(3).standard_normal((V, 3, 3, 2)) * 0.1 for _ in range(4)]
+    ref = O.Lattice(L).asqtad_force(coef, U, eps, xs, force=f0, fnmat_src_min=fsm)
+    arr, _k = _c_opts({"fnmat_src_min": fsm})
+    assert q.lib.QOP_asqtad_force_set_opts(arr, 1) == 0
+    try:
+        G = q.create_G(U)
+        F = q.create_F(f0)
+        hv = [q.create_V(x) for x in xs]
+        assert q.asqtad_force(G, F, coef, eps, hv).status == 0
+        got = q.extract_F(F, V)
+    finally:
+        arr, _k = _c_opts({"fnmat_src_min": 2})
+        assert q.lib.QOP_asqtad_force_set_opts(arr, 1) == 0
+    scale = max(np.max(np.abs(r)) for r in ref)
+    for g_, r in zip(got, ref):
+        assert np.max(np.abs(g_ - r)) <= 1e-12 * scale
+    for h in hv:
+        q.destroy_V(h)
     q.destroy_F(F)
     q.destroy_G(G)

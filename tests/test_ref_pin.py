@@ -278,3 +278,125 @@ def test_live_invert_multi_two_sources(eo):
             # them by up to tens of percent, not by orders of magnitude
             assert abs(a.final_rsq - b.final_rsq) <= 0.25 * b.final_rsq + 1e-22, (s, k, a.final_rsq, b.final_rsq)
             assert rel_norm_err(half(xo[s][k], L, eo), half(xr[s][k], L, eo)) < 1e-3, (s, k)
+
+
+# ---------------------------------------------------------------- forces
+
+@live
+@pytest.mark.parametrize("coeffs", [LT.ASQTAD_BENCH_COEFFS, (0.625, -0.0625, 0.0104, -0.00130, -0.0625, -0.0417)])
+@pytest.mark.parametrize("nsrc,fsm", [(1, 2), (1, 0), (3, 2), (3, 4)])
+def test_live_asqtad_force(coeffs, nsrc, fsm):
+    """QOP_D3_asqtad_force_multi_qdp with the reference's algorithm choice
+    (ASVEC for nsrc < fnmat_src_min, FNMAT otherwise), accumulated into a
+    force field that is not anti-Hermitian: the oracle agrees to rounding in
+    all four cases (ASVEC stores TA(force + C), its contribution half of
+    FNMAT's)."""
+    L = (4, 4, 4, 6)
+    V = int(np.prod(L))
+    G = O.Lattice(L).rephase_G(_gauge(L))
+    rng = np.random.default_rng(9)
+    xs = [rng.standard_normal((V, 6)) for _ in range(nsrc)]
+    eps = [0.3, -0.2, 0.5][:nsrc]
+    f0 = [rng.standard_normal((V, 3, 3, 2)) * 0.1 for _ in range(4)]
+    fo = O.Lattice(L).asqtad_force(coeffs, G, eps, xs, force=f0, fnmat_src_min=fsm)
+    fr = R.asqtad_force(L, coeffs, G, eps, xs, force=f0, fnmat_src_min=fsm)
+    scale = max(float(np.abs(a).max()) for a in fo)
+    assert maxdiff(fo, fr) < 1e-13 * scale
+
+
+@live
+def test_live_asqtad_deriv_differs_only_by_unitary_directions():
+    """The reference's derivative field (QOP_D3_asqtad_deriv, its staple
+    recursion writes U^+ where the general derivative has U^-1) and the
+    oracle's (the derivative for general complex links, pinned by finite
+    differences) differ by U H with H Hermitian: nothing of it survives the
+    force's projection TA(U D^+)."""
+    L = (4, 4, 4, 6)
+    V = int(np.prod(L))
+    G = O.Lattice(L).rephase_G(_gauge(L, eps=0.5))
+    rng = np.random.default_rng(2)
+    mF = [rng.standard_normal((V, 3, 3, 2)) for _ in range(4)]
+    mN = [rng.standard_normal((V, 3, 3, 2)) for _ in range(4)]
+    cz = lambda a: a[..., 0] + 1j * a[..., 1]
+    do = O.Lattice(L).asqtad_deriv(LT.ASQTAD_BENCH_COEFFS, G, mF, mN)
+    dr = R.asqtad_deriv(L, LT.ASQTAD_BENCH_COEFFS, G, mF, mN)
+    assert maxdiff(do, dr) > 1e-3                       # the representations do differ
+    for mu in range(4):
+        x = np.einsum("sij,skj->sik", cz(G[mu]), np.conj(cz(dr[mu]) - cz(do[mu])))   # U (D_ref - D_oracle)^+
+        assert np.abs(x - np.conj(np.swapaxes(x, 1, 2))).max() < 1e-12
+
+
+@live
+@pytest.mark.parametrize("eps_g,ff", [(0.2, 5e-5), (0.5, 0.0)])
+@pytest.mark.parametrize("eps_naik", [(0.0,), (0.0, 0.1)])
+def test_live_hisq_force(eps_g, ff, eps_naik):
+    """QOP_D3_hisq_force_multi_qdp (U(3) projection, the RATIONAL force
+    branch): the oracle agrees to rounding where the force filter changes
+    nothing -- a gauge field whose fat7 links all have V^+V eigenvalues
+    above the 5e-5 default, or the filter off (force_filter 0) on a rough
+    one."""
+    L = (4, 4, 4, 6)
+    V = int(np.prod(L))
+    G = O.Lattice(L).rephase_G(_gauge(L, eps=eps_g))
+    rng = np.random.default_rng(9)
+    xs = [rng.standard_normal((V, 6)) for _ in range(3)]
+    res = [0.3, -0.2, 0.5]
+    n_orders = [3] if len(eps_naik) == 1 else [2, 1]
+    hc = LT.hisq_coeff_vector(LT.hisq_bench_coeffs(), force_filter=ff)
+    hc[11], hc[12] = 0.3, -0.05
+    fo = O.Lattice(L).hisq_force(hc, G, list(eps_naik), np.array(res), xs, n_orders)
+    fr = R.hisq_force(L, hc, G, list(eps_naik), res, xs, n_orders)
+    scale = max(float(np.abs(a).max()) for a in fo)
+    assert maxdiff(fo, fr) < 1e-9 * scale, (maxdiff(fo, fr), scale)
+
+
+@live
+def test_live_force_filter_per_link():
+    """At a filtered link (V^+V eigenvalue below force_filter) the
+    reference's derivative tensors are those of V (V^+V + ff)^-1/2, and its
+    chain rule equals the oracle's adjoint with the filter; elsewhere the
+    filter does nothing.  (On whole forces the filtered results still differ
+    near such links: the W-level derivative the filtered adjoint receives
+    differs between the reference and the oracle by W H terms, H Hermitian,
+    which the unfiltered projection's adjoint removes and the filtered one
+    does not; see test_live_asqtad_deriv_differs_only_by_unitary_directions.)"""
+    L = (4, 4, 4, 6)
+    G = O.Lattice(L).rephase_G(_gauge(L, eps=0.5))
+    hc = LT.hisq_coeff_vector(LT.hisq_bench_coeffs())
+    Vl, _ = O.Lattice(L).make_imp_links([hc[0], hc[1], hc[2], hc[3], 0.0, 0.0], G, naik=False)
+    cz = lambda a: a[..., 0] + 1j * a[..., 1]
+    Vs = np.concatenate([cz(v) for v in Vl])
+    wmin = np.linalg.eigvalsh(np.einsum("sji,sjk->sik", Vs.conj(), Vs)).min(axis=1)
+    bad = int(np.argmin(wmin))
+    assert wmin[bad] < 5e-5 <= np.sort(wmin)[1]     # one filtered link on this field
+
+    def W(X, e):
+        w, Z = np.linalg.eigh(X.conj().T @ X + e * np.eye(3))
+        return X @ (Z @ np.diag(w ** -0.5) @ Z.conj().T)
+
+    def adj(X, GW, e):
+        w, Z = np.linalg.eigh(X.conj().T @ X)
+        if e > 0 and w.min() < e:
+            w = w + e
+        s = np.sqrt(w)
+        At = (Z.conj().T @ (X.conj().T @ GW) @ Z) * (-1.0 / (s[:, None] * s[None, :] * (s[:, None] + s[None, :])))
+        B = Z @ At @ Z.conj().T
+        return GW @ (Z @ np.diag(1 / s) @ Z.conj().T) + X @ (B + B.conj().T)
+
+    rng = np.random.default_rng(4)
+    for k in (bad, 10):
+        X = Vs[k]
+        dw, dwd, ff = R.u3_der(L, X)
+        assert ff == (k == bad)
+        h = 1e-7
+        for m in range(3):
+            for n in range(3):
+                E = np.zeros((3, 3), complex)
+                E[m, n] = 1
+                fd = 0.5 * ((W(X + h * E, 5e-5 if ff else 0) - W(X - h * E, 5e-5 if ff else 0))
+                            - 1j * (W(X + 1j * h * E, 5e-5 if ff else 0) - W(X - 1j * h * E, 5e-5 if ff else 0))) / (2 * h)
+                assert np.abs(dw[:, :, m, n] - fd).max() < 1e-5 * max(1.0, np.abs(fd).max())
+        F = rng.standard_normal((3, 3)) + 1j * rng.standard_normal((3, 3))
+        new = np.einsum("ijmn,ji->nm", dw, F) + np.einsum("ijmn,ji->nm", dwd, F.conj().T)
+        mine = adj(X, F.conj().T, 5e-5).conj().T
+        assert np.abs(new - mine).max() < 1e-8 * np.abs(new).max()
