@@ -718,7 +718,8 @@ def run_small(a):
     """Plain asqtad in single precision (QOP_F3_*) on 8^4 (eps 0.3), m = 0.1:
     the nine (eo_out, eo_in) Dslash cases and the eo-preconditioned CG to
     |r|/|b| <= 1e-5 (rsqmin 1e-10), timed on the GPU (CUDA events, mean over
-    --steps repetitions after --warmup) and with the oracle on the host;
+    --steps repetitions after --warmup) and with the reference's own F3 code
+    (oracle/_ref; the oracle where it was not built) on the host;
     each Dslash checked against the oracle (F3 tolerance 2e-6 per site).
     The whole problem is cache-resident: not an HBM measurement."""
     import torch
@@ -782,23 +783,39 @@ def run_small(a):
         if k >= a.warmup:
             cg_ms.append(e0.elapsed_time(e1))
             iters = ra.final_iter
-    # the oracle on the host: one Dslash (EVENODD) and the same CG
-    t0 = time.perf_counter()
-    for _ in range(20):
-        fo.dslash(m32, src.astype(np.float64), 2, 2)
-    cpu_dslash_us = (time.perf_counter() - t0) / 20 * 1e6
-    t0 = time.perf_counter()
-    ora = O.ResidArg(1e-10, 0, 0, 0, 0, 0)
-    fo.invert(m32, src.astype(np.float64), O.InvertArg(1e9, 2000, 2000, 5, 0), ora)
-    cpu_cg_ms = (time.perf_counter() - t0) * 1e3
+    # on the host: the reference's own F3 build (oracle/_ref) where it was
+    # built, else the oracle: one Dslash (EVENODD) and the same CG
+    import refqop as R
+    kind = "reference" if R.available() else "port"
+    threads = os.cpu_count() or 1
+    if kind == "reference":
+        cores = R.set_threads(L, threads)
+        cpu = R.RefFla(L, [x.astype(np.float64) for x in fat], [x.astype(np.float64) for x in lng], R.F3)
+    else:
+        O.set_threads(threads)
+        cores = O.get_threads()
+        cpu = fo
+    src64 = src.astype(np.float64).reshape(V, 6)
+    with _StdoutToStderr():
+        cpu.dslash(m32, src64, 2, 2)
+        t0 = time.perf_counter()
+        for _ in range(20):
+            cpu.dslash(m32, src64, 2, 2)
+        cpu_dslash_us = (time.perf_counter() - t0) / 20 * 1e6
+        t0 = time.perf_counter()
+        ora = O.ResidArg(1e-10, 0, 0, 0, 0, 0)
+        cpu.invert(m32, src64, O.InvertArg(1e9, 2000, 2000, 5, 0), ora)
+        cpu_cg_ms = (time.perf_counter() - t0) * 1e3
     line = {"metric": "F3 asqtad 8^4: Dslash us and eo CG ms", "value": float(np.mean(cg_ms)), "unit": "ms per CG solve",
             "n_gpus": 1, "steps": a.steps, "warmup": a.warmup, "ms_per_step": float(np.mean(cg_ms)),
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "small", "lattice": L, "mass": mass, "rsqmin": 1e-10, "eps": 0.3,
                        "note": "cache-resident, not an HBM measurement"},
-            "dslash": cases, "dslash_max_site_rel_err": worst, "cg_iters": iters, "oracle_cg_iters": ora.final_iter,
-            "cpu_baseline": {"dslash_us": cpu_dslash_us, "cg_ms": cpu_cg_ms, "kind": "port",
-                             "cores": O.get_threads()}}
+            "dslash": cases, "dslash_max_site_rel_err": worst, "cg_iters": iters, "cpu_cg_iters": ora.final_iter,
+            "cpu_baseline": {"dslash_us": cpu_dslash_us, "cg_ms": cpu_cg_ms, "kind": kind, "cores": cores,
+                             "sample": "one EVENODD Dslash (mean of 20) and the same eo CG, %s" %
+                                       ("the reference's QOP_F3 build (oracle/_ref)" if kind == "reference"
+                                        else "the oracle (FP64)")}}
     print(json.dumps(line), flush=True)
     q.destroy_V(hin)
     q.destroy_V(hout)
@@ -853,18 +870,34 @@ def run_force(a):
         e1 = ev()
         e1.synchronize()
         out[name] = {"ms": e0.elapsed_time(e1) / a.steps}
-    # the oracle on a 12^4 lattice, scaled by volume
+    # the reference's own force code (oracle/_ref) on a 12^4 lattice, scaled
+    # by volume; the oracle's restatement where the reference was not built
+    import refqop as R
     Lc = (12, 12, 12, 12)
     Vc = int(np.prod(Lc))
     lat = O.Lattice(Lc)
     Uc = lat.rephase_G(LT.random_gauge(Lc, a.eps, a.seed, device="cpu"), LT.BENCH_R0, LT.BENCH_BC, LT.BENCH_SIGNMASK)
-    xs = [LT.gaussian_vector(Lc, a.seed + i) for i in range(nsrc)]
-    t0 = time.perf_counter()
-    lat.hisq_force(LT.hisq_coeff_vector(hc), Uc, [0.0], res, xs, [nsrc])
-    out["hisq"]["cpu_ms"] = (time.perf_counter() - t0) * 1e3 * V / Vc
-    t0 = time.perf_counter()
-    lat.asqtad_force(acoef, Uc, res, xs)
-    out["asqtad"]["cpu_ms"] = (time.perf_counter() - t0) * 1e3 * V / Vc
+    xs = [LT.gaussian_vector(Lc, a.seed + i).reshape(Vc, 6) for i in range(nsrc)]
+    kind = "reference" if R.available() else "port"
+    threads = os.cpu_count() or 1
+    if kind == "reference":
+        cores = R.set_threads(Lc, threads)
+        hisq_cpu = lambda: R.hisq_force(Lc, LT.hisq_coeff_vector(hc), Uc, [0.0], res, xs, [nsrc])
+        asq_cpu = lambda: R.asqtad_force(Lc, acoef, Uc, res, xs)
+        what = "QOP_D3_hisq_force_multi_qdp / QOP_D3_asqtad_force_multi_qdp (the reference's own code, oracle/_ref)"
+    else:
+        O.set_threads(threads)
+        cores = O.get_threads()
+        hisq_cpu = lambda: lat.hisq_force(LT.hisq_coeff_vector(hc), Uc, [0.0], res, xs, [nsrc])
+        asq_cpu = lambda: lat.asqtad_force(acoef, Uc, res, xs)
+        what = "the oracle's restatement"
+    with _StdoutToStderr():
+        t0 = time.perf_counter()
+        hisq_cpu()
+        out["hisq"]["cpu_ms"] = (time.perf_counter() - t0) * 1e3 * V / Vc
+        t0 = time.perf_counter()
+        asq_cpu()
+        out["asqtad"]["cpu_ms"] = (time.perf_counter() - t0) * 1e3 * V / Vc
     for k in out:
         out[k]["speedup_vs_cpu"] = out[k]["cpu_ms"] / out[k]["ms"]
     line = {"metric": "fermion force ms per call (8 sources, FP64)", "value": out["hisq"]["ms"], "unit": "ms",
@@ -872,8 +905,9 @@ def run_force(a):
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": "force", "lattice": L, "sources": nsrc, "eps": a.eps},
             "forces": out,
-            "cpu_baseline": {"kind": "port", "cores": O.get_threads(),
-                             "sample": "one oracle force call on 12^4, scaled by the volume ratio"}}
+            "cpu_baseline": {"kind": kind, "cores": cores,
+                             "sample": "one call of %s on 12^4 with %d host threads, scaled by the volume ratio"
+                                       % (what, cores)}}
     print(json.dumps(line), flush=True)
     for h in hv:
         q.destroy_V(h)
