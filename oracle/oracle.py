@@ -58,7 +58,7 @@ def lib():
         l.or_hisq_links.argtypes = [vp, DP, C.POINTER(DP), C.POINTER(DP), C.POINTER(DP), C.POINTER(DP)]
         l.or_hisq_links.restype = C.c_int
         l.or_fla_create.argtypes = [vp, C.POINTER(DP), C.POINTER(DP)]
-        l.or_asqtad_deriv.argtypes = [vp, DP, C.POINTER(DP), C.POINTER(DP), C.POINTER(DP), C.POINTER(DP)]
+        l.or_asqtad_deriv.argtypes = [vp, DP, C.POINTER(DP), C.POINTER(DP), C.POINTER(DP), C.POINTER(DP), C.c_int]
         l.or_asqtad_force.argtypes = [vp, DP, C.POINTER(DP), C.POINTER(DP), DP, C.POINTER(DP), C.c_int, C.c_int]
         l.or_hisq_deriv.argtypes = [vp, DP, C.POINTER(DP), C.c_int, DP, C.POINTER(DP), C.POINTER(DP), C.POINTER(DP)]
         l.or_hisq_force.argtypes = [vp, DP, C.POINTER(DP), C.c_int, DP, C.POINTER(DP), DP, C.POINTER(DP),
@@ -124,14 +124,17 @@ class Lattice:
         lib().or_make_imp_links(self.h, _p(c), _p4(gauge), _p4(gauge), _p4(fat), _p4(lng) if naik else None)
         return fat, lng
 
-    def asqtad_deriv(self, coeffs, gauge, midF, midN=None):
-        """deriv_mu = dE/dU_mu for E = Re sum tr[midF^+ fat + midN^+ long]."""
+    def asqtad_deriv(self, coeffs, gauge, midF, midN=None, lepage_rep=False):
+        """deriv_mu = dE/dU_mu for E = Re sum tr[midF^+ fat + midN^+ long];
+        lepage_rep adds the reference's Lepage term of the form U H (H
+        Hermitian), giving its QOP_asqtad_deriv field."""
         gauge = [f64(a) for a in gauge]
         midF = [f64(a) for a in midF]
         midN = [f64(a) for a in midN] if midN is not None else None
         der = [np.zeros_like(gauge[0]) for _ in range(4)]
         c = np.array(coeffs, dtype=np.float64)
-        lib().or_asqtad_deriv(self.h, _p(c), _p4(gauge), _p4(midF), _p4(midN) if midN is not None else None, _p4(der))
+        lib().or_asqtad_deriv(self.h, _p(c), _p4(gauge), _p4(midF), _p4(midN) if midN is not None else None, _p4(der),
+                              int(bool(lepage_rep)))
         return der
 
     def asqtad_force(self, coeffs, gauge, eps, xs, force=None, fnmat_src_min=2):

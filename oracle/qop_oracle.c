@@ -1225,7 +1225,7 @@ static void adj_staple_link(const or_lat *g, dc *GU, const dc *G, const dc *in, 
 }
 
 void or_asqtad_deriv(const or_lat *g, const double coef[6], double *Ur[4], double *midFr[4], double *midNr[4],
-                     double *derivr[4]) {
+                     double *derivr[4], int lepage_rep) {
   dc *U[4], *M[4], *D[4];
   for (int i = 0; i < 4; i++) { U[i] = (dc *)Ur[i]; M[i] = (dc *)midFr[i]; D[i] = (dc *)derivr[i]; }
   const double c1 = coef[0] - 6 * coef[4], c3 = coef[1], c5 = coef[2], c7 = coef[3], cL = coef[4];
@@ -1281,6 +1281,46 @@ void or_asqtad_deriv(const or_lat *g, const double coef[6], double *Ur[4], doubl
       }
     }
   }
+  /* lepage_rep: with a Lepage term the reference's derivative field carries
+     one more term, of the form U_mu H with H Hermitian
+     (lib/asqtad_force_fnmat_p.c:316-340):
+     D_mu(x) -= cL [F_mu(x) U_mu(x) - U_mu(x) F_mu(x+mu)],
+     F_mu = sum_{nu != mu} (A_nu + A_nu^+),
+     A_nu(x) = M_nu(x) U_nu(x)^+ - M_nu(x-nu)^+ U_nu(x-nu).
+     The force projection TA(U D^+) removes it; the filtered U(3) adjoint of
+     the HISQ force, which receives this field at the W level, does not. */
+  if (lepage_rep && cL != 0) {
+    dc *Hn = calloc(4 * 9 * (size_t)g->V, sizeof(dc));
+    for (int nu = 0; nu < 4; nu++)
+#pragma omp parallel for
+      for (long z = 0; z < g->V; z++) {
+        dc a[9], b[9];
+        long zm = nbr(g, z, nu, -1);
+        m_mul_na(a, M[nu] + 9 * z, U[nu] + 9 * z);
+        m_mul_an(b, M[nu] + 9 * zm, U[nu] + 9 * zm);
+        for (int i = 0; i < 3; i++)
+          for (int j = 0; j < 3; j++) {
+            dc aij = a[3 * i + j] - b[3 * i + j], aji = a[3 * j + i] - b[3 * j + i];
+            Hn[9 * (nu * g->V + z) + 3 * i + j] = aij + conj(aji);
+          }
+      }
+    for (int mu = 0; mu < 4; mu++)
+#pragma omp parallel for
+      for (long z = 0; z < g->V; z++) {
+        dc F0[9] = {0}, F1[9] = {0}, r[9], t[9];
+        long zp = nbr(g, z, mu, 1);
+        for (int nu = 0; nu < 4; nu++) {
+          if (nu == mu) continue;
+          m_acc(F0, Hn + 9 * (nu * g->V + z), 1.0);
+          m_acc(F1, Hn + 9 * (nu * g->V + zp), 1.0);
+        }
+        m_mul(r, F0, U[mu] + 9 * z);
+        m_mul(t, U[mu] + 9 * z, F1);
+        m_acc(r, t, -1.0);
+        m_acc(D[mu] + 9 * z, r, -cL);
+      }
+    free(Hn);
+  }
   free(S3); free(S5); free(G3); free(G5); free(junk);
 }
 
@@ -1307,7 +1347,7 @@ void or_asqtad_force(const or_lat *g, const double coef[6], double *Ur[4], doubl
       }
     }
   }
-  or_asqtad_deriv(g, coef, Ur, mid, coef[5] != 0 ? mid + 4 : NULL, der);
+  or_asqtad_deriv(g, coef, Ur, mid, coef[5] != 0 ? mid + 4 : NULL, der, 0);
   /* FNMAT (asqtad_force_fnmat_p.c:530-540): force += -2 TA(U deriv^+).
      ASVEC (asqtad_force_asvec_p.c:180-184, 403-408; chosen by
      asqtad_force_p.c:22 when nsrc < fnmat_src_min): the outer products are
@@ -1403,7 +1443,7 @@ void or_hisq_deriv(const or_lat *g, const double h[18], double *U[4], int n_naik
   const double ca[6] = {h[5], h[6], h[7], h[8], h[9], h[10]}, cd[6] = {h[11], 0, 0, 0, 0, h[12]};
   for (int k = 0; k < n_naiks; k++) {
     for (int i = 0; i < 4; i++) memset(tmp[i], 0, n * sizeof(double));
-    or_asqtad_deriv(g, k == 0 ? ca : cd, Wl, midF + 4 * k, midN + 4 * k, tmp);
+    or_asqtad_deriv(g, k == 0 ? ca : cd, Wl, midF + 4 * k, midN + 4 * k, tmp, 1);
     const double c = k == 0 ? 1.0 : eps_naik[k];
     for (int i = 0; i < 4; i++)
       for (size_t e = 0; e < n; e++) GW[i][e] += c * tmp[i][e];
@@ -1412,7 +1452,7 @@ void or_hisq_deriv(const or_lat *g, const double h[18], double *U[4], int n_naik
 #pragma omp parallel for
     for (long s = 0; s < g->V; s++)
       reunit_adj((const dc *)Vl[i] + 9 * s, (const dc *)GW[i] + 9 * s, (dc *)GV[i] + 9 * s, h[17]);
-  or_asqtad_deriv(g, c7, U, GV, NULL, deriv);
+  or_asqtad_deriv(g, c7, U, GV, NULL, deriv, 0);
   for (int i = 0; i < 4; i++) { free(Vl[i]); free(Wl[i]); free(GW[i]); free(tmp[i]); free(GV[i]); }
 }
 

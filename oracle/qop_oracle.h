@@ -97,8 +97,11 @@ void or_solve_multi(or_fla *f, or_invert_arg *ia, or_resid_arg *ra[],
    (the FNMAT algorithm); asvec != 0 gives the reference's ASVEC result,
    force_mu = TA(force_mu) - TA(U_mu deriv_mu^+) (asqtad_force_p.c:22 picks it
    for nsrc < fnmat_src_min, 2 by default). */
+/* lepage_rep != 0 adds the reference's extra Lepage term, of the form
+   U_mu H with H Hermitian (asqtad_force_fnmat_p.c:316-340), giving the
+   reference's own derivative field; 0 gives dE/dU for general complex U. */
 void or_asqtad_deriv(const or_lat *g, const double coef[6], double *U[4],
-                     double *midF[4], double *midN[4], double *deriv[4]);
+                     double *midF[4], double *midN[4], double *deriv[4], int lepage_rep);
 void or_asqtad_force(const or_lat *g, const double coef[6], double *U[4],
                      double *force[4], const double *eps, double *x[], int nsrc, int asvec);
 
@@ -108,7 +111,10 @@ void or_asqtad_force(const or_lat *g, const double coef[6], double *U[4],
    (k = 0: asqtad coefficients, c_0 = 1; k >= 1: difference coefficients,
    c_k = eps_naik[k]); mids are n_naiks x 4 fields.  The force builds
    MF_k = s(x) sum_i res_i x_i(x) x_i(x+mu)^+ over group k's sources (group 0:
-   all sources; s = +1 even, -1 odd) and adds TA(U_mu (2 deriv_mu)^+). */
+   all sources; s = +1 even, -1 odd) and adds TA(U_mu (2 deriv_mu)^+).  The
+   W-level derivative is the reference's field (or_asqtad_deriv with
+   lepage_rep): the filtered U(3) adjoint (hcoef[17] > 0) does not remove its
+   Lepage term. */
 void or_hisq_deriv(const or_lat *g, const double hcoef[18], double *U[4], int n_naiks, const double *eps_naik,
                    double **midF, double **midN, double *deriv[4]);
 void or_hisq_force(const or_lat *g, const double hcoef[18], double *U[4], int n_naiks, const double *eps_naik,

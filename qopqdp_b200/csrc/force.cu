@@ -123,6 +123,57 @@ __global__ void k_adj_naik(double2 *D, const double2 *N, const double2 *U, int m
   accf(D, g, p, i, r, c);
 }
 
+// The reference's derivative field carries, with a Lepage term, one more
+// term of the form U_mu H, H Hermitian (lib/asqtad_force_fnmat_p.c:316-340):
+//   D_mu(x) -= cL [F_mu(x) U_mu(x) - U_mu(x) F_mu(x+mu)],
+//   F_mu = sum_{nu != mu} H_nu,  H_nu = A_nu + A_nu^+,
+//   A_nu(x) = M_nu(x) U_nu(x)^+ - M_nu(x-nu)^+ U_nu(x-nu).
+// The force projection TA(U D^+) removes it; the filtered U(3) adjoint of
+// the HISQ force, which receives this field at the W level, does not.
+// k_lep_h: H = H_nu for one nu
+__global__ void k_lep_h(double2 *H, const double2 *M, const double2 *Unu, int nu, Geom g) {
+  const i64 s = blockIdx.x * (i64)blockDim.x + threadIdx.x;
+  if (s >= 2 * g.Vh) return;
+  int p, i, z[4], pm, im;
+  site_of(g, s, p, i, z);
+  nbr_pi(g, z, nu, -1, pm, im);
+  const M3 a = mul_na(ldf(M, g, p, i), ldf(Unu, g, p, i));
+  const M3 b = mul_an(ldf(M, g, pm, im), ldf(Unu, g, pm, im));
+  M3 h;
+#pragma unroll
+  for (int r = 0; r < 3; r++)
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const double2 x = a.e[3 * r + c], y = b.e[3 * r + c], xt = a.e[3 * c + r], yt = b.e[3 * c + r];
+      h.e[3 * r + c] = make_double2(x.x - y.x + xt.x - yt.x, x.y - y.y - xt.y + yt.y);
+    }
+  st3(H + (i64)p * 9 * g.Vh + i, g.Vh, h);
+}
+
+// k_lep_fix: D_mu -= cL [F U_mu - U_mu F(x+mu)] with F the sum of the three
+// H_nu (nu != mu) given in h0..h2
+__global__ void k_lep_fix(double2 *D, const double2 *Umu, const double2 *h0, const double2 *h1, const double2 *h2,
+                          int mu, double cL, Geom g) {
+  const i64 s = blockIdx.x * (i64)blockDim.x + threadIdx.x;
+  if (s >= 2 * g.Vh) return;
+  int p, i, z[4], pp, ip;
+  site_of(g, s, p, i, z);
+  nbr_pi(g, z, mu, 1, pp, ip);
+  M3 f0 = ldf(h0, g, p, i), f1 = ldf(h0, g, pp, ip);
+  const M3 a0 = ldf(h1, g, p, i), a1 = ldf(h1, g, pp, ip), b0 = ldf(h2, g, p, i), b1 = ldf(h2, g, pp, ip);
+#pragma unroll
+  for (int e = 0; e < 9; e++) {
+    f0.e[e] = make_double2(f0.e[e].x + a0.e[e].x + b0.e[e].x, f0.e[e].y + a0.e[e].y + b0.e[e].y);
+    f1.e[e] = make_double2(f1.e[e].x + a1.e[e].x + b1.e[e].x, f1.e[e].y + a1.e[e].y + b1.e[e].y);
+  }
+  const M3 U = ldf(Umu, g, p, i);
+  M3 r = mul(f0, U);
+  const M3 t = mul(U, f1);
+#pragma unroll
+  for (int e = 0; e < 9; e++) r.e[e] = make_double2(r.e[e].x - t.e[e].x, r.e[e].y - t.e[e].y);
+  accf(D, g, p, i, r, -cL);
+}
+
 __global__ void k_field_axpby(double2 *d, double a, const double2 *s, double b, i64 n) {   // d = a d + b s
   const i64 k = blockIdx.x * (i64)blockDim.x + threadIdx.x;
   if (k >= n) return;
@@ -291,9 +342,11 @@ struct SweepWork {
 
 // D += derivative of Re sum tr[midF^+ fat + midN^+ long] with (fat, long) =
 // make_imp_links(c, U): the reverse sweep over its staple sums and the Naik
-// products; midN may be null.  Returns the number of kernels launched.
+// products; midN may be null.  lepage_rep adds the reference's Lepage term
+// of the form U H (k_lep_h), for a derivative that feeds something other
+// than the force projection.  Returns the number of kernels launched.
 int smear_adjoint(const double2 *U, const double c[6], const double2 *mid, const double2 *midN, double2 *D,
-                  const SweepWork &w) {
+                  const SweepWork &w, bool lepage_rep = false) {
   Context &cx = ctx();
   const Geom &g = cx.g;
   const i64 F1 = 18 * g.Vh;
@@ -346,6 +399,17 @@ int smear_adjoint(const double2 *U, const double c[6], const double2 *mid, const
       k_adj_naik<<<grid2, 128, 0, cx.s>>>(Df(mu), midN + mu * F1, Uf(mu), mu, c[5], g);
       nk++;
     }
+  if (lepage_rep && cL != 0) {
+    double2 *H[4] = {w.S3, w.S5, w.G3, w.G5};   // free once the sweep is done
+    for (int nu = 0; nu < 4; nu++) k_lep_h<<<grid2, 128, 0, cx.s>>>(H[nu], mid + nu * F1, Uf(nu), nu, g);
+    for (int mu = 0; mu < 4; mu++) {
+      const double2 *o[3];
+      for (int nu = 0, k = 0; nu < 4; nu++)
+        if (nu != mu) o[k++] = H[nu];
+      k_lep_fix<<<grid2, 128, 0, cx.s>>>(Df(mu), Uf(mu), o[0], o[1], o[2], mu, cL, g);
+    }
+    nk += 8;
+  }
   QLAUNCHN(nk);
   return nk;
 }
@@ -436,7 +500,7 @@ void hisq_force(QOP_info_t *info, HisqT<T> *h, GaugeT<T> *F, const QOP_hisq_coef
     if (count == 0) continue;
     force_mids<T>(mid, mid + F4, x + first, res + first, count, 1.0);
     dzero(T1, sizeof(double2) * F4);
-    nk += smear_adjoint(W, k == 0 ? ca : cd, mid, mid + F4, T1, w);
+    nk += smear_adjoint(W, k == 0 ? ca : cd, mid, mid + F4, T1, w, true);
     k_field_axpby<<<grid_for(F4, 256), 256, 0, c.s>>>(GW, 1.0, T1, k == 0 ? 1.0 : cf->eps_naik[k], F4);
     QLAUNCH();
   }

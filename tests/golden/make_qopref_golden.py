@@ -18,6 +18,16 @@ Outputs (reference D3 build):
   hisq_*     HISQ links (examples/hisq_invert_bench.c coefficients, U(3),
              analytic projection) of QOP_hisq_create_L_from_G; Dslash
              EVENODD<-EVENODD at mass 0.05
+  force_*    fermion forces on a rough field, random_gauge(L, 0.5, seed=2)
+             rephased as above (two fat7 links with a V^+V eigenvalue below
+             the 5e-5 force filter), sources gaussian_vector(L, 51 + i):
+             force_asq_asvec  QOP_asqtad_force_multi, one source, eps 0.3
+                              (ASVEC: below fnmat_src_min = 2)
+             force_asq_fnmat  the same with three sources, eps .3 -.2 .5
+             force_hisq       QOP_hisq_force_multi, three sources, residues
+                              .3 -.2 .5, Naik groups [2, 1] with eps_naik
+                              (0, 0.1), difference one-link .3 / Naik -.05,
+                              default force filter
   *_ck       link checksums: sum of squares and sum of w * links with the
              fixed weights w = cos(0.37 k) over the flattened array
 Run from the repository root: python tests/golden/make_qopref_golden.py
@@ -75,6 +85,17 @@ def main():
     out["hisq_fat_ck"], out["hisq_long_ck"], out["hisq_W_ck"] = checksum(hfat), checksum(hlng), checksum(W)
     hfla = R.RefFla(L, hfat, hlng, R.D3)
     out["hisq_dslash_eoeo"] = hfla.dslash(0.05, src, 2, 2)
+
+    Ur = LT.random_gauge(L, 0.5, 2)
+    Gr = R.rephase_G(L, Ur, LT.BENCH_R0, LT.BENCH_BC, LT.BENCH_SIGNMASK)
+    out["force_gauge_ck"] = checksum(Ur)
+    xs = [LT.gaussian_vector(L, 51 + i).reshape(V, 6) for i in range(3)]
+    eps = [0.3, -0.2, 0.5]
+    out["force_asq_asvec"] = np.stack(R.asqtad_force(L, LT.ASQTAD_BENCH_COEFFS, Gr, eps[:1], xs[:1]))
+    out["force_asq_fnmat"] = np.stack(R.asqtad_force(L, LT.ASQTAD_BENCH_COEFFS, Gr, eps, xs))
+    hf = LT.hisq_coeff_vector(LT.hisq_bench_coeffs())
+    hf[11], hf[12] = 0.3, -0.05
+    out["force_hisq"] = np.stack(R.hisq_force(L, hf, Gr, [0.0, 0.1], eps, xs, [2, 1]))
     np.savez_compressed(OUT, **out)
     print("wrote", OUT, os.path.getsize(OUT), "bytes")
 

@@ -120,3 +120,45 @@ def test_device_solves_match_reference(gold, sloppy):
     q.destroy_V(hout)
     q.destroy_L(fla)
     q.destroy_G(hG)
+
+
+def test_device_forces_match_reference(gold):
+    """Fermion forces on the device (FP64) against the reference's on a rough
+    field with two filtered fat7 links: the asqtad force by ASVEC (one
+    source) and FNMAT (three), and the HISQ force with two Naik groups and
+    the default force filter, whose W-level derivative carries the
+    reference's Lepage term into the filtered U(3) adjoint."""
+    d = gold
+    q = gpu_lattice(L, "D")
+    Ur = LT.random_gauge(L, 0.5, 2)
+    assert close_ck(checksum(Ur), d["force_gauge_ck"], 1e-12), "gauge generator changed"
+    hG = q.create_G([np.asarray(u, dtype=np.float64) for u in Ur])
+    q.rephase_G(hG, LT.BENCH_R0, LT.BENCH_BC, LT.BENCH_SIGNMASK)
+    xs = [LT.gaussian_vector(L, 51 + i) for i in range(3)]
+    hv = [q.create_V(x) for x in xs]
+    eps = [0.3, -0.2, 0.5]
+    zero = [np.zeros((V, 3, 3, 2)) for _ in range(4)]
+
+    def agree(F, key, tol):
+        got = np.stack([np.asarray(f, dtype=np.float64) for f in q.extract_F(F, V)]).reshape(d[key].shape)
+        assert np.abs(got - d[key]).max() <= tol * np.abs(d[key]).max(), key
+
+    for n, key in ((1, "force_asq_asvec"), (3, "force_asq_fnmat")):
+        F = q.create_F(zero)
+        assert q.asqtad_force(hG, F, LT.ASQTAD_BENCH_COEFFS, eps[:n], hv[:n]).status == 0
+        agree(F, key, 1e-12)
+        q.destroy_F(F)
+    hc = LT.hisq_bench_coeffs()
+    hc.n_naiks = 2
+    hc.eps_naik[1] = 0.1
+    hc.difference_one_link, hc.difference_naik = 0.3, -0.05
+    q.set_hisq_opts(want_aux=1)
+    H = q.hisq_create_L_from_G(hc, hG)
+    F = q.create_F(zero)
+    assert q.hisq_force(H, F, hc, eps, hv, [2, 1]).status == 0
+    agree(F, "force_hisq", 1e-9)
+    q.destroy_F(F)
+    q.hisq_destroy_L(H)
+    for h in hv:
+        q.destroy_V(h)
+    q.destroy_G(hG)

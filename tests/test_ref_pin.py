@@ -101,6 +101,31 @@ def test_golden_hisq_links_and_dslash(gold):
     assert rel_norm_err(fo.dslash(0.05, src, 2, 2), d["hisq_dslash_eoeo"]) < 1e-13
 
 
+def test_golden_forces(gold):
+    """Fermion forces on a rough field with two filtered fat7 links: the
+    oracle's asqtad force (ASVEC with one source, FNMAT with three) and its
+    HISQ force (two Naik groups, the default force filter) equal the
+    reference's outputs to rounding."""
+    d, L, _, _ = gold
+    V = int(np.prod(L))
+    Ur = LT.random_gauge(L, 0.5, 2)
+    assert close_ck(checksum(Ur), d["force_gauge_ck"])
+    Gr = O.Lattice(L).rephase_G(Ur, LT.BENCH_R0, LT.BENCH_BC, LT.BENCH_SIGNMASK)
+    xs = [LT.gaussian_vector(L, 51 + i).reshape(V, 6) for i in range(3)]
+    eps = [0.3, -0.2, 0.5]
+    lat = O.Lattice(L)
+
+    def agree(got, key, tol):
+        ref = d[key]
+        assert np.abs(np.stack(got) - ref).max() <= tol * np.abs(ref).max(), key
+
+    agree(lat.asqtad_force(LT.ASQTAD_BENCH_COEFFS, Gr, eps[:1], xs[:1]), "force_asq_asvec", 1e-13)
+    agree(lat.asqtad_force(LT.ASQTAD_BENCH_COEFFS, Gr, eps, xs), "force_asq_fnmat", 1e-13)
+    hf = LT.hisq_coeff_vector(LT.hisq_bench_coeffs())
+    hf[11], hf[12] = 0.3, -0.05
+    agree(lat.hisq_force(hf, Gr, [0.0, 0.1], np.array(eps), xs, [2, 1]), "force_hisq", 1e-9)
+
+
 # ---------------------------------------------------------------- live library
 
 LIVE_L = [(4, 4, 4, 4), (4, 4, 4, 6), (8, 8, 8, 8), (6, 4, 4, 8)]
@@ -305,12 +330,13 @@ def test_live_asqtad_force(coeffs, nsrc, fsm):
 
 
 @live
-def test_live_asqtad_deriv_differs_only_by_unitary_directions():
-    """The reference's derivative field (QOP_D3_asqtad_deriv, its staple
-    recursion writes U^+ where the general derivative has U^-1) and the
-    oracle's (the derivative for general complex links, pinned by finite
-    differences) differ by U H with H Hermitian: nothing of it survives the
-    force's projection TA(U D^+)."""
+@pytest.mark.parametrize("coeffs", [LT.ASQTAD_BENCH_COEFFS, (0.625, -0.0625, 0.0104, -0.00130, -0.0625, -0.0417)])
+def test_live_asqtad_deriv(coeffs):
+    """The derivative field itself (QOP_D3_asqtad_deriv): the oracle's
+    reverse sweep plus the reference's Lepage term (lepage_rep) equals the
+    reference's field to rounding; the general-complex derivative (pinned by
+    finite differences in test_oracle.py) differs from it by U H with H
+    Hermitian, which the force projection TA(U D^+) removes."""
     L = (4, 4, 4, 6)
     V = int(np.prod(L))
     G = O.Lattice(L).rephase_G(_gauge(L, eps=0.5))
@@ -318,12 +344,15 @@ def test_live_asqtad_deriv_differs_only_by_unitary_directions():
     mF = [rng.standard_normal((V, 3, 3, 2)) for _ in range(4)]
     mN = [rng.standard_normal((V, 3, 3, 2)) for _ in range(4)]
     cz = lambda a: a[..., 0] + 1j * a[..., 1]
-    do = O.Lattice(L).asqtad_deriv(LT.ASQTAD_BENCH_COEFFS, G, mF, mN)
-    dr = R.asqtad_deriv(L, LT.ASQTAD_BENCH_COEFFS, G, mF, mN)
-    assert maxdiff(do, dr) > 1e-3                       # the representations do differ
+    dr = R.asqtad_deriv(L, coeffs, G, mF, mN)
+    do = O.Lattice(L).asqtad_deriv(coeffs, G, mF, mN, lepage_rep=True)
+    scale = max(float(np.abs(a).max()) for a in dr)
+    assert maxdiff(do, dr) < 1e-13 * scale
+    dg = O.Lattice(L).asqtad_deriv(coeffs, G, mF, mN)
+    assert maxdiff(dg, dr) > 1e-3 * scale               # the Lepage term is there
     for mu in range(4):
-        x = np.einsum("sij,skj->sik", cz(G[mu]), np.conj(cz(dr[mu]) - cz(do[mu])))   # U (D_ref - D_oracle)^+
-        assert np.abs(x - np.conj(np.swapaxes(x, 1, 2))).max() < 1e-12
+        x = np.einsum("sij,skj->sik", cz(G[mu]), np.conj(cz(dr[mu]) - cz(dg[mu])))   # U (D_ref - D_general)^+
+        assert np.abs(x - np.conj(np.swapaxes(x, 1, 2))).max() < 1e-12 * scale
 
 
 @live
@@ -331,10 +360,9 @@ def test_live_asqtad_deriv_differs_only_by_unitary_directions():
 @pytest.mark.parametrize("eps_naik", [(0.0,), (0.0, 0.1)])
 def test_live_hisq_force(eps_g, ff, eps_naik):
     """QOP_D3_hisq_force_multi_qdp (U(3) projection, the RATIONAL force
-    branch): the oracle agrees to rounding where the force filter changes
-    nothing -- a gauge field whose fat7 links all have V^+V eigenvalues
-    above the 5e-5 default, or the filter off (force_filter 0) on a rough
-    one."""
+    branch): the oracle agrees to rounding on a smooth gauge field (every
+    fat7 link's V^+V eigenvalues above the 5e-5 default filter) and on a
+    rough one with the filter off (force_filter 0)."""
     L = (4, 4, 4, 6)
     V = int(np.prod(L))
     G = O.Lattice(L).rephase_G(_gauge(L, eps=eps_g))
@@ -355,11 +383,7 @@ def test_live_force_filter_per_link():
     """At a filtered link (V^+V eigenvalue below force_filter) the
     reference's derivative tensors are those of V (V^+V + ff)^-1/2, and its
     chain rule equals the oracle's adjoint with the filter; elsewhere the
-    filter does nothing.  (On whole forces the filtered results still differ
-    near such links: the W-level derivative the filtered adjoint receives
-    differs between the reference and the oracle by W H terms, H Hermitian,
-    which the unfiltered projection's adjoint removes and the filtered one
-    does not; see test_live_asqtad_deriv_differs_only_by_unitary_directions.)"""
+    filter does nothing."""
     L = (4, 4, 4, 6)
     G = O.Lattice(L).rephase_G(_gauge(L, eps=0.5))
     hc = LT.hisq_coeff_vector(LT.hisq_bench_coeffs())
@@ -400,3 +424,31 @@ def test_live_force_filter_per_link():
         new = np.einsum("ijmn,ji->nm", dw, F) + np.einsum("ijmn,ji->nm", dwd, F.conj().T)
         mine = adj(X, F.conj().T, 5e-5).conj().T
         assert np.abs(new - mine).max() < 1e-8 * np.abs(new).max()
+
+
+@live
+@pytest.mark.parametrize("eps_naik", [(0.0,), (0.0, 0.1)])
+def test_live_hisq_force_filtered(eps_naik):
+    """The whole HISQ force on a rough field with one filtered link and the
+    default filter: the W-level derivative that the filtered U(3) adjoint
+    receives carries the reference's Lepage term (test_live_asqtad_deriv),
+    which that adjoint does not remove, so the oracle matches the reference
+    on every link, the ~140 around the filtered one included."""
+    L = (4, 4, 4, 6)
+    V = int(np.prod(L))
+    G = O.Lattice(L).rephase_G(_gauge(L, eps=0.5))
+    hc = LT.hisq_coeff_vector(LT.hisq_bench_coeffs())
+    Vl, _ = O.Lattice(L).make_imp_links([hc[0], hc[1], hc[2], hc[3], 0.0, 0.0], G, naik=False)
+    cz = lambda a: a[..., 0] + 1j * a[..., 1]
+    Vs = np.concatenate([cz(v) for v in Vl])
+    wmin = np.linalg.eigvalsh(np.einsum("sji,sjk->sik", Vs.conj(), Vs)).min(axis=1)
+    assert (wmin < 5e-5).sum() == 1                 # one filtered link on this field
+    rng = np.random.default_rng(9)
+    xs = [rng.standard_normal((V, 6)) for _ in range(3)]
+    res = [0.3, -0.2, 0.5]
+    n_orders = [3] if len(eps_naik) == 1 else [2, 1]
+    hc[11], hc[12] = 0.3, -0.05
+    fo = O.Lattice(L).hisq_force(hc, G, list(eps_naik), np.array(res), xs, n_orders)
+    fr = R.hisq_force(L, hc, G, list(eps_naik), res, xs, n_orders)
+    scale = max(float(np.abs(a).max()) for a in fo)
+    assert maxdiff(fo, fr) < 1e-9 * scale, (maxdiff(fo, fr), scale)
