@@ -82,6 +82,9 @@ def parse():
                          "after each host check is not over-represented)")
     ap.add_argument("--quick", action="store_true", help="skip FP64 baseline and e2e (development)")
     ap.add_argument("--dd-mask", type=int, default=15, help="dd workload on one GPU: self-split directions")
+    ap.add_argument("--dd-runs", default="u16,u64,d16,d64",
+                    help="dd workload runs: u/d (undecomposed / decomposed) x 16/64 (sloppy precision)")
+    ap.add_argument("--dd-max-iter", type=int, default=200000, help="dd workload: iteration limit of each solve")
     ap.add_argument("--hop-kernel", type=int, default=None, help="int16 hop variant (library default if unset)")
     ap.add_argument("--batch-kernel", type=int, default=None, help="batched hop variant (chosen by batch size if unset)")
     ap.add_argument("--ab", default=None, help="A/B of a 0/1 solver option (e.g. fuse_update) on the headline solve: "
@@ -1034,7 +1037,8 @@ def run_dd(a):
         def solve():
             q.dslash(fla, 0.0, hout, hout, QOP_EVEN, QOP_EVEN)   # zero initial guess
             ra = QOP_resid_arg_t(rsq, 0, 0, 0, 0, 0)
-            inf = q.invert(fla, a.mass, hout, hin, QOP_invert_arg_t(1e9, 200000, 200000, 10, QOP_EVEN), ra)
+            inf = q.invert(fla, a.mass, hout, hin, QOP_invert_arg_t(1e9, a.dd_max_iter, a.dd_max_iter, 10, QOP_EVEN),
+                           ra)
             assert inf.status == 0
             return ra
 
@@ -1061,11 +1065,15 @@ def run_dd(a):
                if k.startswith("hop_")}
         return {"label": label, "prec_sloppy": prec, "ms_per_solve": ms, "iters": int(np.median(its)), "hop": hop}
 
+    want = set(a.dd_runs.split(","))
+    if not want & {"d16", "d64"}:
+        raise SystemExit("--dd-runs needs d16 or d64")
     runs = []
     if world == 1:
         assert q.init(L) == 0
-        runs.append(measure("undecomposed", 16))
-        runs.append(measure("undecomposed", 64))
+        for prec in (16, 64):
+            if "u%d" % prec in want:
+                runs.append(measure("undecomposed", prec))
         q.finalize()
         uid = q.comm_unique_id()
     else:
@@ -1080,12 +1088,13 @@ def run_dd(a):
     else:
         assert q.init(L, machsize=P) == 0
     info = q.dd_info()
-    runs.append(measure("decomposed", 16))
-    runs.append(measure("decomposed", 64))
+    for prec in (16, 64):
+        if "d%d" % prec in want:
+            runs.append(measure("decomposed", prec))
     q.finalize()
     q.dd_self_split(0)
     q.comm_finalize()
-    dd = runs[-2]
+    dd = next(r for r in runs if r["label"] == "decomposed")
     value = world * 1e3 / dd["ms_per_solve"] if world > 1 else 1e3 / dd["ms_per_solve"]
     if rank == 0:
         line = {"metric": "mixed-prec CG solves/s @%g, decomposed lattice" % a.tol, "value": value, "unit": "solves/s",
@@ -1096,8 +1105,9 @@ def run_dd(a):
                            "mass": a.mass, "tol": a.tol, "eps": a.eps},
                 "runs": runs}
         if world == 1:
-            line["overhead_vs_undecomposed"] = {"int16": runs[2]["ms_per_solve"] / runs[0]["ms_per_solve"],
-                                                "fp64": runs[3]["ms_per_solve"] / runs[1]["ms_per_solve"]}
+            ms = {(r["label"][0], r["prec_sloppy"]): r["ms_per_solve"] for r in runs}
+            line["overhead_vs_undecomposed"] = {k: ms[("d", p)] / ms[("u", p)] for k, p in (("int16", 16), ("fp64", 64))
+                                                if ("d", p) in ms and ("u", p) in ms}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()

@@ -373,9 +373,46 @@ template <typename T> DdGhost<T> dd_halo(FlaT<T> *f, const c2<T> *in, int q) {
 }
 
 // int16 records: raw slabs copy the records; product slabs decode the
-// record, apply -U^+ with the FP64 forward link and store a new record
-__global__ void k_dd_pack_q16(const uint4 *__restrict__ in, const double2 *__restrict__ lk, Geom g, int q, int nl,
-                              DdPackPlan pl) {
+// record and the forward link from the solver's blocked int16 links (the
+// same stored values the hop multiplies; 40 bytes per fat and 28 per
+// reconstructed long link instead of 144 in FP64), apply -U^+ and store a
+// new record
+__device__ __forceinline__ void q16_link_decode(const unsigned char *lq, int nl, bool recon, float c_long, int k,
+                                                i64 i, float2 U[9]) {
+  const unsigned char *base = lq + (size_t)(i / QB) * q16_block_bytes(nl, recon) + q16_slot_off(k, recon);
+  const int t = (int)(i % QB);
+  const uint4 ua = reinterpret_cast<const uint4 *>(base)[t];
+  U[0] = make_float2(u16_lo(ua.x), u16_hi(ua.x)); U[1] = make_float2(u16_lo(ua.y), u16_hi(ua.y));
+  U[2] = make_float2(u16_lo(ua.z), u16_hi(ua.z)); U[3] = make_float2(u16_lo(ua.w), u16_hi(ua.w));
+  float sc;
+  if (recon && (k & 1)) {   // two rows / |c| and the det phase; row 2 = det conj(row0 x row1)
+    const uint2 ub = reinterpret_cast<const uint2 *>(base + 16 * QB)[t];
+    const float phase = reinterpret_cast<const float *>(base + 24 * QB)[t];
+    U[4] = make_float2(u16_lo(ub.x), u16_hi(ub.x)); U[5] = make_float2(u16_lo(ub.y), u16_hi(ub.y));
+    float sn, cs;
+    __sincosf(phase, &sn, &cs);
+    const float2 z = make_float2(cs * (1.0f / 32767.0f), sn * (1.0f / 32767.0f));
+    const float2 c0 = csub<float>(cmul<float>(U[1], U[5]), cmul<float>(U[2], U[4]));
+    const float2 c1 = csub<float>(cmul<float>(U[2], U[3]), cmul<float>(U[0], U[5]));
+    const float2 c2 = csub<float>(cmul<float>(U[0], U[4]), cmul<float>(U[1], U[3]));
+    U[6] = cmul<float>(z, make_float2(c0.x, -c0.y));
+    U[7] = cmul<float>(z, make_float2(c1.x, -c1.y));
+    U[8] = cmul<float>(z, make_float2(c2.x, -c2.y));
+    sc = c_long * (1.0f / 32767.0f);
+  } else {
+    const uint4 ub = reinterpret_cast<const uint4 *>(base + 16 * QB)[t];
+    const uint2 uc = reinterpret_cast<const uint2 *>(base + 32 * QB)[t];
+    U[4] = make_float2(u16_lo(ub.x), u16_hi(ub.x)); U[5] = make_float2(u16_lo(ub.y), u16_hi(ub.y));
+    U[6] = make_float2(u16_lo(ub.z), u16_hi(ub.z)); U[7] = make_float2(u16_lo(ub.w), u16_hi(ub.w));
+    U[8] = make_float2(u16_lo(uc.x), u16_hi(uc.x));
+    sc = __uint_as_float(uc.y) * (1.0f / 32767.0f);
+  }
+#pragma unroll
+  for (int e = 0; e < 9; e++) U[e] = make_float2(U[e].x * sc, U[e].y * sc);
+}
+
+__global__ void k_dd_pack_q16(const uint4 *__restrict__ in, const unsigned char *__restrict__ lq, Geom g, int q,
+                              int nl, bool recon, float c_long, DdPackPlan pl) {
   const int depth = dd_depth(nl);
   int j, s, fi;
   if (!dd_plan_entry(pl, blockIdx.x * (i64)blockDim.x + threadIdx.x, j, s, fi)) return;
@@ -389,39 +426,37 @@ __global__ void k_dd_pack_q16(const uint4 *__restrict__ in, const double2 *__res
     sraw[(i64)s * fh + fi] = in[i];
     return;
   }
-  float2 v[3];
+  float2 v[3], U[9];
   SpQ16::load(in, i, Vh, v);
-  const double2 *U = lk + (i64)slot * 9 * Vh + i;
+  q16_link_decode(lq, nl, recon, c_long, slot, i, U);
   float2 o[3];
 #pragma unroll
   for (int r = 0; r < 3; r++) {   // -(U^+ v)_r = -sum_c conj(U_cr) v_c
-    double ax = 0, ay = 0;
+    float ax = 0.f, ay = 0.f;
 #pragma unroll
     for (int cc = 0; cc < 3; cc++) {
-      const double2 u = U[(3 * cc + r) * Vh];
-      ax += u.x * v[cc].x + u.y * v[cc].y;
-      ay += u.x * v[cc].y - u.y * v[cc].x;
+      const float2 u = U[3 * cc + r];
+      ax = fmaf(u.x, v[cc].x, fmaf(u.y, v[cc].y, ax));
+      ay = fmaf(u.x, v[cc].y, fmaf(-u.y, v[cc].x, ay));
     }
-    o[r] = make_float2((float)-ax, (float)-ay);
+    o[r] = make_float2(-ax, -ay);
   }
   SpQ16::store(sprod + (i64)(s - depth) * fh, fi, fh, o);
 }
 
-DdQ16Ghost dd_halo_q16(FlaT<double> *f, const uint4 *in, int q) {
+DdQ16Ghost dd_halo_q16(int nl, const unsigned char *lq, bool recon, float c_long, const uint4 *in, int q) {
   Context &c = ctx();
   Dd &d = *c.dd;
   const Geom &g = c.g;
   DdQ16Ghost h{};
   h.mask = d.mask;
-  const int nl = f->nlinks;
-  const double2 *lk = f->d + (i64)q * nl * 9 * g.Vh;
   for (int mu = 0; mu < 4; mu++) {
     h.fh[mu] = d.fh[mu];
     h.up[mu] = (const uint4 *)d.gup[mu];
     h.dn[mu] = (const uint4 *)d.gdn[mu];
   }
   const DdPackPlan pl = dd_plan(d, nl);
-  k_dd_pack_q16<<<grid_for(pl.start[pl.n], 128), 128, 0, c.s>>>(in, lk, g, q, nl, pl);
+  k_dd_pack_q16<<<grid_for(pl.start[pl.n], 128), 128, 0, c.s>>>(in, lq, g, q, nl, recon, c_long, pl);
   QLAUNCH();
   dd_exchange(d, nl, sizeof(uint4), sizeof(uint4));
   return h;

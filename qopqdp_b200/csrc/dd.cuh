@@ -87,13 +87,15 @@ template <typename T> DdGhost<T> dd_halo(FlaT<T> *f, const c2<T> *in, int q);
 
 // the same for the int16 sloppy solver: in holds the parity-q int16 site
 // records (16 bytes each); the up halo carries records, the down halo the
-// products -U^+ psi (formed with the FP64 links, stored as int16 records)
+// products -U^+ psi, formed with lq, the solver's blocked int16 links of
+// parity q (nl slots, long links reconstructed with |c| = c_long when
+// recon), and stored as int16 records
 struct DdQ16Ghost {
   const uint4 *up[4];
   const uint4 *dn[4];
   int fh[4];
   int mask;
 };
-DdQ16Ghost dd_halo_q16(FlaT<double> *f, const uint4 *in, int q);
+DdQ16Ghost dd_halo_q16(int nl, const unsigned char *lq, bool recon, float c_long, const uint4 *in, int q);
 
 }  // namespace qopb

@@ -492,18 +492,20 @@ __global__ void k_links_f16(uint4 *A, uint4 *B, __half2 *C, const double2 *src, 
 // sites beyond Vh in the last block are zero links
 
 // largest unitarity defect |L L^+ / c^2 - 1| and the range of row-0 norms c
-// over all long links; decides whether RECON is exact enough
+// over all long links; decides whether RECON is exact enough.  Each warp
+// reduces its lanes first and one lane per warp updates the three words
+// (the values are non-negative, so their bit patterns order as integers).
 __global__ void k_long_check(const double2 *src, int nl, i64 Vh, unsigned long long *defect,
                              unsigned long long *cmax, unsigned long long *cmin) {
   i64 s = blockIdx.x * (i64)blockDim.x + threadIdx.x;   // over [2][nl/2 long slots][Vh]
-  if (s >= 2 * (nl / 2) * Vh) return;
+  double d = 0, cx = 0, cn = 1e300;
+  if (s < 2 * (nl / 2) * Vh) {
   const i64 i = s % Vh, r = s / Vh;
   const int k = 2 * (int)(r % (nl / 2)) + 1, p = (int)(r / (nl / 2));
   double2 e[9];
   for (int j = 0; j < 9; j++) e[j] = src[(((i64)p * nl + k) * 9 + j) * Vh + i];
   double c2 = e[0].x * e[0].x + e[0].y * e[0].y + e[1].x * e[1].x + e[1].y * e[1].y + e[2].x * e[2].x +
               e[2].y * e[2].y;
-  double d = 0;
   for (int a = 0; a < 3; a++)
     for (int b = 0; b < 3; b++) {
       double re = 0, im = 0;
@@ -516,10 +518,19 @@ __global__ void k_long_check(const double2 *src, int nl, i64 Vh, unsigned long l
       im = im / c2;
       d = fmax(d, fmax(fabs(re), fabs(im)));
     }
-  const double c = sqrt(c2);
-  atomicMax(defect, (unsigned long long)__double_as_longlong(d));
-  atomicMax(cmax, (unsigned long long)__double_as_longlong(c));
-  atomicMin(cmin, (unsigned long long)__double_as_longlong(c));
+  cx = cn = sqrt(c2);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    d = fmax(d, __shfl_xor_sync(0xffffffffu, d, o));
+    cx = fmax(cx, __shfl_xor_sync(0xffffffffu, cx, o));
+    cn = fmin(cn, __shfl_xor_sync(0xffffffffu, cn, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(defect, (unsigned long long)__double_as_longlong(d));
+    atomicMax(cmax, (unsigned long long)__double_as_longlong(cx));
+    atomicMin(cmin, (unsigned long long)__double_as_longlong(cn));
+  }
 }
 
 __global__ void k_links_q16b(unsigned char *dst, const double2 *src, int nl, i64 Vh, i64 nblk, int recon,
@@ -1386,14 +1397,14 @@ static void run_mixed(LinOp<double> &L, QOP_invert_arg_t *ia, QOP_resid_arg_t *r
           const unsigned char *lq = (const unsigned char *)lk_q.a, *lp = (const unsigned char *)lk_p.a;
           {
             ProfScope ps1(hname, hop_bytes);
-            const DdQ16Ghost g1 = dd_halo_q16(L.f, ps, p);
+            const DdQ16Ghost g1 = dd_halo_q16(nl, lp, recon, c_long, ps, p);
             launch_q16_dd(1, nl, recon, c_long, gridq, ts, ps, lq, nullptr, g, ng, q, dst, nullptr, 0, g1);
             recs.push_back(ps1.idx);
           }
           dd_allreduce(&dst->dp2, 1);
           {
             ProfScope ps2(hname3, hop_bytes + (double)Vh * Sp::site_bytes * 2);
-            const DdQ16Ghost g2 = dd_halo_q16(L.f, ts, q);
+            const DdQ16Ghost g2 = dd_halo_q16(nl, lq, recon, c_long, ts, q);
             launch_q16_dd(3, nl, recon, c_long, gridq, Aps, ts, lp, ps, g, ng, p, dst, rs, ++seq, g2);
             recs.push_back(ps2.idx);
           }
