@@ -81,6 +81,9 @@ def parse():
                          "the samples rotate over the positions in a 16-iteration chunk, so the first launch "
                          "after each host check is not over-represented)")
     ap.add_argument("--quick", action="store_true", help="skip FP64 baseline and e2e (development)")
+    ap.add_argument("--other-configs", default="multimass,multisrc",
+                    help="headline run on one GPU: batched workloads also run (own processes, after the timed "
+                         "region) and summarised in its line; empty to skip")
     ap.add_argument("--dd-mask", type=int, default=15, help="dd workload on one GPU: self-split directions")
     ap.add_argument("--dd-runs", default="u16,u64,d16,d64",
                     help="dd workload runs: u/d (undecomposed / decomposed) x 16/64 (sloppy precision)")
@@ -336,6 +339,35 @@ def run_reference(a):
 
 
 # ---------------------------------------------------------------- device arm
+def other_configs(a):
+    """The batched workloads in their own processes after the headline's
+    timed region (one warm-up call and one timed call each; multisrc without
+    its 16-solve FP64 comparison), summarised for the headline line."""
+    out = {}
+    for wl in a.other_configs.split(","):
+        cmd = [sys.executable, os.path.abspath(__file__), "--workload", wl, "--steps", "1", "--warmup", "1",
+               "--seed", str(a.seed), "--tol", str(a.tol)]
+        if wl == "multisrc":
+            cmd.append("--quick")
+        try:
+            r = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+            d = json.loads([x for x in r.stdout.splitlines() if x.startswith("{")][-1])
+            keep = ("metric", "value", "unit", "ms_per_step", "steps", "warmup", "final_rsq_max", "config",
+                    "speedup_vs_fp64", "gpu_launches", "clocks")
+            o = {k: d.get(k) for k in keep}
+            roof = d.get("roofline") or {}
+            o["roofline"] = {k: roof.get(k) for k in ("kernel", "avg_us", "achieved", "frac", "peak")}
+            if d.get("fp64"):
+                o["fp64_solves_per_s"] = d["fp64"]["solves_per_s"]
+            if d.get("batched_mode"):
+                o["batched_mode_solves_per_s"] = d["batched_mode"]["solves_per_s"]
+            o["command"] = " ".join(["python bench.py"] + cmd[2:])
+            out[wl] = o
+        except Exception as e:   # recorded, never fatal to the headline line
+            out[wl] = {"error": "%s: %s" % (type(e).__name__, str(e)[:200])}
+    return out
+
+
 def run_b200(a):
     rank, local, world = rank_info()
     import torch
@@ -532,6 +564,8 @@ def run_b200(a):
         mhz = line["clocks"].get("sm_mhz")
         if roof and mhz:
             roof["avg_us_x_sm_mhz"] = kernels[roof["kernel"]]["avg_us"] * mhz
+        if world == 1 and not a.quick and a.other_configs:
+            line["other_configs"] = other_configs(a)
         print(json.dumps(line), flush=True)
     q.destroy_V(hin)
     q.destroy_V(hout)
