@@ -55,7 +55,8 @@ int QOPB_inject_alloc_failure(int n);
    sites per parity are rejected with info->status = QOP_FAIL and a return
    value of -1.  The call is synchronous (it returns the norm to the host).
    The first call on a device looks up that array's device address under a
-   lock.  All calls share the array: calls that overlap on the GPU race and
+   lock; make that first call before any stream capture begins.  All calls
+   share the array: calls that overlap on the GPU race and
    must be serialised by the caller. */
 double QOPB_D3_asqtad_ddagd_norm2_noalloc(QOP_info_t *info, QOP_D3_FermionLinksAsqtad *asqtad, double mass,
                                           QOP_D3_ColorVector *out, QOP_D3_ColorVector *in, QOP_evenodd_t eo);

@@ -22,9 +22,10 @@
 //
 // The first call on a device looks up the array's device address (the host
 // symbol is only a stand-in) with that device current; the lookup is
-// guarded by a lock, so first calls from several host threads are safe.  The
-// call is synchronous: it waits on the library stream and returns the norm
-// to the host.
+// guarded by a lock, so first calls from several host threads are safe.
+// That first call should come before any stream capture begins.  The call
+// is synchronous: it waits on the library stream and returns the norm to
+// the host.
 #include "qopb.h"
 #include <mutex>
 
