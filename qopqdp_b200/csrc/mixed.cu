@@ -492,33 +492,38 @@ __global__ void k_links_f16(uint4 *A, uint4 *B, __half2 *C, const double2 *src, 
 // sites beyond Vh in the last block are zero links
 
 // largest unitarity defect |L L^+ / c^2 - 1| and the range of row-0 norms c
-// over all long links; decides whether RECON is exact enough.  Each warp
-// reduces its lanes first and one lane per warp updates the three words
-// (the values are non-negative, so their bit patterns order as integers).
-__global__ void k_long_check(const double2 *src, int nl, i64 Vh, unsigned long long *defect,
-                             unsigned long long *cmax, unsigned long long *cmin) {
-  i64 s = blockIdx.x * (i64)blockDim.x + threadIdx.x;   // over [2][nl/2 long slots][Vh]
+// over all long links; decides whether RECON is exact enough.  A grid of a
+// few blocks per SM strides over the links; each block reduces its threads
+// (warp shuffles, then its warps through shared memory) and one thread per
+// block updates the three words (the values are non-negative, so their bit
+// patterns order as integers).
+__global__ void __launch_bounds__(256) k_long_check(const double2 *src, int nl, i64 Vh, unsigned long long *defect,
+                                                    unsigned long long *cmax, unsigned long long *cmin) {
+  const i64 n = 2 * (nl / 2) * Vh;   // over [2][nl/2 long slots][Vh]
   double d = 0, cx = 0, cn = 1e300;
-  if (s < 2 * (nl / 2) * Vh) {
-  const i64 i = s % Vh, r = s / Vh;
-  const int k = 2 * (int)(r % (nl / 2)) + 1, p = (int)(r / (nl / 2));
-  double2 e[9];
-  for (int j = 0; j < 9; j++) e[j] = src[(((i64)p * nl + k) * 9 + j) * Vh + i];
-  double c2 = e[0].x * e[0].x + e[0].y * e[0].y + e[1].x * e[1].x + e[1].y * e[1].y + e[2].x * e[2].x +
-              e[2].y * e[2].y;
-  for (int a = 0; a < 3; a++)
-    for (int b = 0; b < 3; b++) {
-      double re = 0, im = 0;
-      for (int j = 0; j < 3; j++) {
-        double2 x = e[3 * a + j], y = e[3 * b + j];
-        re += x.x * y.x + x.y * y.y;
-        im += x.y * y.x - x.x * y.y;
+  for (i64 s = blockIdx.x * (i64)blockDim.x + threadIdx.x; s < n; s += (i64)gridDim.x * blockDim.x) {
+    const i64 i = s % Vh, r = s / Vh;
+    const int k = 2 * (int)(r % (nl / 2)) + 1, p = (int)(r / (nl / 2));
+    double2 e[9];
+    for (int j = 0; j < 9; j++) e[j] = src[(((i64)p * nl + k) * 9 + j) * Vh + i];
+    const double c2 = e[0].x * e[0].x + e[0].y * e[0].y + e[1].x * e[1].x + e[1].y * e[1].y + e[2].x * e[2].x +
+                      e[2].y * e[2].y;
+    const double ic2 = 1.0 / c2;
+    for (int a = 0; a < 3; a++)
+      for (int b = 0; b < 3; b++) {
+        double re = 0, im = 0;
+        for (int j = 0; j < 3; j++) {
+          double2 x = e[3 * a + j], y = e[3 * b + j];
+          re += x.x * y.x + x.y * y.y;
+          im += x.y * y.x - x.x * y.y;
+        }
+        re = re * ic2 - (a == b ? 1.0 : 0.0);
+        im = im * ic2;
+        d = fmax(d, fmax(fabs(re), fabs(im)));
       }
-      re = re / c2 - (a == b ? 1.0 : 0.0);
-      im = im / c2;
-      d = fmax(d, fmax(fabs(re), fabs(im)));
-    }
-  cx = cn = sqrt(c2);
+    const double c = sqrt(c2);
+    cx = fmax(cx, c);
+    cn = fmin(cn, c);
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
@@ -526,7 +531,16 @@ __global__ void k_long_check(const double2 *src, int nl, i64 Vh, unsigned long l
     cx = fmax(cx, __shfl_xor_sync(0xffffffffu, cx, o));
     cn = fmin(cn, __shfl_xor_sync(0xffffffffu, cn, o));
   }
-  if ((threadIdx.x & 31) == 0) {
+  __shared__ double sd[8], sx[8], sn[8];
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) { sd[w] = d; sx[w] = cx; sn[w] = cn; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 1; k < (int)(blockDim.x >> 5); k++) {
+      d = fmax(d, sd[k]);
+      cx = fmax(cx, sx[k]);
+      cn = fmin(cn, sn[k]);
+    }
     atomicMax(defect, (unsigned long long)__double_as_longlong(d));
     atomicMax(cmax, (unsigned long long)__double_as_longlong(cx));
     atomicMin(cmin, (unsigned long long)__double_as_longlong(cn));
@@ -1040,7 +1054,8 @@ SloppyLinks *sloppy_get(FlaT<double> *f, int lkfmt) {
       memcpy(&init[2], &big, 8);
       QCHECK(cudaMemcpyAsync(st, init, sizeof init, cudaMemcpyHostToDevice, ctx().s));
       const i64 nc = 2 * (f->nlinks / 2) * g.Vh;
-      k_long_check<<<grid_for(nc, 256), 256, 0, ctx().s>>>(f->d, f->nlinks, g.Vh, st, st + 1, st + 2);
+      k_long_check<<<std::min<i64>(grid_for(nc, 256), (i64)ctx().red_blocks), 256, 0, ctx().s>>>(
+          f->d, f->nlinks, g.Vh, st, st + 1, st + 2);
       QLAUNCH();
       unsigned long long h[3];
       QCHECK(cudaMemcpyAsync(h, st, sizeof h, cudaMemcpyDeviceToHost, ctx().s));
