@@ -327,7 +327,7 @@ QOP_status_t QOP_asqtad_invert_set_opts(QOP_opt_t opts[], int nopts) {
     } else if (!strcmp(t, "recon_long")) {
       n.recon_long = v != 0;
     } else if (!strcmp(t, "hop_kernel")) {
-      if (v < -1 || v > 28) return QOP_FAIL;
+      if (v < -1 || v > 31) return QOP_FAIL;
       n.hop_kernel = (int)v;
     } else if (!strcmp(t, "half_format")) {
       if (v < 0 || v > 2) return QOP_FAIL;

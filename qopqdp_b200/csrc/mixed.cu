@@ -915,8 +915,18 @@ k_mix_hop_q16a(uint4 *__restrict__ out, const uint4 *__restrict__ src, const uns
 // lattice): a neighbour outside the block comes from the halos of gh (an
 // up record multiplies the link as usual; a down record is the product
 // -U^+ psi and is added as is)
+// PF > 0 (persistent variants 29-31): thread 0 of a block asks L2 to fetch
+// the link bytes of the slot batch PF batches ahead of the one the block
+// starts (cp.async.bulk.prefetch.L2: no destination, no registers, no
+// completion to wait for), so the block's own loads of that batch later hit
+// L2 instead of waiting on HBM.  Batch b of site block sb is the contiguous
+// span of slots [b BATCH, (b + 1) BATCH) of that block's link record.
+__device__ __forceinline__ void l2_prefetch_bulk(const void *p, unsigned bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
 template <int NL, int KIND, int BATCH, bool RECON, int MINB = 1, bool PERSIST = false, bool PK = false,
-          bool DDQ = false>
+          bool DDQ = false, int PF = 0>
 __global__ void __launch_bounds__(QB, MINB)
 k_mix_hop_q16r(uint4 *__restrict__ out, const uint4 *__restrict__ src, const unsigned char *__restrict__ lk,
                const uint4 *__restrict__ same, Geom g, NbrGeom ng, int p, MixState *st, double *part,
@@ -950,6 +960,16 @@ k_mix_hop_q16r(uint4 *__restrict__ out, const uint4 *__restrict__ src, const uns
     }
 #pragma unroll
     for (int k0 = 0; k0 < NL; k0 += BATCH) {
+      if constexpr (PERSIST && PF > 0) {
+        constexpr int NB = NL / BATCH;
+        if (tid == 0) {
+          const int lin = k0 / BATCH + PF, blk = sb + (lin / NB) * gridDim.x, bb = lin % NB;
+          if (blk < nsb) {
+            const int o0 = q16_slot_off(bb * BATCH, RECON), o1 = q16_slot_off((bb + 1) * BATCH, RECON);
+            l2_prefetch_bulk(lk + (size_t)blk * q16_block_bytes(NL, RECON) + o0, (unsigned)(o1 - o0));
+          }
+        }
+      }
       uint4 ua[BATCH], ub[BATCH], nb[BATCH];
       uint2 uc[BATCH];
       bool prd[BATCH];
@@ -1115,6 +1135,10 @@ LinksSloppy links_parity(SloppyLinks *s, int lkfmt, int p) {
 // default), 110.0 with 23, 111.2 with 20 / 21, 112-113 with 22, 24, 26,
 // against 117.3 for the scalar variant 15 (a third fewer instructions per
 // slot; the kernel was issue-bound at 62 % issue-active).
+// 29-31 = 25 with an L2 bulk prefetch of the link stream 2 / 4 / 1 slot
+// batches ahead: slower at 32^3x64 (hop / fused hop 118.1 / 123.4,
+// 118.7 / 121.4 and 135.0 / 139.6 us against 113.0 / 119.2 us for 25, same
+// box), the block's own loads already keep HBM as busy as the prefetches do.
 // decomposed lattice: the hop of variant 25 (4 slots, 5 blocks per SM,
 // persistent, packed) reading the halos of gh; KIND 1 or 3
 static void launch_q16_dd(int kind, int nl, bool recon, float c_long, int grid, uint4 *out, const uint4 *src,
@@ -1148,6 +1172,13 @@ static void launch_q16_fused(int variant, int nl, bool recon, float c_long, int 
     else if (recon) launch_k(pdl, k_mix_hop_q16r<16, 3, B, true, M, true, true>, gp, QB, c.s, Q16_ARGS3);     \
     else launch_k(pdl, k_mix_hop_q16r<16, 3, B, false, M, true, true>, gp, QB, c.s, Q16_ARGS3);               \
   } while (0)
+#define Q16RPK3F(B, M, F)                                                                                           \
+  do {                                                                                                              \
+    const int gp = std::min(grid, (c.red_blocks / 8) * M);                                                          \
+    if (nl != 16) launch_k(pdl, k_mix_hop_q16r<8, 3, B, false, M, true, true, false, F>, gp, QB, c.s, Q16_ARGS3);   \
+    else if (recon) launch_k(pdl, k_mix_hop_q16r<16, 3, B, true, M, true, true, false, F>, gp, QB, c.s, Q16_ARGS3); \
+    else launch_k(pdl, k_mix_hop_q16r<16, 3, B, false, M, true, true, false, F>, gp, QB, c.s, Q16_ARGS3);           \
+  } while (0)
   switch (variant) {
     case 20: Q16RPK3(2, 6); break;
     case 21: Q16RPK3(2, 7); break;
@@ -1157,8 +1188,12 @@ static void launch_q16_fused(int variant, int nl, bool recon, float c_long, int 
     case 26: Q16RPK3(8, 6); break;
     case 27: Q16RPK3(4, 4); break;
     case 28: Q16RPK3(8, 4); break;
+    case 29: Q16RPK3F(4, 5, 2); break;
+    case 30: Q16RPK3F(4, 5, 4); break;
+    case 31: Q16RPK3F(4, 5, 1); break;
     default: Q16RPK3(4, 5); break;
   }
+#undef Q16RPK3F
 #undef Q16RPK3
 #undef Q16_ARGS3
 }
@@ -1195,6 +1230,16 @@ static void launch_q16(int variant, int nl, bool recon, float c_long, int grid, 
     else if (recon) launch_k(pdl, k_mix_hop_q16r<16, KIND, B, true, M, true, true>, gp, QB, c.s, Q16_ARGS, Q16PK_TAIL); \
     else launch_k(pdl, k_mix_hop_q16r<16, KIND, B, false, M, true, true>, gp, QB, c.s, Q16_ARGS, Q16PK_TAIL);           \
   } while (0)
+#define Q16RPKF(B, M, F)                                                                                      \
+  do {                                                                                                         \
+    const int gp = std::min(grid, (c.red_blocks / 8) * M);                                                     \
+    if (nl != 16)                                                                                              \
+      launch_k(pdl, k_mix_hop_q16r<8, KIND, B, false, M, true, true, false, F>, gp, QB, c.s, Q16_ARGS, Q16PK_TAIL);  \
+    else if (recon)                                                                                            \
+      launch_k(pdl, k_mix_hop_q16r<16, KIND, B, true, M, true, true, false, F>, gp, QB, c.s, Q16_ARGS, Q16PK_TAIL);  \
+    else                                                                                                       \
+      launch_k(pdl, k_mix_hop_q16r<16, KIND, B, false, M, true, true, false, F>, gp, QB, c.s, Q16_ARGS, Q16PK_TAIL); \
+  } while (0)
 #define Q16A(RR, M)                                                                                       \
   do {                                                                                                    \
     const int gp = std::min(grid, (c.red_blocks / 8) * M);                                                \
@@ -1227,6 +1272,9 @@ static void launch_q16(int variant, int nl, bool recon, float c_long, int grid, 
     case 26: Q16RPK(8, 6); break;
     case 27: Q16RPK(4, 4); break;
     case 28: Q16RPK(8, 4); break;
+    case 29: Q16RPKF(4, 5, 2); break;   // 25 with an L2 prefetch two slot batches ahead
+    case 30: Q16RPKF(4, 5, 4); break;   // ... one site block ahead
+    case 31: Q16RPKF(4, 5, 1); break;   // ... one slot batch ahead
     case 1:
       if (nl == 16) k_mix_hop_q16<16, KIND, 2><<<grid, QB, 4 * QSLOT, c.s>>>(Q16_ARGS);
       else k_mix_hop_q16<8, KIND, 2><<<grid, QB, 4 * QSLOT, c.s>>>(Q16_ARGS);

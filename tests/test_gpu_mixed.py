@@ -239,9 +239,10 @@ def _single_iters(q, fla, src, m, L, eo=0):
 
 
 def test_every_hop_kernel_variant():
-    """Each selectable int16 hop kernel (option hop_kernel 0-28: plain,
+    """Each selectable int16 hop kernel (option hop_kernel 0-31: plain,
     TMA-staged, register-capped, persistent, cp.async-ring and packed
-    FP32x2 forms) solves to the FP64 target; the scalar forms share the
+    FP32x2 forms, the last three with an L2 prefetch of the link stream)
+    solves to the FP64 target; the scalar forms share the
     decode and arithmetic order and the packed forms round the scaled site
     components first, so the iteration counts agree within a few per cent."""
     L = (8, 8, 8, 8)
@@ -251,13 +252,13 @@ def test_every_hop_kernel_variant():
     fla = q.create_L_from_raw(fat, lng)
     src = LT.gaussian_vector(L, 330)
     its = {}
-    for v in range(29):
+    for v in range(32):
         assert q.set_opts(prec_sloppy=16, hop_kernel=v) == 0
         st, it, got = _single_iters(q, fla, src, 0.03, L)
         assert st == 0
         assert eo_residual(fo, 0.03, got, src, L, 0) <= 1.05e-20, v
         its[v] = it
-    assert q.set_opts(hop_kernel=29) != 0                  # out of range
+    assert q.set_opts(hop_kernel=32) != 0                  # out of range
     assert q.set_opts(prec_sloppy=64, hop_kernel=25) == 0
     ref = its[25]
     assert all(abs(i - ref) <= 0.03 * ref + 3 for i in its.values()), its
