@@ -90,6 +90,8 @@ def parse():
     ap.add_argument("--dd-max-iter", type=int, default=200000, help="dd workload: iteration limit of each solve")
     ap.add_argument("--hop-kernel", type=int, default=None, help="int16 hop variant (library default if unset)")
     ap.add_argument("--batch-kernel", type=int, default=None, help="batched hop variant (chosen by batch size if unset)")
+    ap.add_argument("--ms-stop", type=float, default=None,
+                    help="multi-shift phase: stop target of the shifted systems (relative |r|^2; library default if unset)")
     ap.add_argument("--ab", default=None, help="A/B of a 0/1 solver option (e.g. fuse_update) on the headline solve: "
                                                "--steps pairs of solves interleaved in one process, clocks sampled")
     ap.add_argument("--workload", default="single",
@@ -110,6 +112,8 @@ def kernel_opts(a):
         o["hop_kernel"] = a.hop_kernel
     if a.batch_kernel is not None:
         o["batch_kernel"] = a.batch_kernel
+    if a.ms_stop is not None:
+        o["ms_stop"] = a.ms_stop
     return o
 
 

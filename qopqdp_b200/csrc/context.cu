@@ -279,7 +279,7 @@ int QOP_sites_on_node_raw_G(QOP_evenodd_t eo) { (void)eo; return (int)ctx().g.V;
 
 // tags: st, ns, nm, cg, eigcg_nev, eigcg_m, eigcg_l (reference) and
 // prec_sloppy (64|32|16), half_format, hop_kernel, recon_long, multi_shift,
-// batch_tail, ru_delta, chunk (B200 additions)
+// batch_tail, ms_stop, ru_delta, chunk (B200 additions)
 QOP_status_t QOP_asqtad_invert_set_opts(QOP_opt_t opts[], int nopts) {
   Options &o = ctx().opt;
   int st = o.style, ns = o.nsvec, nm = o.nvec;
@@ -313,6 +313,9 @@ QOP_status_t QOP_asqtad_invert_set_opts(QOP_opt_t opts[], int nopts) {
       n.fuse_update = v != 0;
     } else if (!strcmp(t, "batch_tail")) {
       n.batch_tail = v != 0;
+    } else if (!strcmp(t, "ms_stop")) {
+      if (!(v == -1 || (v >= 0 && v < 1))) return QOP_FAIL;
+      n.ms_stop = v;
     } else if (!strcmp(t, "pdl")) {
       n.pdl = v != 0;
     } else if (!strcmp(t, "serve_policy")) {

@@ -1662,9 +1662,16 @@ void solve_multi_mixed(QOP_info_t *info, FlaT<double> *f, QOP_invert_arg_t *ia, 
     if (!ok || b2 == 0.0) continue;
     std::vector<double> sigma(ns), stop(ns, -1.0);
     for (int s = 0; s < ns; s++) sigma[s] = m2[s] - m2[0];
+    // The shifted systems are refined afterwards, and their phase-1
+    // residuals cannot fall below the sloppy operator's drift, (eps kappa_s)^2
+    // relative with eps ~ 2^-15 for int16 storage (>= 1e-9 for kappa_s >= 1):
+    // they stop at ms_stop (by default 1e-10 with int16 storage), which
+    // spares the update of shifts that can no longer improve.  The lightest
+    // mass keeps its own target.
+    const double ms_stop = o.ms_stop >= 0 ? o.ms_stop : (batched ? 1e-10 : 0.0);
     for (int j : grp) {
       const int s = (int)(std::lower_bound(m2.begin(), m2.end(), masses[j] * masses[j]) - m2.begin());
-      const double t = ra[j]->rsqmin * b2;
+      const double t = (s > 0 ? std::max(ra[j]->rsqmin, ms_stop) : ra[j]->rsqmin) * b2;
       stop[s] = stop[s] < 0 ? t : std::min(stop[s], t);
     }
     ScopedVecs own;   // the phase's vectors

@@ -114,6 +114,7 @@ struct Options {
   int recon_long = 1;            // int16 long links as two rows + det phase when exact
   int batch_kernel = -1;         // batched int16 hop variant (batch.cu kBhop); -1: by the number of systems, -2: autotuned
   int multi_shift = 1;           // int16 multi-mass: 1 = sloppy multi-shift CG before the batched refinement (default), 0 = batched only
+  double ms_stop = -1;           // multi-shift phase: a shifted system (not the lightest mass) stops at max(its rsqmin, ms_stop); -1: 1e-10 with int16 storage, else 0
   int fuse_update = 1;           // int16 hop variants 20-26: 1 = the second hop reduces for a fused x / r / p update
   int batch_tail = 1;            // batched solves: 1 = the last running system finishes in the one-system solver
   int pdl = 1;                   // fused int16 iteration: 1 = its kernels launched as programmatic dependents
